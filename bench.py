@@ -1,0 +1,319 @@
+"""Benchmark: 30-qubit depth-20 random circuit, FP64, through libdgq.
+
+One step = one full circuit on the resident 2^30-amplitude complex128 state
+(16 GiB in HBM): initialise |0...0> and apply every planned sweep. Workload
+(the reference's headline configuration for this path): per layer a random
+Rx/Ry/Rz with angle U[0, 2pi) on each of the 30 qubits, then CZ on a seeded
+perfect matching; 20 layers; seed 20261203 + 2000; MT19937 draws.
+
+  value   circuits/s over all ranks, kernels only, state resident in HBM
+          (CUDA events on the library's stream around K steps)
+  e2e     the same metric through the public QuEST API each step: record
+          every gate call, getAmp(q, 0) (plans + runs), calcProbOfOutcome
+          for every qubit; kernel programs travel host->device as kernel
+          parameters, the amplitude and probabilities come back
+  roofline  the tile kernel (the only kernel of a step) against the measured
+          HBM copy bandwidth; algorithmic bytes per launch = 2 * 2^30 * 16 B
+
+Inputs are larger than L2 (16 GiB state vs 126 MB L2), so no flush is needed.
+With --gpus N (torchrun), each rank runs an independent replica (the path
+does not shard on one GPU); the time is the max over ranks.
+`--impl reference` times the reference's algorithm on the host cores instead
+(the CPU oracle, OpenMP on all cores, on a bounded sample of the circuit).
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "30q circuit time & HBM GB/s FP64 vs FP32-TC @fidelity≥1−1e-6; serving p99 ms"
+N_QUBITS = 30
+DEPTH = 20
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, nm in enumerate(names):
+                if s[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        loaded = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU legs
+def cpu_sample(ops, n, gates, threads=None):
+    """Times the oracle on the first `gates` calls of the circuit (state of n qubits)."""
+    import oracle
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    o = oracle.Oracle(n)
+    sample = ops[:gates]
+    t0 = time.perf_counter()
+    o.apply(sample)
+    dt = time.perf_counter() - t0
+    o.close()
+    return dt, oracle.max_threads()
+
+
+def run_reference_arm(args, world, rank):
+    from dgquest_b200 import circuits as C
+    if rank != 0:
+        return
+    ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))
+    gates = args.ref_gates
+    for _ in range(args.warmup):
+        cpu_sample(ops, N_QUBITS, max(1, gates // 4))
+    times = []
+    cores = 1
+    for _ in range(args.steps):
+        dt, cores = cpu_sample(ops, N_QUBITS, gates)
+        times.append(dt)
+    t = float(np.mean(times))
+    circuits_per_s = (gates / len(ops)) / t
+    sample = f"first {gates} of {len(ops)} gate calls of the 30-qubit circuit per step, scaled by {len(ops)}/{gates}"
+    line = {"metric": METRIC, "value": circuits_per_s, "unit": "circuits/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * len(ops) / gates * 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded MT19937 random circuit)", "impl": "reference",
+            "config": {"workload": "random circuit n=30 depth=20 (Rx/Ry/Rz + CZ matching), complex128",
+                       "qubits": N_QUBITS, "depth": DEPTH, "parallelism": "host cores"},
+            "cpu_baseline": {"value": circuits_per_s, "unit": "circuits/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": circuits_per_s, "unit": "circuits/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_gpu(args, world, rank, local):
+    import torch
+
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+
+    torch.cuda.set_device(local)
+    n, depth = args.qubits, args.depth
+    ops = C.random_layers(n, depth, C.config_seed(2))
+    env = Q.createQuESTEnv()
+    q = Q.createQureg(n, env)
+    if args.tile_bits:
+        Q.dgq_setTileBits(q, args.tile_bits)
+    stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+
+    # plan once (host), then every step relaunches the full plan from |0...0>
+    Q.initZeroState(q)
+    C.replay(q, ops)
+    Q.dgq_planPending(q)
+    st = Q.plan_stats(q)
+    for _ in range(args.warmup):
+        Q.dgq_launchPlanned(q)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = Q.dgq_getLaunchCount()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        Q.dgq_launchPlanned(q)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = Q.dgq_getLaunchCount() - l0
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms, world)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1000.0)
+
+    # numerics of the timed plan: norm must stay 1
+    norm = Q.calcTotalProb(q)
+
+    # e2e through the public API
+    e2e_times = []
+    for i in range(args.e2e_steps + 1):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Q.initZeroState(q)
+        C.replay(q, ops)
+        a = Q.getAmp(q, 0)
+        probs = [Q.calcProbOfOutcome(q, k, 0) for k in range(n)]
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+    e2e_t = max_over_ranks(float(np.mean(e2e_times)), world)
+    st2 = Q.plan_stats(q)
+    from dgquest_b200.quest import ctypes as _ct  # noqa: F401
+    prog_bytes = 25048  # sizeof(TileProgram): the kernel parameter block of one launch
+    h2d = st2.sweeps * prog_bytes
+    d2h = 16 + (n + 1) * 8
+
+    hbm, hbm_kind = peaks()
+    bytes_per_launch = 2.0 * (1 << n) * 16
+    avg_launch_s = (ms_step / 1000.0) / st.sweeps
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    flops = st.flopsPerAmp * (1 << n)
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("tile_kernel_bytes_per_launch_n30")
+    Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded MT19937 random circuit)",
+                "config": {"workload": "random circuit n=30 depth=20 (Rx/Ry/Rz + CZ matching), complex128",
+                           "qubits": n, "depth": depth, "tile_bits": st.tileBits, "sweeps": st.sweeps,
+                           "phases": st.phases, "gates_after_merge": st.gates,
+                           "l2": "inputs larger than L2 (16 GiB state)", "parallelism": f"replicas x{world}"},
+                "gate_layers_per_s": depth / (ms_step / 1000.0),
+                "hbm_gbs_step": bytes_per_launch * st.sweeps / (ms_step / 1000.0) / 1e9,
+                "fp64_tflops_algorithmic": flops / (ms_step / 1000.0) / 1e12,
+                "norm_error": abs(norm - 1.0),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": achieved / hbm, "traffic": traffic,
+                             "peak_source": hbm_kind, "kernel": f"tileKernel<{st.tileBits}>"},
+                "e2e": {"value": world / e2e_t, "unit": "circuits/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t * 1000.0,
+                        "plan_ms": st2.planMillis},
+                "gpu_launches": int(launches), "clocks": clk}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dgq", choices=["dgq", "reference"])
+    ap.add_argument("--qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--depth", type=int, default=DEPTH)
+    ap.add_argument("--tile-bits", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-gates", type=int, default=8)
+    ap.add_argument("--cpu-gates", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "dgq" else args.warmup
+
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    line = run_gpu(args, world, rank, local)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from dgquest_b200 import circuits as C
+        ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))
+        dt, cores = cpu_sample(ops, N_QUBITS, args.cpu_gates)
+        line["cpu_baseline"] = {"value": (args.cpu_gates / len(ops)) / dt, "unit": "circuits/s", "cores": cores,
+                                "kind": "port",
+                                "sample": f"oracle (OpenMP) on the first {args.cpu_gates} of {len(ops)} gate "
+                                          f"calls, 30 qubits, scaled by {len(ops)}/{args.cpu_gates}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

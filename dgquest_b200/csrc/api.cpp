@@ -1,0 +1,1186 @@
+// api.cpp -- the QuEST C API of libdgq and the per-register engine behind it.
+//
+// Front end (validation, API -> gate encoding) follows dgQuEST's
+// src/QuEST.c:30-458, src/QuEST_validation.c and
+// src/cpp/QuEST_distributed.cpp:106-364. The engine replaces dgQuEST's
+// orchestrator (src/cpp/QuEST_backend_distributed.cpp): the state is
+// resident in HBM, so there are no tasks, pages or MPI exchanges; pending
+// gates are planned into tile sweeps and launched on the register's stream
+// when a read-out needs them (QuEST_distributed.cpp:106-116).
+#include <sys/time.h>
+#include <unistd.h>
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "QuEST.h"
+#include "dgq.h"
+#include "dag.h"
+#include "ir.h"
+#include "kernels.h"
+#include "planner.h"
+#include "rng.h"
+
+using dgq::Gate;
+
+
+// ====================================================================
+// errors (codes and messages of src/QuEST_validation.c:19-80)
+// ====================================================================
+namespace {
+
+enum ErrorCode {
+    E_SUCCESS = 0,
+    E_INVALID_NUM_QUBITS,
+    E_INVALID_TARGET_QUBIT,
+    E_INVALID_CONTROL_QUBIT,
+    E_INVALID_STATE_INDEX,
+    E_INVALID_NUM_AMPS,
+    E_INVALID_OFFSET_NUM_AMPS,
+    E_TARGET_IS_CONTROL,
+    E_TARGET_IN_CONTROLS,
+    E_TARGETS_NOT_UNIQUE,
+    E_INVALID_NUM_CONTROLS,
+    E_NON_UNITARY_MATRIX,
+    E_NON_UNITARY_COMPLEX_PAIR,
+    E_ZERO_VECTOR,
+    E_SYS_TOO_BIG_TO_PRINT,
+    E_COLLAPSE_STATE_ZERO_PROB,
+    E_INVALID_QUBIT_OUTCOME,
+    E_CANNOT_OPEN_FILE,
+    E_SECOND_ARG_MUST_BE_STATEVEC,
+    E_MISMATCHING_QUREG_DIMENSIONS,
+    E_MISMATCHING_QUREG_TYPES,
+    E_DEFINED_ONLY_FOR_STATEVECS,
+    E_DEFINED_ONLY_FOR_DENSMATRS,
+    E_INVALID_PROB,
+    E_UNNORM_PROBS,
+    E_INVALID_ONE_QUBIT_DEPHASE_PROB,
+    E_INVALID_TWO_QUBIT_DEPHASE_PROB,
+    E_INVALID_ONE_QUBIT_DEPOL_PROB,
+    E_INVALID_TWO_QUBIT_DEPOL_PROB,
+    // codes of this library (no counterpart in dgQuEST)
+    E_INVALID_NUM_TARGETS = 100,
+    E_SYS_TOO_BIG_FOR_DEVICE = 101,
+    E_UNSUPPORTED = 102,
+    E_CUDA = 103,
+    E_INVALID_ARGUMENT = 104,
+};
+
+const char *errorMessage(int code) {
+    switch (code) {
+        case E_INVALID_NUM_QUBITS: return "Invalid number of qubits. Must create >0.";
+        case E_INVALID_TARGET_QUBIT: return "Invalid target qubit. Note qubits are zero indexed.";
+        case E_INVALID_CONTROL_QUBIT: return "Invalid control qubit. Note qubits are zero indexed.";
+        case E_INVALID_STATE_INDEX: return "Invalid state index. Must be >=0 and <2^numQubits.";
+        case E_INVALID_NUM_AMPS: return "Invalid number of amplitudes. Must be >=0 and <=2^numQubits.";
+        case E_INVALID_OFFSET_NUM_AMPS: return "More amplitudes given than exist in the statevector from the given starting index.";
+        case E_TARGET_IS_CONTROL: return "Control qubit cannot equal target qubit.";
+        case E_TARGET_IN_CONTROLS: return "Control qubits cannot include target qubit.";
+        case E_TARGETS_NOT_UNIQUE: return "The two target qubits must be unique.";
+        case E_INVALID_NUM_CONTROLS: return "Invalid number of control qubits. Must be >0 and <numQubits.";
+        case E_NON_UNITARY_MATRIX: return "Matrix is not unitary.";
+        case E_NON_UNITARY_COMPLEX_PAIR: return "Compact matrix formed by given complex numbers is not unitary.";
+        case E_ZERO_VECTOR: return "Invalid axis vector. Must be non-zero.";
+        case E_COLLAPSE_STATE_ZERO_PROB: return "Can't collapse to state with zero probability.";
+        case E_INVALID_QUBIT_OUTCOME: return "Invalid measurement outcome -- must be either 0 or 1.";
+        case E_DEFINED_ONLY_FOR_STATEVECS: return "Operation valid only for state-vectors.";
+        case E_INVALID_NUM_TARGETS: return "Invalid number of target qubits. Must be >0 and <=numQubits, and unique.";
+        case E_SYS_TOO_BIG_FOR_DEVICE: return "The state-vector does not fit in free GPU memory.";
+        case E_UNSUPPORTED: return "Operation not supported by this build.";
+        case E_CUDA: return "CUDA runtime error.";
+        case E_INVALID_ARGUMENT: return "Invalid argument.";
+        default: return "Unknown error.";
+    }
+}
+
+std::mutex g_errMutex;
+int g_errMode = DGQ_ERRORS_EXIT;
+int g_lastError = 0;
+std::string g_lastMessage;
+std::atomic<int64_t> g_launches{0};
+dgq::Mt19937 g_rng;
+
+// Raises an error: exits (default) or records it. Always returns false so
+// that callers can write `if (!ok) return ...`.
+bool raise(int code, const char *func, const char *detail = nullptr) {
+    std::string msg = std::string("QuEST Error in function ") + func + ": " + errorMessage(code);
+    if (detail && *detail) msg += std::string(" (") + detail + ")";
+    if (g_errMode == DGQ_ERRORS_EXIT) {
+        printf("!!!\n%s\n!!!\nexiting..\n", msg.c_str());
+        fflush(stdout);
+        exit(code);
+    }
+    std::lock_guard<std::mutex> lk(g_errMutex);
+    g_lastError = code;
+    g_lastMessage = msg;
+    return false;
+}
+
+bool cudaOk(cudaError_t e, const char *func) {
+    if (e == cudaSuccess) return true;
+    return raise(E_CUDA, func, cudaGetErrorString(e));
+}
+
+double nowMillis() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+// ====================================================================
+// environment and register state
+// ====================================================================
+struct QuESTEnvValue {
+    int device = 0;
+};
+
+struct QuregState {
+    int numQubits = 0;  // user-visible qubits
+    int numBits = 0;    // address bits of the buffer (>= numQubits, >= kMinTileBits)
+    double2 *dState = nullptr;
+    cudaStream_t stream = nullptr;
+
+    // recorded, not yet executed
+    std::vector<Gate> pending;
+    dgq::MatrixPool pool;
+    bool initPending = false;
+    int32_t initKind = dgq::INIT_NONE;
+    uint64_t initIndex = 0;
+    double initAmp = 0.0;
+
+    // lazy measurement collapse applied to the state in HBM
+    bool restrictActive = false;
+    uint64_t rMask = 0, rValue = 0;
+    double rScale = 1.0;
+
+    // logical qubit -> address bit (swapGate relabels instead of moving data)
+    int l2v[64];
+    int v2l[64];
+
+    // P(bit = 0) per address bit, of the (collapsed, normalised) state
+    bool probsValid = false;
+    std::vector<double> p0;
+    double totalProb = 1.0;
+    double *dPartial = nullptr;
+    size_t partialCap = 0;
+    double *dProbOut = nullptr;
+
+    int tileBitsSetting = 0;  // 0 = cost model
+    std::vector<dgq::TileProgram> planned;
+    int plannedTileBits = 0;
+    dgq_plan_stats stats{};
+};
+
+namespace {
+
+QuregState *stateOf(const Qureg &q) { return q.state; }
+
+void resetMapping(QuregState &s) {
+    for (int i = 0; i < 64; i++) {
+        s.l2v[i] = i;
+        s.v2l[i] = i;
+    }
+}
+
+u64 toVirtualMask(const QuregState &s, u64 logicalMask) {
+    u64 v = 0;
+    for (int b = 0; b < s.numQubits; b++)
+        if ((logicalMask >> b) & 1ULL) v |= 1ULL << s.l2v[b];
+    return v;
+}
+
+uint64_t toVirtualIndex(const QuregState &s, uint64_t logical) {
+    uint64_t v = 0;
+    for (int b = 0; b < s.numQubits; b++) v |= ((logical >> b) & 1ULL) << s.l2v[b];
+    return v;
+}
+
+// ---------------------------------------------------------------- cost model
+// Recast of dgQuEST's time predictor (src/cpp/time_predictor.cpp:201-395):
+// dgQuEST predicts T(K) = sum over sections of the calculation time
+// (processTime + sum of per-gate times per fused gate) plus transfers, and
+// takes the argmin over K. Here the state stays in HBM, so a plan's time is
+// the sum over sweeps of max(HBM time, FP64 time + shared-memory time), and
+// the argmin is over the tile width W.
+struct CostModel {
+    double hbmBytesPerSec = 6.0e12;
+    double fp64FlopsPerSec = 3.0e13;
+    double smemBytesPerSec = 3.0e13;
+};
+
+double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, const dgq::MatrixPool &pool) {
+    const CostModel cm;
+    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(gates, numBits, W);
+    const double amps = std::ldexp(1.0, numBits);
+    double t = 0.0;
+    for (const auto &b : blocks) {
+        std::vector<dgq::TileProgram> progs;
+        dgq::PlanStats st;
+        dgq::SweepHeader h;
+        std::string err;
+        if (!dgq::encodeBlock(b, numBits, numBits, W, pool, h, progs, &st, &err)) return 1e30;
+        const double mem = st.sweeps * amps * 32.0 / cm.hbmBytesPerSec;
+        const double comp = amps * st.flopsPerAmp / cm.fp64FlopsPerSec +
+                            (st.phases + st.sweeps) * amps * 32.0 / cm.smemBytesPerSec;
+        t += std::max(mem, comp);
+    }
+    return t;
+}
+
+int chooseTileBits(QuregState &s) {
+    const int hi = std::min(dgq::kMaxTileBits, s.numBits);
+    const int lo = dgq::kMinTileBits;
+    if (s.tileBitsSetting > 0) return std::max(lo, std::min(hi, s.tileBitsSetting));
+    if (const char *env = getenv("DGQ_TILE_BITS")) {
+        const int w = atoi(env);
+        if (w > 0) return std::max(lo, std::min(hi, w));
+    }
+    int best = std::min(hi, 12);
+    double bestT = 1e300;
+    for (int W = lo; W <= hi; W++) {
+        const double t = predictPlanSeconds(s.pending, s.numBits, W, s.pool);
+        if (t < bestT * 0.98) {  // prefer the smaller tile on near ties
+            bestT = t;
+            best = W;
+        }
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------- execution
+bool planPending(QuregState &s, const char *func) {
+    s.planned.clear();
+    if (s.pending.empty() && !s.initPending) return true;
+    const double t0 = nowMillis();
+    const int W = chooseTileBits(s);
+    dgq::SweepHeader h;
+    if (s.initPending) {
+        h.initKind = s.initKind;
+        h.initIndex = s.initIndex;
+        h.initAmp = s.initAmp;
+    } else if (s.restrictActive) {
+        h.hasRestrict = true;
+        h.restrictMask = s.rMask;
+        h.restrictValue = s.rValue;
+        h.restrictScale = s.rScale;
+    }
+    dgq::PlanStats st;
+    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(s.pending, s.numBits, W);
+    size_t planned = 0;
+    for (const auto &b : blocks) planned += b.gates.size();
+    {
+        // gates left unplanned would be wider than a tile
+        dgq::GateDag check(s.numBits, true);
+        for (const Gate &g : s.pending) check.add(g);
+        if (planned != check.size()) {
+            return raise(E_UNSUPPORTED, func, "a multi-qubit gate is wider than the register tile (max 4 targets)");
+        }
+    }
+    std::string err;
+    bool first = true;
+    for (const auto &b : blocks) {
+        dgq::SweepHeader hb = first ? h : dgq::SweepHeader();
+        if (!dgq::encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, s.planned, &st, &err))
+            return raise(E_UNSUPPORTED, func, err.c_str());
+        first = false;
+    }
+    if (blocks.empty()) {
+        s.planned.emplace_back();
+        dgq::encodeHeaderOnly(s.numBits, s.numQubits, W, h, s.planned.back());
+        st.sweeps = 1;
+    }
+    s.plannedTileBits = W;
+    s.stats.sweeps = st.sweeps;
+    s.stats.phases = st.phases;
+    s.stats.ops = st.ops;
+    s.stats.gates = st.gates;
+    s.stats.tileBits = W;
+    s.stats.numBits = s.numBits;
+    s.stats.flopsPerAmp = st.flopsPerAmp;
+    s.stats.planMillis = nowMillis() - t0;
+    s.pending.clear();
+    s.pool.mats.clear();
+    s.initPending = false;
+    s.restrictActive = false;
+    s.rMask = s.rValue = 0;
+    s.rScale = 1.0;
+    s.probsValid = false;
+    return true;
+}
+
+bool launchPlanned(QuregState &s, const char *func) {
+    for (const auto &p : s.planned) {
+        if (!cudaOk(dgq::launchTile(s.dState, s.plannedTileBits, p, s.stream), func)) return false;
+        g_launches++;
+    }
+    return true;
+}
+
+bool flush(QuregState &s, const char *func) {
+    if (s.pending.empty() && !s.initPending) return true;
+    if (!planPending(s, func)) return false;
+    return launchPlanned(s, func);
+}
+
+bool ensureProbs(QuregState &s, const char *func) {
+    if (s.probsValid) return true;
+    if (!flush(s, func)) return false;
+    dgq::ProbArgs a;
+    std::memset(&a, 0, sizeof(a));
+    int nf = 0;
+    for (int b = 0; b < s.numBits; b++) {
+        if (s.restrictActive && ((s.rMask >> b) & 1ULL)) continue;
+        a.freePos[nf++] = (uint8_t) b;
+    }
+    a.nFree = nf;
+    a.kappa = std::min(4, std::max(0, nf - 12));
+    a.rValue = s.restrictActive ? s.rValue : 0;
+    const size_t need = (size_t) dgq::probNumCtas(a) * 17;
+    if (need > s.partialCap) {
+        if (s.dPartial) cudaFree(s.dPartial);
+        s.dPartial = nullptr;
+        if (!cudaOk(cudaMalloc(&s.dPartial, need * sizeof(double)), func)) return false;
+        s.partialCap = need;
+    }
+    if (!cudaOk(dgq::launchProb(s.dState, a, s.dPartial, s.dProbOut, s.stream), func)) return false;
+    g_launches += 2;
+    std::vector<double> out((size_t) nf + 1);
+    if (!cudaOk(cudaMemcpyAsync(out.data(), s.dProbOut, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s.stream),
+                func))
+        return false;
+    if (!cudaOk(cudaStreamSynchronize(s.stream), func)) return false;
+    const double sc2 = s.restrictActive ? s.rScale * s.rScale : 1.0;
+    s.p0.assign((size_t) s.numBits, 0.0);
+    s.totalProb = out[(size_t) nf] * sc2;
+    for (int i = 0; i < nf; i++) s.p0[a.freePos[i]] = out[(size_t) i] * sc2;
+    if (s.restrictActive) {
+        for (int b = 0; b < s.numBits; b++) {
+            if (!((s.rMask >> b) & 1ULL)) continue;
+            s.p0[(size_t) b] = ((s.rValue >> b) & 1ULL) ? 0.0 : s.totalProb;
+        }
+    }
+    s.probsValid = true;
+    return true;
+}
+
+// ---------------------------------------------------------------- validation
+bool vQureg(const Qureg &q, const char *func) {
+    if (!q.state) return raise(E_INVALID_ARGUMENT, func, "destroyed or uninitialised Qureg");
+    return true;
+}
+bool vTarget(const Qureg &q, int t, const char *func) {
+    if (!vQureg(q, func)) return false;
+    if (t < 0 || t >= (int) q.numQubitsRepresented) return raise(E_INVALID_TARGET_QUBIT, func);
+    return true;
+}
+bool vControlTarget(const Qureg &q, int c, int t, const char *func) {
+    if (!vTarget(q, t, func)) return false;
+    if (c < 0 || c >= (int) q.numQubitsRepresented) return raise(E_INVALID_CONTROL_QUBIT, func);
+    if (c == t) return raise(E_TARGET_IS_CONTROL, func);
+    return true;
+}
+bool vUniqueTargets(const Qureg &q, int a, int b, const char *func) {
+    if (!vTarget(q, a, func) || !vTarget(q, b, func)) return false;
+    if (a == b) return raise(E_TARGETS_NOT_UNIQUE, func);
+    return true;
+}
+bool vMultiControls(const Qureg &q, const int *c, int n, const char *func) {
+    if (!vQureg(q, func)) return false;
+    if (n < 1 || n > (int) q.numQubitsRepresented || !c) return raise(E_INVALID_NUM_CONTROLS, func);
+    for (int i = 0; i < n; i++)
+        if (c[i] < 0 || c[i] >= (int) q.numQubitsRepresented) return raise(E_INVALID_CONTROL_QUBIT, func);
+    return true;
+}
+bool vStateIndex(const Qureg &q, long long idx, const char *func) {
+    if (!vQureg(q, func)) return false;
+    const long long maxIdx = 1LL << q.numQubitsRepresented;
+    if (idx < 0 || idx >= maxIdx) return raise(E_INVALID_STATE_INDEX, func);
+    return true;
+}
+bool vOutcome(int o, const char *func) {
+    if (o != 0 && o != 1) return raise(E_INVALID_QUBIT_OUTCOME, func);
+    return true;
+}
+// src/QuEST_validation.c:103-128
+bool isPairUnitary(Complex a, Complex b) {
+    return std::fabs(-1 + a.real * a.real + a.imag * a.imag + b.real * b.real + b.imag * b.imag) < REAL_EPS;
+}
+bool isMatrix2Unitary(const ComplexMatrix2 &u) {
+    if (std::fabs(u.r0c0.real * u.r0c0.real + u.r0c0.imag * u.r0c0.imag + u.r1c0.real * u.r1c0.real +
+                  u.r1c0.imag * u.r1c0.imag - 1) > REAL_EPS)
+        return false;
+    if (std::fabs(u.r0c1.real * u.r0c1.real + u.r0c1.imag * u.r0c1.imag + u.r1c1.real * u.r1c1.real +
+                  u.r1c1.imag * u.r1c1.imag - 1) > REAL_EPS)
+        return false;
+    if (std::fabs(u.r0c0.real * u.r0c1.real + u.r0c0.imag * u.r0c1.imag + u.r1c0.real * u.r1c1.real +
+                  u.r1c0.imag * u.r1c1.imag) > REAL_EPS)
+        return false;
+    if (std::fabs(u.r0c1.real * u.r0c0.imag - u.r0c0.real * u.r0c1.imag + u.r1c1.real * u.r1c0.imag -
+                  u.r1c0.real * u.r1c1.imag) > REAL_EPS)
+        return false;
+    return true;
+}
+
+// ---------------------------------------------------------------- recording
+void record(const Qureg &q, dgq::GateType type, u64 logicalTargets, u64 logicalControls, const double *op, int nop) {
+    QuregState &s = *stateOf(q);
+    Gate g;
+    g.type = type;
+    g.targetMask = toVirtualMask(s, logicalTargets);
+    g.controlMask = toVirtualMask(s, logicalControls);
+    for (int i = 0; i < nop; i++) g.op[i] = op[i];
+    s.pending.push_back(g);
+    s.probsValid = false;
+}
+
+void recordMatrix(const Qureg &q, u64 targets, u64 controls, const ComplexMatrix2 &u) {
+    const double m[8] = {u.r0c0.real, u.r0c0.imag, u.r0c1.real, u.r0c1.imag,
+                         u.r1c0.real, u.r1c0.imag, u.r1c1.real, u.r1c1.imag};
+    record(q, dgq::OP_UNITARY, targets, controls, m, 8);
+}
+
+u64 bit(int q) { return 1ULL << q; }
+
+}  // namespace
+
+// ====================================================================
+// C API
+// ====================================================================
+extern "C" {
+
+int dgq_setErrorMode(int mode) {
+    const int prev = g_errMode;
+    g_errMode = mode == DGQ_ERRORS_RECORD ? DGQ_ERRORS_RECORD : DGQ_ERRORS_EXIT;
+    return prev;
+}
+
+int dgq_getLastError(char *msg, int len) {
+    std::lock_guard<std::mutex> lk(g_errMutex);
+    const int code = g_lastError;
+    if (msg && len > 0) {
+        std::strncpy(msg, g_lastMessage.c_str(), (size_t) len - 1);
+        msg[len - 1] = '\0';
+    }
+    g_lastError = 0;
+    g_lastMessage.clear();
+    return code;
+}
+
+int64_t dgq_getLaunchCount(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------- env
+void seedQuESTDefault(void) {
+    // src/QuEST_common.c:127-142: milliseconds since the epoch and the pid
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    const double ms = (double) tv.tv_sec * 1000 + (double) (tv.tv_usec / 1000);
+    unsigned long key[2] = {(unsigned long) ms, (unsigned long) getpid()};
+    g_rng.seedArray(key, 2);
+}
+
+void seedQuEST(unsigned long int *seedArray, int numSeeds) {
+    if (!seedArray || numSeeds < 1) {
+        raise(E_INVALID_ARGUMENT, __func__, "need at least one seed");
+        return;
+    }
+    g_rng.seedArray(seedArray, numSeeds);
+}
+
+QuESTEnv createQuESTEnv(void) {
+    seedQuESTDefault();
+    QuESTEnv env;
+    env.value = new QuESTEnvValue();
+    env.rank = 0;
+    int dev = 0;
+    if (!cudaOk(cudaGetDevice(&dev), __func__)) return env;
+    env.value->device = dev;
+    return env;
+}
+
+void destroyQuESTEnv(QuESTEnv env) { delete env.value; }
+
+int getQuEST_PREC(void) { return (int) (sizeof(qreal) / 4); }
+
+// ---------------------------------------------------------------- registers
+Qureg createQureg(int numQubits, QuESTEnv env) {
+    Qureg q;
+    std::memset(&q, 0, sizeof(q));
+    if (numQubits <= 0) {
+        raise(E_INVALID_NUM_QUBITS, __func__);
+        return q;
+    }
+    if (numQubits > dgq::kMaxStateBits - 2) {
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, __func__);
+        return q;
+    }
+    auto *s = new QuregState();
+    s->numQubits = numQubits;
+    s->numBits = std::max(numQubits, dgq::kMinTileBits);
+    resetMapping(*s);
+    const size_t bytes = sizeof(double2) << s->numBits;
+    size_t freeB = 0, totalB = 0;
+    if (!cudaOk(cudaMemGetInfo(&freeB, &totalB), __func__)) {
+        delete s;
+        return q;
+    }
+    if (bytes + (64u << 20) > freeB) {
+        delete s;
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, __func__);
+        return q;
+    }
+    if (!cudaOk(cudaMalloc(&s->dState, bytes), __func__) ||
+        !cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), __func__) ||
+        !cudaOk(cudaMalloc(&s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1)), __func__)) {
+        if (s->dState) cudaFree(s->dState);
+        delete s;
+        return q;
+    }
+    q.isDensityMatrix = 0;
+    q.numQubitsRepresented = (u64) numQubits;
+    q.numQubitsInStateVec = (u64) numQubits;
+    q.numAmpsTotal = 1ULL << numQubits;
+    q.env = env;
+    q.state = s;
+    initZeroState(q);
+    return q;
+}
+
+void searchQuregTaskPartitions(Qureg qureg, QuESTEnv env) {
+    (void) env;
+    if (!vQureg(qureg, __func__)) return;
+    // dgQuEST picks its partition K here (QuEST_backend_distributed.cpp:86-121);
+    // the recast picks the tile width for the gates recorded so far.
+    QuregState &s = *stateOf(qureg);
+    if (s.tileBitsSetting == 0 && !s.pending.empty()) s.tileBitsSetting = chooseTileBits(s);
+}
+
+void destroyQureg(Qureg qureg, QuESTEnv env) {
+    (void) env;
+    QuregState *s = qureg.state;
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->dState) cudaFree(s->dState);
+    if (s->dPartial) cudaFree(s->dPartial);
+    if (s->dProbOut) cudaFree(s->dProbOut);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int getNumQubits(Qureg qureg) { return (int) qureg.numQubitsRepresented; }
+int getNumAmps(Qureg qureg) { return (int) qureg.numAmpsTotal; }
+
+// ---------------------------------------------------------------- init
+static void setInit(Qureg q, int32_t kind, uint64_t index, double amp) {
+    QuregState &s = *stateOf(q);
+    s.pending.clear();
+    s.pool.mats.clear();
+    resetMapping(s);
+    s.restrictActive = false;
+    s.rMask = s.rValue = 0;
+    s.rScale = 1.0;
+    s.initPending = true;
+    s.initKind = kind;
+    s.initIndex = index;
+    s.initAmp = amp;
+    s.probsValid = false;
+}
+
+void initZeroState(Qureg qureg) {
+    if (!vQureg(qureg, __func__)) return;
+    setInit(qureg, dgq::INIT_CLASSICAL, 0, 0.0);
+}
+
+void initPlusState(Qureg qureg) {
+    if (!vQureg(qureg, __func__)) return;
+    setInit(qureg, dgq::INIT_PLUS, 0, 1.0 / std::sqrt((double) (1LL << qureg.numQubitsRepresented)));
+}
+
+void initClassicalState(Qureg qureg, long long int stateInd) {
+    if (!vStateIndex(qureg, stateInd, __func__)) return;
+    setInit(qureg, dgq::INIT_CLASSICAL, (uint64_t) stateInd, 0.0);
+}
+
+void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
+    if (!vQureg(qureg, __func__)) return;
+    if (!reals || !imags) {
+        raise(E_INVALID_ARGUMENT, __func__, "null amplitude array");
+        return;
+    }
+    QuregState &s = *stateOf(qureg);
+    s.pending.clear();
+    s.pool.mats.clear();
+    s.initPending = false;
+    resetMapping(s);
+    s.restrictActive = false;
+    s.rMask = s.rValue = 0;
+    s.rScale = 1.0;
+    s.probsValid = false;
+    const uint64_t n = 1ULL << s.numQubits;
+    const uint64_t total = 1ULL << s.numBits;
+    // stage re and im in chunks, interleave on the GPU
+    const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 24);
+    double *dRe = nullptr, *dIm = nullptr;
+    if (!cudaOk(cudaMalloc(&dRe, chunk * sizeof(double)), __func__)) return;
+    if (!cudaOk(cudaMalloc(&dIm, chunk * sizeof(double)), __func__)) {
+        cudaFree(dRe);
+        return;
+    }
+    if (total > n) {
+        cudaOk(cudaMemsetAsync(s.dState + n, 0, (total - n) * sizeof(double2), s.stream), __func__);
+    }
+    for (uint64_t off = 0; off < n; off += chunk) {
+        const uint64_t c = std::min(chunk, n - off);
+        cudaOk(cudaMemcpyAsync(dRe, reals + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
+        cudaOk(cudaMemcpyAsync(dIm, imags + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
+        cudaOk(dgq::launchInterleave(dRe, dIm, c, c, s.dState + off, s.stream), __func__);
+        g_launches++;
+    }
+    cudaOk(cudaStreamSynchronize(s.stream), __func__);
+    cudaFree(dRe);
+    cudaFree(dIm);
+}
+
+// ---------------------------------------------------------------- gates
+// Encodings: src/cpp/QuEST_distributed.cpp:118-364 (rotations store angle/2).
+void hadamard(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_HADAMARD, bit(t), 0, nullptr, 0);
+}
+void pauliX(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_PAULI_X, bit(t), 0, nullptr, 0);
+}
+void pauliY(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_PAULI_Y, bit(t), 0, nullptr, 0);
+}
+void pauliZ(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_PAULI_Z, 0, bit(t), nullptr, 0);
+}
+void sGate(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_S_GATE, 0, bit(t), nullptr, 0);
+}
+void tGate(Qureg q, const int t) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_T_GATE, 0, bit(t), nullptr, 0);
+}
+void phaseShift(Qureg q, const int t, qreal angle) {
+    if (!vTarget(q, t, __func__)) return;
+    record(q, dgq::OP_PHASE_SHIFT, 0, bit(t), &angle, 1);
+}
+void rotateX(Qureg q, const int t, qreal angle) {
+    if (!vTarget(q, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_X, bit(t), 0, &a, 1);
+}
+void rotateY(Qureg q, const int t, qreal angle) {
+    if (!vTarget(q, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_Y, bit(t), 0, &a, 1);
+}
+void rotateZ(Qureg q, const int t, qreal angle) {
+    if (!vTarget(q, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_Z, bit(t), 0, &a, 1);
+}
+void controlledRotateX(Qureg q, const int c, const int t, qreal angle) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_X, bit(t), bit(c), &a, 1);
+}
+void controlledRotateY(Qureg q, const int c, const int t, qreal angle) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_Y, bit(t), bit(c), &a, 1);
+}
+void controlledRotateZ(Qureg q, const int c, const int t, qreal angle) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    const double a = angle * 0.5;
+    record(q, dgq::OP_ROTATE_Z, bit(t), bit(c), &a, 1);
+}
+// src/QuEST_common.c:56-63 and :154-183
+static void pairFromRotation(qreal angle, Vector axis, Complex *alpha, Complex *beta) {
+    const double mag = std::sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    const double ux = axis.x / mag, uy = axis.y / mag, uz = axis.z / mag;
+    alpha->real = std::cos(angle / 2.0);
+    alpha->imag = -std::sin(angle / 2.0) * uz;
+    beta->real = std::sin(angle / 2.0) * uy;
+    beta->imag = -std::sin(angle / 2.0) * ux;
+}
+void rotateAroundAxis(Qureg q, const int t, qreal angle, Vector axis) {
+    if (!vTarget(q, t, __func__)) return;
+    if (axis.x == 0 && axis.y == 0 && axis.z == 0) {
+        raise(E_ZERO_VECTOR, __func__);
+        return;
+    }
+    Complex a, b;
+    pairFromRotation(angle, axis, &a, &b);
+    const double op[4] = {a.real, a.imag, b.real, b.imag};
+    record(q, dgq::OP_COMPACT_UNITARY, bit(t), 0, op, 4);
+}
+void controlledRotateAroundAxis(Qureg q, const int c, const int t, qreal angle, Vector axis) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    if (axis.x == 0 && axis.y == 0 && axis.z == 0) {
+        raise(E_ZERO_VECTOR, __func__);
+        return;
+    }
+    Complex a, b;
+    pairFromRotation(angle, axis, &a, &b);
+    const double op[4] = {a.real, a.imag, b.real, b.imag};
+    record(q, dgq::OP_COMPACT_UNITARY, bit(t), bit(c), op, 4);
+}
+void compactUnitary(Qureg q, const int t, Complex alpha, Complex beta) {
+    if (!vTarget(q, t, __func__)) return;
+    if (!isPairUnitary(alpha, beta)) {
+        raise(E_NON_UNITARY_COMPLEX_PAIR, __func__);
+        return;
+    }
+    const double op[4] = {alpha.real, alpha.imag, beta.real, beta.imag};
+    record(q, dgq::OP_COMPACT_UNITARY, bit(t), 0, op, 4);
+}
+void controlledCompactUnitary(Qureg q, const int c, const int t, Complex alpha, Complex beta) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    if (!isPairUnitary(alpha, beta)) {
+        raise(E_NON_UNITARY_COMPLEX_PAIR, __func__);
+        return;
+    }
+    const double op[4] = {alpha.real, alpha.imag, beta.real, beta.imag};
+    record(q, dgq::OP_COMPACT_UNITARY, bit(t), bit(c), op, 4);
+}
+void unitary(Qureg q, const int t, ComplexMatrix2 u) {
+    if (!vTarget(q, t, __func__)) return;
+    if (!isMatrix2Unitary(u)) {
+        raise(E_NON_UNITARY_MATRIX, __func__);
+        return;
+    }
+    recordMatrix(q, bit(t), 0, u);
+}
+void controlledUnitary(Qureg q, const int c, const int t, ComplexMatrix2 u) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    if (!isMatrix2Unitary(u)) {
+        raise(E_NON_UNITARY_MATRIX, __func__);
+        return;
+    }
+    recordMatrix(q, bit(t), bit(c), u);
+}
+void multiControlledUnitary(Qureg q, int *cs, const int nc, const int t, ComplexMatrix2 u) {
+    if (!vTarget(q, t, __func__) || !vMultiControls(q, cs, nc, __func__)) return;
+    u64 cm = 0;
+    for (int i = 0; i < nc; i++) {
+        if (cs[i] == t) {
+            raise(E_TARGET_IN_CONTROLS, __func__);
+            return;
+        }
+        cm |= bit(cs[i]);
+    }
+    if (!isMatrix2Unitary(u)) {
+        raise(E_NON_UNITARY_MATRIX, __func__);
+        return;
+    }
+    recordMatrix(q, bit(t), cm, u);
+}
+void controlledNot(Qureg q, const int c, const int t) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    record(q, dgq::OP_PAULI_X, bit(t), bit(c), nullptr, 0);
+}
+void controlledPauliY(Qureg q, const int c, const int t) {
+    if (!vControlTarget(q, c, t, __func__)) return;
+    record(q, dgq::OP_PAULI_Y, bit(t), bit(c), nullptr, 0);
+}
+void controlledPhaseFlip(Qureg q, const int a, const int b) {
+    if (!vControlTarget(q, a, b, __func__)) return;
+    record(q, dgq::OP_PAULI_Z, 0, bit(a) | bit(b), nullptr, 0);
+}
+void multiControlledPhaseFlip(Qureg q, int *cs, int nc) {
+    if (!vMultiControls(q, cs, nc, __func__)) return;
+    u64 cm = 0;
+    for (int i = 0; i < nc; i++) cm |= bit(cs[i]);
+    record(q, dgq::OP_PAULI_Z, 0, cm, nullptr, 0);
+}
+void controlledPhaseShift(Qureg q, const int a, const int b, qreal angle) {
+    if (!vControlTarget(q, a, b, __func__)) return;
+    record(q, dgq::OP_PHASE_SHIFT, 0, bit(a) | bit(b), &angle, 1);
+}
+void multiControlledPhaseShift(Qureg q, int *cs, int nc, qreal angle) {
+    if (!vMultiControls(q, cs, nc, __func__)) return;
+    u64 cm = 0;
+    for (int i = 0; i < nc; i++) cm |= bit(cs[i]);
+    record(q, dgq::OP_PHASE_SHIFT, 0, cm, &angle, 1);
+}
+void swapGate(Qureg q, int a, int b) {
+    if (!vUniqueTargets(q, a, b, __func__)) return;
+    // relabel logical qubits instead of moving amplitudes: later gates and
+    // read-outs translate through l2v
+    QuregState &s = *stateOf(q);
+    std::swap(s.l2v[a], s.l2v[b]);
+    s.v2l[s.l2v[a]] = a;
+    s.v2l[s.l2v[b]] = b;
+}
+// src/QuEST.c:320-416 (u1/u2/u3 and the square-root gates are 2x2 unitaries)
+void u1Gate(Qureg q, int t, qreal lambda) {
+    ComplexMatrix2 u{{1.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {std::cos(lambda), std::sin(lambda)}};
+    unitary(q, t, u);
+}
+void u2Gate(Qureg q, int t, qreal phi, qreal lambda) {
+    const double r = 1 / std::sqrt(2);
+    ComplexMatrix2 u{{r, 0.0},
+                     {-std::cos(lambda) * r, -std::sin(lambda) * r},
+                     {std::cos(phi) * r, std::sin(phi) * r},
+                     {std::cos(phi + lambda) * r, std::sin(phi + lambda) * r}};
+    unitary(q, t, u);
+}
+void u3Gate(Qureg q, int t, qreal theta, qreal phi, qreal lambda) {
+    const double ct = std::cos(theta / 2), st = std::sin(theta / 2);
+    ComplexMatrix2 u{{ct, 0.0},
+                     {-std::cos(lambda) * st, -std::sin(lambda) * st},
+                     {std::cos(phi) * st, std::sin(phi) * st},
+                     {std::cos(phi + lambda) * ct, std::sin(phi + lambda) * ct}};
+    unitary(q, t, u);
+}
+void SqX(Qureg q, int t) {
+    const double r = 1 / std::sqrt(2);
+    ComplexMatrix2 u{{r, 0.0}, {0.0, -r}, {0.0, -r}, {r, 0.0}};
+    unitary(q, t, u);
+}
+void SqY(Qureg q, int t) {
+    const double r = 1 / std::sqrt(2);
+    ComplexMatrix2 u{{r, 0.0}, {-r, 0.0}, {r, 0.0}, {r, 0.0}};
+    unitary(q, t, u);
+}
+void SqW(Qureg q, int t) {
+    const double r = 1 / std::sqrt(2);
+    ComplexMatrix2 u{{r, 0.0}, {-0.5, -0.5}, {0.5, -0.5}, {r, 0.0}};
+    unitary(q, t, u);
+}
+void fSim(Qureg q, int t1, int t2, qreal theta, qreal phi) {
+    controlledPhaseShift(q, t1, t2, -phi);
+    controlledNot(q, t1, t2);
+    controlledRotateX(q, t2, t1, theta * 2);
+    controlledNot(q, t1, t2);
+}
+
+ComplexMatrixN createComplexMatrixN(int numQubits) {
+    ComplexMatrixN m;
+    m.numQubits = numQubits;
+    m.real = nullptr;
+    m.imag = nullptr;
+    if (numQubits < 1 || numQubits > 12) {
+        raise(E_INVALID_NUM_TARGETS, __func__);
+        return m;
+    }
+    const int d = 1 << numQubits;
+    m.real = (qreal **) malloc(sizeof(qreal *) * (size_t) d);
+    m.imag = (qreal **) malloc(sizeof(qreal *) * (size_t) d);
+    for (int r = 0; r < d; r++) {
+        m.real[r] = (qreal *) calloc((size_t) d, sizeof(qreal));
+        m.imag[r] = (qreal *) calloc((size_t) d, sizeof(qreal));
+    }
+    return m;
+}
+
+void destroyComplexMatrixN(ComplexMatrixN m) {
+    if (!m.real) return;
+    const int d = 1 << m.numQubits;
+    for (int r = 0; r < d; r++) {
+        free(m.real[r]);
+        free(m.imag[r]);
+    }
+    free(m.real);
+    free(m.imag);
+}
+
+void multiQubitUnitary(Qureg q, int *targs, int numTargs, ComplexMatrixN u) {
+    if (!vQureg(q, __func__)) return;
+    if (!targs || numTargs < 1 || numTargs > (int) q.numQubitsRepresented || u.numQubits != numTargs || !u.real ||
+        !u.imag) {
+        raise(E_INVALID_NUM_TARGETS, __func__);
+        return;
+    }
+    u64 tm = 0;
+    for (int i = 0; i < numTargs; i++) {
+        if (targs[i] < 0 || targs[i] >= (int) q.numQubitsRepresented) {
+            raise(E_INVALID_TARGET_QUBIT, __func__);
+            return;
+        }
+        if (tm & bit(targs[i])) {
+            raise(E_INVALID_NUM_TARGETS, __func__);
+            return;
+        }
+        tm |= bit(targs[i]);
+    }
+    const int d = 1 << numTargs;
+    // unitarity: U^dagger U = 1 within the tolerance QuEST uses for 2x2
+    for (int r = 0; r < d; r++) {
+        for (int c = 0; c < d; c++) {
+            double re = 0.0, im = 0.0;
+            for (int k = 0; k < d; k++) {
+                re += u.real[k][r] * u.real[k][c] + u.imag[k][r] * u.imag[k][c];
+                im += u.real[k][r] * u.imag[k][c] - u.imag[k][r] * u.real[k][c];
+            }
+            if (std::fabs(re - (r == c ? 1.0 : 0.0)) > 1e3 * REAL_EPS || std::fabs(im) > 1e3 * REAL_EPS) {
+                raise(E_NON_UNITARY_MATRIX, __func__);
+                return;
+            }
+        }
+    }
+    if (numTargs == 1) {
+        ComplexMatrix2 m2{{u.real[0][0], u.imag[0][0]},
+                          {u.real[0][1], u.imag[0][1]},
+                          {u.real[1][0], u.imag[1][0]},
+                          {u.real[1][1], u.imag[1][1]}};
+        recordMatrix(q, tm, 0, m2);
+        return;
+    }
+    if (numTargs > dgq::kRegBits) {
+        raise(E_UNSUPPORTED, __func__, "multiQubitUnitary supports at most 4 targets in the FP64 tile path");
+        return;
+    }
+    QuregState &s = *stateOf(q);
+    std::vector<double> m((size_t) 2 * d * d);
+    for (int r = 0; r < d; r++)
+        for (int c = 0; c < d; c++) {
+            m[(size_t) 2 * (r * d + c)] = u.real[r][c];
+            m[(size_t) 2 * (r * d + c) + 1] = u.imag[r][c];
+        }
+    Gate g;
+    g.type = dgq::OP_MULTI_UNITARY;
+    g.targetMask = toVirtualMask(s, tm);
+    g.controlMask = 0;
+    g.numMultiTargets = numTargs;
+    for (int i = 0; i < numTargs; i++) g.multiTargets[i] = s.l2v[targs[i]];
+    g.multiIndex = (int32_t) s.pool.mats.size();
+    s.pool.mats.push_back(std::move(m));
+    s.pending.push_back(g);
+    s.probsValid = false;
+}
+
+// ---------------------------------------------------------------- read-outs
+Complex getAmp(Qureg q, long long int index) {
+    Complex out{0.0, 0.0};
+    if (!vStateIndex(q, index, __func__)) return out;
+    QuregState &s = *stateOf(q);
+    if (!flush(s, __func__)) return out;
+    const uint64_t v = toVirtualIndex(s, (uint64_t) index);
+    if (s.restrictActive && (v & s.rMask) != s.rValue) {
+        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+        return out;
+    }
+    double2 a;
+    if (!cudaOk(cudaMemcpyAsync(&a, s.dState + v, sizeof(a), cudaMemcpyDeviceToHost, s.stream), __func__)) return out;
+    if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+    const double sc = s.restrictActive ? s.rScale : 1.0;
+    out.real = a.x * sc;
+    out.imag = a.y * sc;
+    return out;
+}
+qreal getRealAmp(Qureg q, long long int index) { return getAmp(q, index).real; }
+qreal getImagAmp(Qureg q, long long int index) { return getAmp(q, index).imag; }
+qreal getProbAmp(Qureg q, long long int index) {
+    const Complex a = getAmp(q, index);
+    return a.real * a.real + a.imag * a.imag;
+}
+
+qreal calcProbOfOutcome(Qureg q, const int measureQubit, int outcome) {
+    if (!vTarget(q, measureQubit, __func__) || !vOutcome(outcome, __func__)) return 0.0;
+    QuregState &s = *stateOf(q);
+    if (!ensureProbs(s, __func__)) return 0.0;
+    const double p0 = s.p0[(size_t) s.l2v[measureQubit]];
+    return outcome == 1 ? 1.0 - p0 : p0;
+}
+
+qreal calcTotalProb(Qureg q) {
+    if (!vQureg(q, __func__)) return 0.0;
+    QuregState &s = *stateOf(q);
+    if (!ensureProbs(s, __func__)) return 0.0;
+    return s.totalProb;
+}
+
+static void applyCollapse(QuregState &s, int v, int outcome, double prob) {
+    if ((s.rMask >> v) & 1ULL) return;  // already fixed by an earlier collapse
+    s.rMask |= 1ULL << v;
+    if (outcome) s.rValue |= 1ULL << v;
+    s.rScale /= std::sqrt(prob);
+    s.restrictActive = true;
+    s.probsValid = false;
+}
+
+qreal collapseToOutcome(Qureg q, const int measureQubit, int outcome) {
+    if (!vTarget(q, measureQubit, __func__) || !vOutcome(outcome, __func__)) return 0.0;
+    QuregState &s = *stateOf(q);
+    if (!ensureProbs(s, __func__)) return 0.0;
+    const int v = s.l2v[measureQubit];
+    const double p0 = s.p0[(size_t) v];
+    const double prob = outcome == 1 ? 1.0 - p0 : p0;
+    if (prob < REAL_EPS) {
+        raise(E_COLLAPSE_STATE_ZERO_PROB, __func__);
+        return 0.0;
+    }
+    applyCollapse(s, v, outcome, prob);
+    return prob;
+}
+
+// src/QuEST_common.c:97-115 (outcome rule) with QuEST's collapse semantics
+int measureWithStats(Qureg q, int measureQubit, qreal *outcomeProb) {
+    if (!vTarget(q, measureQubit, __func__)) return 0;
+    QuregState &s = *stateOf(q);
+    if (!ensureProbs(s, __func__)) return 0;
+    const int v = s.l2v[measureQubit];
+    const double zeroProb = s.p0[(size_t) v];
+    int outcome;
+    if (zeroProb < REAL_EPS)
+        outcome = 1;
+    else if (1 - zeroProb < REAL_EPS)
+        outcome = 0;
+    else
+        outcome = (g_rng.real1() > zeroProb);
+    const double prob = outcome == 0 ? zeroProb : 1 - zeroProb;
+    if (outcomeProb) *outcomeProb = prob;
+    applyCollapse(s, v, outcome, prob);
+    return outcome;
+}
+
+int measure(Qureg q, int measureQubit) { return measureWithStats(q, measureQubit, nullptr); }
+
+// ---------------------------------------------------------------- extensions
+int dgq_setTileBits(Qureg q, int tileBits) {
+    if (!vQureg(q, __func__)) return -1;
+    QuregState &s = *stateOf(q);
+    const int prev = s.tileBitsSetting;
+    if (tileBits != 0 && (tileBits < dgq::kMinTileBits || tileBits > dgq::kMaxTileBits)) {
+        raise(E_INVALID_ARGUMENT, __func__, "tile bits must be 0 or in [9, 13]");
+        return prev;
+    }
+    s.tileBitsSetting = tileBits;
+    return prev;
+}
+
+int dgq_getPlanStats(Qureg q, dgq_plan_stats *out) {
+    if (!vQureg(q, __func__) || !out) return -1;
+    *out = stateOf(q)->stats;
+    return 0;
+}
+
+int dgq_planPending(Qureg q) {
+    if (!vQureg(q, __func__)) return -1;
+    return planPending(*stateOf(q), __func__) ? 0 : -1;
+}
+
+int dgq_launchPlanned(Qureg q) {
+    if (!vQureg(q, __func__)) return -1;
+    QuregState &s = *stateOf(q);
+    if (!launchPlanned(s, __func__)) return -1;
+    s.probsValid = false;
+    return 0;
+}
+
+int dgq_sync(Qureg q) {
+    if (!vQureg(q, __func__)) return -1;
+    QuregState &s = *stateOf(q);
+    if (!flush(s, __func__)) return -1;
+    return cudaOk(cudaStreamSynchronize(s.stream), __func__) ? 0 : -1;
+}
+
+void *dgq_getStream(Qureg q) {
+    if (!vQureg(q, __func__)) return nullptr;
+    return (void *) stateOf(q)->stream;
+}
+
+void *dgq_getDeviceState(Qureg q, int *numBits) {
+    if (!vQureg(q, __func__)) return nullptr;
+    if (numBits) *numBits = stateOf(q)->numBits;
+    return (void *) stateOf(q)->dState;
+}
+
+int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
+    if (!vQureg(q, __func__) || !re || !im) return -1;
+    QuregState &s = *stateOf(q);
+    if (!flush(s, __func__)) return -1;
+    const uint64_t n = 1ULL << s.numQubits;
+    const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 22);
+    double2 *dOut = nullptr;
+    if (!cudaOk(cudaMalloc(&dOut, chunk * sizeof(double2)), __func__)) return -1;
+    std::vector<double2> host((size_t) chunk);
+    dgq::GatherArgs ga;
+    std::memset(&ga, 0, sizeof(ga));
+    ga.numReal = s.numQubits;
+    ga.hasRestrict = s.restrictActive ? 1 : 0;
+    ga.restrictMask = s.rMask;
+    ga.restrictValue = s.rValue;
+    ga.restrictScale = s.rScale;
+    for (int b = 0; b < s.numQubits; b++) ga.l2v[b] = (uint8_t) s.l2v[b];
+    bool ok = true;
+    for (uint64_t off = 0; off < n && ok; off += chunk) {
+        ga.begin = off;
+        ga.count = std::min(chunk, n - off);
+        ok = cudaOk(dgq::launchGather(s.dState, ga, dOut, s.stream), __func__) &&
+             cudaOk(cudaMemcpyAsync(host.data(), dOut, ga.count * sizeof(double2), cudaMemcpyDeviceToHost, s.stream),
+                    __func__) &&
+             cudaOk(cudaStreamSynchronize(s.stream), __func__);
+        g_launches++;
+        for (uint64_t i = 0; ok && i < ga.count; i++) {
+            re[off + i] = host[(size_t) i].x;
+            im[off + i] = host[(size_t) i].y;
+        }
+    }
+    cudaFree(dOut);
+    return ok ? 0 : -1;
+}
+
+int dgq_calcProbOfAllZero(Qureg q, qreal *probs) {
+    if (!vQureg(q, __func__) || !probs) return -1;
+    QuregState &s = *stateOf(q);
+    if (!ensureProbs(s, __func__)) return -1;
+    for (int i = 0; i < s.numQubits; i++) probs[i] = s.p0[(size_t) s.l2v[i]];
+    return 0;
+}
+
+int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
+                  const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
+                  int32_t *numMerged) {
+    if (numQubits < 1 || numQubits > dgq::kMaxStateBits - 2 || count < 0 || (count > 0 && (!types || !targetMasks ||
+        !controlMasks || !operands)) || !out) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
+    }
+    QuregState s;
+    s.numQubits = numQubits;
+    s.numBits = std::max(numQubits, dgq::kMinTileBits);
+    resetMapping(s);
+    s.tileBitsSetting = tileBits;
+    for (int i = 0; i < count; i++) {
+        Gate g;
+        g.type = (dgq::GateType) types[i];
+        g.targetMask = targetMasks[i];
+        g.controlMask = controlMasks[i];
+        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
+        s.pending.push_back(g);
+    }
+    if (mergedTypes || numMerged) {
+        dgq::GateDag dag(s.numBits, true);
+        for (const Gate &g : s.pending) dag.add(g);
+        const std::vector<Gate> merged = dag.gatesInOrder();
+        if (numMerged) *numMerged = (int32_t) merged.size();
+        if (mergedTypes)
+            for (size_t i = 0; i < merged.size(); i++) mergedTypes[i] = (int32_t) merged[i].type;
+    }
+    s.initPending = true;
+    s.initKind = dgq::INIT_CLASSICAL;
+    if (!planPending(s, __func__)) return -1;
+    *out = s.stats;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,499 @@
+// kernels.cu -- the sm_100a kernels of the FP64 state-vector path.
+//
+//   tileKernel<W>    one sweep of the state applying a fused block
+//                    (dgQuEST statevec_fusedKernel, QuEST_gpu_kernel.cu:175-359)
+//   probKernel       P(bit = 0) for every address bit in one read pass
+//   probFinalize     (statevec_findProbabilityOfZeroKernel + reducePingpong,
+//                    QuEST_gpu_kernel.cu:656-840)
+//   swapBitsKernel   in-HBM exchange of address-bit pairs (the successor of
+//                    reorder_data_kernel, QuEST_gpu_kernel.cu:589-654)
+//   gatherKernel     logical-order copy-out of the state through the
+//                    logical->virtual map
+//
+// The state is 2^numBits double2 (re, im) amplitudes in HBM, in place.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+#include "tile_program.h"
+
+namespace dgq {
+
+__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u); }
+
+// ------------------------------------------------------------------ ops
+template <int K, class F>
+__device__ __forceinline__ void forPairs(double2 (&a)[kRegs], uint32_t ctrlReg, F f) {
+#pragma unroll
+    for (int p = 0; p < kRegs / 2; p++) {
+        const int j0 = ((p >> K) << (K + 1)) | (p & ((1 << K) - 1));
+        const int j1 = j0 | (1 << K);
+        if ((j0 & ctrlReg) == ctrlReg) f(a[j0], a[j1]);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void forAll(double2 (&a)[kRegs], uint32_t ctrlReg, F f) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        if ((j & ctrlReg) == ctrlReg) f(a[j], j);
+    }
+}
+
+#define DGQ_DISPATCH_K(kval, ...)       \
+    switch (kval) {                     \
+        case 0: {                       \
+            constexpr int K = 0;        \
+            __VA_ARGS__;                \
+        } break;                        \
+        case 1: {                       \
+            constexpr int K = 1;        \
+            __VA_ARGS__;                \
+        } break;                        \
+        case 2: {                       \
+            constexpr int K = 2;        \
+            __VA_ARGS__;                \
+        } break;                        \
+        default: {                      \
+            constexpr int K = 3;        \
+            __VA_ARGS__;                \
+        } break;                        \
+    }
+
+template <int KK>
+__device__ __forceinline__ void denseApply(double2 (&a)[kRegs], uint32_t ctrlReg, const double *m) {
+    constexpr int D = 1 << KK;
+#pragma unroll
+    for (int g = 0; g < (kRegs >> KK); g++) {
+        const int base = g << KK;
+        if ((base & ctrlReg) != ctrlReg) continue;
+        double2 v[D];
+#pragma unroll
+        for (int c = 0; c < D; c++) v[c] = a[base + c];
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+            double re = 0.0, im = 0.0;
+#pragma unroll
+            for (int c = 0; c < D; c++) {
+                const double mr = m[2 * (r * D + c)], mi = m[2 * (r * D + c) + 1];
+                re = fma(mr, v[c].x, re);
+                re = fma(-mi, v[c].y, re);
+                im = fma(mr, v[c].y, im);
+                im = fma(mi, v[c].x, im);
+            }
+            a[base + r] = make_double2(re, im);
+        }
+    }
+}
+
+__device__ __forceinline__ void applyOp(const KOp &op, const double *coef, double2 (&a)[kRegs], uint32_t loc,
+                                        uint32_t cta) {
+    if ((cta & op.ctrlCta) != op.ctrlCta || (loc & op.ctrlLoc) != op.ctrlLoc) return;
+    const uint32_t cr = op.ctrlReg;
+    const double *c = coef + op.coef;
+    switch (op.kind) {
+        case KOP_M2R: {
+            const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 nx = make_double2(m0 * x.x + m1 * y.x, m0 * x.y + m1 * y.y);
+                const double2 ny = make_double2(m2 * x.x + m3 * y.x, m2 * x.y + m3 * y.y);
+                x = nx;
+                y = ny;
+            }));
+            break;
+        }
+        case KOP_M2I: {
+            // [[a, i b], [i c, d]]
+            const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 nx = make_double2(m0 * x.x - m1 * y.y, m0 * x.y + m1 * y.x);
+                const double2 ny = make_double2(m3 * y.x - m2 * x.y, m3 * y.y + m2 * x.x);
+                x = nx;
+                y = ny;
+            }));
+            break;
+        }
+        case KOP_M2C: {
+            const double u0 = c[0], u1 = c[1], u2 = c[2], u3 = c[3], u4 = c[4], u5 = c[5], u6 = c[6], u7 = c[7];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 nx = make_double2(u0 * x.x - u1 * x.y + u2 * y.x - u3 * y.y,
+                                                u0 * x.y + u1 * x.x + u2 * y.y + u3 * y.x);
+                const double2 ny = make_double2(u4 * x.x - u5 * x.y + u6 * y.x - u7 * y.y,
+                                                u4 * x.y + u5 * x.x + u6 * y.y + u7 * y.x);
+                x = nx;
+                y = ny;
+            }));
+            break;
+        }
+        case KOP_X:
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 t = x;
+                x = y;
+                y = t;
+            }));
+            break;
+        case KOP_Y:
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 t = x;
+                x = make_double2(y.y, -y.x);
+                y = make_double2(-t.y, t.x);
+            }));
+            break;
+        case KOP_YC:
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
+                const double2 t = x;
+                x = make_double2(-y.y, y.x);
+                y = make_double2(t.y, -t.x);
+            }));
+            break;
+        case KOP_NEG:
+            forAll(a, cr, [&](double2 &x, int) { x = make_double2(-x.x, -x.y); });
+            break;
+        case KOP_MULI:
+            forAll(a, cr, [&](double2 &x, int) { x = make_double2(-x.y, x.x); });
+            break;
+        case KOP_MULNI:
+            forAll(a, cr, [&](double2 &x, int) { x = make_double2(x.y, -x.x); });
+            break;
+        case KOP_PH: {
+            const double cs = c[0], sn = c[1];
+            forAll(a, cr, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
+            break;
+        }
+        case KOP_Z2: {
+            const double cs = c[0], sn = c[1];
+            const uint32_t sr = op.selReg;
+            const bool thrBit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
+            forAll(a, cr, [&](double2 &x, int j) {
+                const bool bit = sr ? ((j & sr) != 0u) : thrBit;
+                const double s = bit ? sn : -sn;
+                x = make_double2(cs * x.x - s * x.y, cs * x.y + s * x.x);
+            });
+            break;
+        }
+        case KOP_DENSE:
+            switch (op.k) {
+                case 1: denseApply<1>(a, cr, c); break;
+                case 2: denseApply<2>(a, cr, c); break;
+                case 3: denseApply<3>(a, cr, c); break;
+                default: denseApply<4>(a, cr, c); break;
+            }
+            break;
+        default:
+            break;
+    }
+}
+
+// ------------------------------------------------------------ tile kernel
+// 128 registers per thread: 16 warps per SM at every tile width.
+template <int W>
+__global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kRegBits)))
+    tileKernel(double2 *__restrict__ st, const __grid_constant__ TileProgram prog) {
+    constexpr int T = 1 << (W - kRegBits);
+    extern __shared__ double2 sm[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t cta = blockIdx.x;
+
+    // address of canonical element (tid, j): base | lane bits | thread high bits | j bits
+    uint64_t tpart = tid & 31u;
+    const int nCta = prog.numBits - W;
+    for (int i = 0; i < nCta; i++) tpart |= (uint64_t) ((cta >> i) & 1u) << prog.ctaPos[i];
+#pragma unroll
+    for (int i = 0; i < W - 9; i++) tpart |= (uint64_t) ((tid >> (5 + i)) & 1u) << prog.highPos[i];
+    const uint64_t jb0 = 1ULL << prog.highPos[W - 9];
+    const uint64_t jb1 = 1ULL << prog.highPos[W - 8];
+    const uint64_t jb2 = 1ULL << prog.highPos[W - 7];
+    const uint64_t jb3 = 1ULL << prog.highPos[W - 6];
+    auto gidx = [&](int j) -> uint64_t {
+        return tpart | ((j & 1) ? jb0 : 0ULL) | ((j & 2) ? jb1 : 0ULL) | ((j & 4) ? jb2 : 0ULL) | ((j & 8) ? jb3 : 0ULL);
+    };
+
+    double2 a[kRegs];
+    if (prog.initKind == INIT_NONE) {
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) a[j] = st[gidx(j)];
+    } else {
+        const uint64_t ci = prog.initIndex;
+        const double pa = prog.initAmp;
+        const int kind = prog.initKind;
+        const int nr = prog.numReal;
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) {
+            const uint64_t g = gidx(j);
+            double re = 0.0;
+            if (kind == INIT_CLASSICAL)
+                re = (g == ci) ? 1.0 : 0.0;
+            else if (kind == INIT_PLUS)
+                re = ((g >> nr) == 0ULL) ? pa : 0.0;
+            a[j] = make_double2(re, 0.0);
+        }
+    }
+    if (prog.hasRestrict) {
+        const uint64_t rm = prog.restrictMask, rv = prog.restrictValue;
+        const double sc = prog.restrictScale;
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) {
+            const bool keep = (gidx(j) & rm) == rv;
+            a[j] = keep ? make_double2(a[j].x * sc, a[j].y * sc) : make_double2(0.0, 0.0);
+        }
+    }
+
+    const int numPhases = prog.numPhases;
+    if (numPhases > 0) {
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) sm[swz(tid + (uint32_t) (T * j))] = a[j];
+        __syncthreads();
+        for (int p = 0; p < numPhases; p++) {
+            const KPhase &ph = prog.phases[p];
+            uint32_t loc = 0;
+#pragma unroll
+            for (int i = 0; i < W - kRegBits; i++) loc |= ((tid >> i) & 1u) << ph.thrPos[i];
+            const uint32_t sb = swz(loc);
+#pragma unroll
+            for (int j = 0; j < kRegs; j++) a[j] = sm[sb ^ ph.regOff[j]];
+            const int e = ph.opEnd;
+            for (int o = ph.opBegin; o < e; o++) applyOp(prog.ops[o], prog.coef, a, loc, cta);
+#pragma unroll
+            for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) a[j] = sm[swz(tid + (uint32_t) (T * j))];
+    }
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) st[gidx(j)] = a[j];
+}
+
+template <int W>
+static cudaError_t launchTileW(double2 *st, const TileProgram &prog, cudaStream_t s) {
+    static bool attrSet = false;
+    const size_t smem = sizeof(double2) << W;
+    if (!attrSet) {
+        cudaError_t e = cudaFuncSetAttribute(tileKernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        if (e != cudaSuccess) return e;
+        attrSet = true;
+    }
+    const unsigned grid = 1u << (prog.numBits - W);
+    tileKernel<W><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
+    return cudaGetLastError();
+}
+
+cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s) {
+    switch (tileBits) {
+        case 9: return launchTileW<9>(st, prog, s);
+        case 10: return launchTileW<10>(st, prog, s);
+        case 11: return launchTileW<11>(st, prog, s);
+        case 12: return launchTileW<12>(st, prog, s);
+        case 13: return launchTileW<13>(st, prog, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ------------------------------------------------------- probabilities
+// Sub-index s enumerates the amplitudes allowed by the lazy collapse
+// (address bits outside `restrict` mask): address = rValue | deposit(s).
+// s bits 0..7 = thread, 8..11 = register j, 12..12+kappa-1 = unit within
+// the CTA, the rest = blockIdx. Each CTA writes 17 partial sums:
+// [0..7] zero-sums of the thread bits, [8..11] of the j bits,
+// [12..15] of the unit bits, [16] the CTA total.
+__global__ void __launch_bounds__(256) probKernel(const double2 *__restrict__ st, const __grid_constant__ ProbArgs args, double *partial) {
+    const uint32_t tid = threadIdx.x;
+    const uint32_t cta = blockIdx.x;
+    const int nFree = args.nFree;
+    const int kappa = args.kappa;
+    auto bitOf = [&](int i) -> uint64_t { return i < nFree ? (1ULL << args.freePos[i]) : 0ULL; };
+    uint64_t dTid = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if ((tid >> i) & 1u) dTid |= bitOf(i);
+    uint64_t dCta = 0;
+    for (int i = 0; 12 + kappa + i < nFree; i++)
+        if ((cta >> i) & 1u) dCta |= bitOf(12 + kappa + i);
+    const uint64_t j0 = bitOf(8), j1 = bitOf(9), j2 = bitOf(10), j3 = bitOf(11);
+    const uint64_t limit = nFree >= 63 ? ~0ULL : (1ULL << nFree);
+
+    double tot = 0.0, zj0 = 0.0, zj1 = 0.0, zj2 = 0.0, zj3 = 0.0;
+    double zu[4] = {0.0, 0.0, 0.0, 0.0};
+    const int units = 1 << kappa;
+    for (int u = 0; u < units; u++) {
+        uint64_t dU = 0;
+        for (int b = 0; b < kappa; b++)
+            if ((u >> b) & 1) dU |= bitOf(12 + b);
+        const uint64_t gbase = args.rValue | dCta | dU | dTid;
+        const uint64_t sbase = ((((uint64_t) cta << kappa) | (uint64_t) u) << 12) | tid;
+        double ut = 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const uint64_t s = sbase | ((uint64_t) j << 8);
+            const uint64_t g = gbase | ((j & 1) ? j0 : 0ULL) | ((j & 2) ? j1 : 0ULL) | ((j & 4) ? j2 : 0ULL) | ((j & 8) ? j3 : 0ULL);
+            double p = 0.0;
+            if (s < limit) {
+                const double2 v = st[g];
+                p = v.x * v.x + v.y * v.y;
+            }
+            ut += p;
+            if (!(j & 1)) zj0 += p;
+            if (!(j & 2)) zj1 += p;
+            if (!(j & 4)) zj2 += p;
+            if (!(j & 8)) zj3 += p;
+        }
+        tot += ut;
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            if (b < kappa && !((u >> b) & 1)) zu[b] += ut;
+    }
+    double v[17];
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = ((tid >> i) & 1u) ? 0.0 : tot;
+    v[8] = zj0;
+    v[9] = zj1;
+    v[10] = zj2;
+    v[11] = zj3;
+#pragma unroll
+    for (int b = 0; b < 4; b++) v[12 + b] = zu[b];
+    v[16] = tot;
+    __shared__ double red[8][17];
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int i = 0; i < 17; i++) {
+        double x = v[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp][i] = x;
+    }
+    __syncthreads();
+    if (tid < 17) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; w++) x += red[w][tid];
+        partial[(size_t) cta * 17 + tid] = x;
+    }
+}
+
+// out[b] for sub-index bit b < nFree, out[nFree] = total.
+__global__ void __launch_bounds__(256) probFinalize(const double *__restrict__ partial, int numCtas, int nFree,
+                                                   int kappa, double *out) {
+    const int b = blockIdx.x;  // 0..nFree
+    double x = 0.0;
+    const int local = 12 + kappa;
+    for (int c = threadIdx.x; c < numCtas; c += blockDim.x) {
+        if (b == nFree) {
+            x += partial[(size_t) c * 17 + 16];
+        } else if (b < local) {
+            x += partial[(size_t) c * 17 + b];
+        } else if (!((c >> (b - local)) & 1)) {
+            x += partial[(size_t) c * 17 + 16];
+        }
+    }
+    __shared__ double red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int) (blockDim.x >> 5); w++) t += red[w];
+        out[b] = t;
+    }
+}
+
+cudaError_t launchProb(const double2 *st, const ProbArgs &args, double *partial, double *out, cudaStream_t s) {
+    const int grid = args.nFree > 12 + args.kappa ? (1 << (args.nFree - 12 - args.kappa)) : 1;
+    probKernel<<<grid, 256, 0, s>>>(st, args, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    probFinalize<<<args.nFree + 1, 256, 0, s>>>(partial, grid, args.nFree, args.kappa, out);
+    return cudaGetLastError();
+}
+
+int probNumCtas(const ProbArgs &args) {
+    return args.nFree > 12 + args.kappa ? (1 << (args.nFree - 12 - args.kappa)) : 1;
+}
+
+// --------------------------------------------------- bit-pair exchange
+// For every index whose bits at a[i] read pattern p and at b[i] read q with
+// p > q (as integers over the k pairs), exchange it with the index whose
+// patterns are swapped. Every orbit has length 1 or 2, so this is in place.
+__global__ void swapBitsKernel(double2 *__restrict__ st, const __grid_constant__ SwapArgs args) {
+    const uint64_t numAmps = 1ULL << args.numBits;
+    for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < numAmps;
+         i += (uint64_t) gridDim.x * blockDim.x) {
+        uint32_t p = 0, q = 0;
+        for (int k = 0; k < args.numPairs; k++) {
+            p |= (uint32_t) ((i >> args.a[k]) & 1ULL) << k;
+            q |= (uint32_t) ((i >> args.b[k]) & 1ULL) << k;
+        }
+        if (p <= q) continue;
+        uint64_t j = i;
+        for (int k = 0; k < args.numPairs; k++) {
+            j &= ~((1ULL << args.a[k]) | (1ULL << args.b[k]));
+            j |= (uint64_t) ((q >> k) & 1u) << args.a[k];
+            j |= (uint64_t) ((p >> k) & 1u) << args.b[k];
+        }
+        const double2 x = st[i];
+        const double2 y = st[j];
+        st[i] = y;
+        st[j] = x;
+    }
+}
+
+cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s) {
+    const uint64_t numAmps = 1ULL << args.numBits;
+    uint64_t blocks = (numAmps + 255) / 256;
+    if (blocks > 148ULL * 64) blocks = 148ULL * 64;
+    swapBitsKernel<<<(unsigned) blocks, 256, 0, s>>>(st, args);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ gather
+// out[l] = st[virt(l)] for logical indices l in [begin, begin + count),
+// with virt() the logical->virtual bit map and the lazy collapse applied.
+__global__ void gatherKernel(const double2 *__restrict__ st, const __grid_constant__ GatherArgs args, double2 *__restrict__ out) {
+    for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < args.count;
+         i += (uint64_t) gridDim.x * blockDim.x) {
+        const uint64_t l = args.begin + i;
+        uint64_t v = 0;
+        for (int b = 0; b < args.numReal; b++) v |= ((l >> b) & 1ULL) << args.l2v[b];
+        double2 x = st[v];
+        if (args.hasRestrict) {
+            if ((v & args.restrictMask) != args.restrictValue)
+                x = make_double2(0.0, 0.0);
+            else
+                x = make_double2(x.x * args.restrictScale, x.y * args.restrictScale);
+        }
+        out[i] = x;
+    }
+}
+
+cudaError_t launchGather(const double2 *st, const GatherArgs &args, double2 *out, cudaStream_t s) {
+    uint64_t blocks = (args.count + 255) / 256;
+    if (blocks > 148ULL * 32) blocks = 148ULL * 32;
+    if (blocks == 0) blocks = 1;
+    gatherKernel<<<(unsigned) blocks, 256, 0, s>>>(st, args, out);
+    return cudaGetLastError();
+}
+
+}  // namespace dgq
+
+namespace dgq {
+
+// ------------------------------------------------- amplitude upload
+// out[i] = (re[i], im[i]) for i < count, zero for count <= i < total.
+__global__ void interleaveKernel(const double *__restrict__ re, const double *__restrict__ im, uint64_t count,
+                                 uint64_t total, double2 *__restrict__ out) {
+    for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t) gridDim.x * blockDim.x) {
+        out[i] = i < count ? make_double2(re[i], im[i]) : make_double2(0.0, 0.0);
+    }
+}
+
+cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, double2 *out,
+                             cudaStream_t s) {
+    uint64_t blocks = (total + 255) / 256;
+    if (blocks > 148ULL * 32) blocks = 148ULL * 32;
+    interleaveKernel<<<(unsigned) blocks, 256, 0, s>>>(re, im, count, total, out);
+    return cudaGetLastError();
+}
+
+}  // namespace dgq

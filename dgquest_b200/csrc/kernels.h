@@ -1,0 +1,43 @@
+// kernels.h -- host-side launch interface of kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tile_program.h"
+
+namespace dgq {
+
+struct ProbArgs {
+    int32_t nFree;     // address bits not fixed by the lazy collapse
+    int32_t kappa;     // log2 of 4096-amplitude units per CTA (0..4)
+    uint64_t rValue;   // fixed bits' values
+    uint8_t freePos[kMaxStateBits];  // address bit of sub-index bit i
+};
+
+struct SwapArgs {
+    int32_t numBits;
+    int32_t numPairs;  // exchange bit a[i] with bit b[i]
+    uint8_t a[32];
+    uint8_t b[32];
+};
+
+struct GatherArgs {
+    uint64_t begin, count;
+    int32_t numReal;
+    int32_t hasRestrict;
+    uint64_t restrictMask, restrictValue;
+    double restrictScale;
+    uint8_t l2v[kMaxStateBits];
+};
+
+cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s);
+cudaError_t launchProb(const double2 *st, const ProbArgs &args, double *partial, double *out, cudaStream_t s);
+int probNumCtas(const ProbArgs &args);
+cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s);
+cudaError_t launchGather(const double2 *st, const GatherArgs &args, double2 *out, cudaStream_t s);
+cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, double2 *out,
+                             cudaStream_t s);
+
+}  // namespace dgq

@@ -1,0 +1,386 @@
+// planner.cpp -- see planner.h.
+#include "planner.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "dag.h"
+
+namespace dgq {
+
+static const double kRsqrt2 = 0.7071067811865475244008443621;
+
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits) {
+    std::vector<BlockPlan> blocks;
+    GateDag dag(numBits, true);
+    for (const Gate &g : gates) dag.add(g);
+    const u64 seed = (1ULL << kCoalescedBits) - 1;
+    const u64 all = numBits >= 64 ? ~0ULL : ((1ULL << numBits) - 1);
+    while (!dag.empty()) {
+        BlockPlan b;
+        u64 mask = seed;
+        b.gates = dag.takeBlock(tileBits, mask, 1u << 20);
+        // pad to tileBits with the lowest unused bits from bit 5 upward
+        for (int bit = kCoalescedBits; popcount64(mask) < tileBits && bit < numBits; bit++) mask |= 1ULL << bit;
+        b.tileMask = mask & all;
+        if (b.gates.empty()) {
+            // only a gate wider than the tile is left: not plannable here
+            break;
+        }
+        blocks.push_back(std::move(b));
+    }
+    return blocks;
+}
+
+namespace {
+
+struct TileMap {
+    int local[64];   // address bit -> tile-local bit, -1 if not in tile
+    int ctaIdx[64];  // address bit -> blockIdx bit, -1 if in tile
+    int tilePos[kMaxTileBits];
+};
+
+TileMap makeTileMap(u64 tileMask, int numBits) {
+    TileMap m;
+    int nl = 0, nc = 0;
+    for (int b = 0; b < 64; b++) {
+        m.local[b] = -1;
+        m.ctaIdx[b] = -1;
+    }
+    for (int b = 0; b < numBits; b++) {
+        if ((tileMask >> b) & 1ULL) {
+            m.tilePos[nl] = b;
+            m.local[b] = nl++;
+        } else {
+            m.ctaIdx[b] = nc++;
+        }
+    }
+    return m;
+}
+
+struct Split {
+    uint32_t tileLocal = 0;  // tile-local mask
+    uint32_t cta = 0;        // blockIdx-space mask
+};
+
+Split splitMask(u64 m, const TileMap &tm) {
+    Split s;
+    for (int b = 0; b < 64 && m; b++) {
+        if (!((m >> b) & 1ULL)) continue;
+        m &= ~(1ULL << b);
+        if (tm.local[b] >= 0)
+            s.tileLocal |= 1u << tm.local[b];
+        else
+            s.cta |= 1u << tm.ctaIdx[b];
+    }
+    return s;
+}
+
+struct PhaseLayout {
+    int regPos[kRegBits];
+    int thrPos[kMaxThreadBits];
+    uint32_t regLocalMask = 0;
+};
+
+// Register bits: `front` first (dense-gate target order), then the other
+// targets, then padding from the top tile bit down. Thread bits: three bits
+// of distinct (position mod 3) first, so that each quarter-warp touches 8
+// distinct swizzled bank groups, then the rest in increasing order.
+PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int tileBits) {
+    PhaseLayout L;
+    int nr = 0;
+    uint32_t used = 0;
+    for (int p : front) {
+        L.regPos[nr++] = p;
+        used |= 1u << p;
+    }
+    for (int p = 0; p < tileBits && nr < kRegBits; p++) {
+        if (((targetsLocal >> p) & 1u) && !((used >> p) & 1u)) {
+            L.regPos[nr++] = p;
+            used |= 1u << p;
+        }
+    }
+    for (int p = tileBits - 1; p >= 0 && nr < kRegBits; p--) {
+        if (!((used >> p) & 1u)) {
+            L.regPos[nr++] = p;
+            used |= 1u << p;
+        }
+    }
+    L.regLocalMask = used;
+    std::vector<int> thr;
+    for (int p = 0; p < tileBits; p++)
+        if (!((used >> p) & 1u)) thr.push_back(p);
+    std::vector<int> lanes, rest;
+    int classes = 0;
+    for (int p : thr) {
+        if ((int) lanes.size() < 3 && !((classes >> (p % 3)) & 1)) {
+            lanes.push_back(p);
+            classes |= 1 << (p % 3);
+        } else {
+            rest.push_back(p);
+        }
+    }
+    int i = 0;
+    for (int p : lanes) L.thrPos[i++] = p;
+    for (int p : rest) L.thrPos[i++] = p;
+    return L;
+}
+
+uint8_t regSpace(uint32_t tileLocal, const PhaseLayout &L) {
+    uint8_t r = 0;
+    for (int b = 0; b < kRegBits; b++)
+        if ((tileLocal >> L.regPos[b]) & 1u) r |= (uint8_t) (1u << b);
+    return r;
+}
+
+bool isZero(double x) { return x == 0.0; }
+
+}  // namespace
+
+double opFlopsPerAmp(const KOp &op) {
+    double f = 0.0;
+    switch (op.kind) {
+        case KOP_M2R:
+        case KOP_M2I:
+        case KOP_PH:
+        case KOP_Z2: f = 6.0; break;
+        case KOP_M2C: f = 14.0; break;
+        case KOP_DENSE: f = 8.0 * (double) (1 << op.k) - 2.0; break;
+        default: f = 0.0; break;
+    }
+    const int c = __builtin_popcount(op.ctrlReg) + __builtin_popcount(op.ctrlLoc) + __builtin_popcount(op.ctrlCta);
+    return f / (double) (1u << c);
+}
+
+void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out) {
+    std::memset(&out, 0, sizeof(out));
+    out.numBits = numBits;
+    out.numReal = numReal;
+    out.initKind = hdr.initKind;
+    out.initIndex = hdr.initIndex;
+    out.initAmp = hdr.initAmp;
+    out.hasRestrict = hdr.hasRestrict ? 1 : 0;
+    out.restrictMask = hdr.restrictMask;
+    out.restrictValue = hdr.restrictValue;
+    out.restrictScale = hdr.restrictScale;
+    // tile = the lowest tileBits bits
+    for (int i = 0; i < tileBits - kCoalescedBits; i++) out.highPos[i] = (uint8_t) (kCoalescedBits + i);
+    for (int i = 0; i < numBits - tileBits; i++) out.ctaPos[i] = (uint8_t) (tileBits + i);
+}
+
+bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits, const MatrixPool &pool,
+                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err) {
+    const TileMap tm = makeTileMap(block.tileMask, numBits);
+
+    // ---- phases: greedy DAG selection with the register budget
+    struct Phase {
+        std::vector<Gate> gates;
+        std::vector<int> front;  // dense-gate target order (tile-local)
+        uint32_t targetsLocal = 0;
+    };
+    std::vector<Phase> phases;
+    {
+        GateDag dag(numBits, false);
+        for (const Gate &g : block.gates) dag.add(g);
+        while (!dag.empty()) {
+            u64 mask = 0;
+            std::vector<Gate> gs = dag.takeBlock(kRegBits, mask, 1u << 20);
+            if (gs.empty()) {
+                if (err) *err = "a gate has more non-diagonal targets than the register tile holds";
+                return false;
+            }
+            // a dense multi-qubit gate fixes the register order: give it its own phase
+            Phase cur;
+            auto flush = [&]() {
+                if (!cur.gates.empty()) phases.push_back(cur);
+                cur = Phase();
+            };
+            for (const Gate &g : gs) {
+                if (g.type == OP_MULTI_UNITARY) {
+                    flush();
+                    Phase d;
+                    d.gates.push_back(g);
+                    for (int i = 0; i < g.numMultiTargets; i++) d.front.push_back(tm.local[g.multiTargets[i]]);
+                    d.targetsLocal = splitMask(g.targetMask, tm).tileLocal;
+                    phases.push_back(d);
+                    continue;
+                }
+                cur.gates.push_back(g);
+                if (!isDiagonalType(g.type)) cur.targetsLocal |= splitMask(g.targetMask, tm).tileLocal;
+            }
+            flush();
+        }
+    }
+
+    // ---- programs
+    auto newProgram = [&](bool isFirst) {
+        out.emplace_back();
+        TileProgram &p = out.back();
+        std::memset(&p, 0, sizeof(p));
+        p.numBits = numBits;
+        p.numReal = numReal;
+        if (isFirst) {
+            p.initKind = first.initKind;
+            p.initIndex = first.initIndex;
+            p.initAmp = first.initAmp;
+            p.hasRestrict = first.hasRestrict ? 1 : 0;
+            p.restrictMask = first.restrictMask;
+            p.restrictValue = first.restrictValue;
+            p.restrictScale = first.restrictScale;
+        } else {
+            p.initKind = INIT_NONE;
+        }
+        for (int i = 0; i < tileBits - kCoalescedBits; i++) p.highPos[i] = (uint8_t) tm.tilePos[kCoalescedBits + i];
+        for (int b = 0; b < numBits; b++)
+            if (tm.ctaIdx[b] >= 0) p.ctaPos[tm.ctaIdx[b]] = (uint8_t) b;
+        if (stats) stats->sweeps++;
+        return &out.back();
+    };
+    TileProgram *prog = newProgram(true);
+    int numCoef = 0;
+
+    for (const Phase &ph : phases) {
+        const PhaseLayout L = makeLayout(ph.front, ph.targetsLocal, tileBits);
+        // encode the phase's ops into a scratch list first
+        std::vector<KOp> ops;
+        std::vector<double> coef;
+        for (const Gate &g : ph.gates) {
+            KOp op;
+            std::memset(&op, 0, sizeof(op));
+            op.selCta = -1;
+            const Split c = splitMask(g.controlMask, tm);
+            op.ctrlReg = regSpace(c.tileLocal, L);
+            op.ctrlLoc = (uint16_t) (c.tileLocal & ~L.regLocalMask);
+            op.ctrlCta = c.cta;
+            op.coef = (uint16_t) coef.size();  // phase-relative, rebased when copied
+            auto targetReg = [&](u64 tmask) -> int {
+                const Split t = splitMask(tmask, tm);
+                for (int b = 0; b < kRegBits; b++)
+                    if (t.tileLocal == (1u << L.regPos[b])) return b;
+                return -1;
+            };
+            bool emit = true;
+            const int t = (int) g.type;
+            if (t < 8) {
+                switch (t) {
+                    case OP_ONE: emit = false; break;
+                    case OP_S_GATE: op.kind = KOP_MULI; break;
+                    case OP_PAULI_Z: op.kind = KOP_NEG; break;
+                    case OP_S_GATE_CONJ: op.kind = KOP_MULNI; break;
+                    default: {
+                        // odd powers: e^{i pi t / 4} with (+-1 +- i)/sqrt(2)
+                        op.kind = KOP_PH;
+                        const double c0 = (t == 1 || t == 7) ? kRsqrt2 : -kRsqrt2;
+                        const double s0 = (t == 1 || t == 3) ? kRsqrt2 : -kRsqrt2;
+                        coef.push_back(c0);
+                        coef.push_back(s0);
+                        break;
+                    }
+                }
+            } else if (g.type == OP_PHASE_SHIFT) {
+                op.kind = KOP_PH;
+                coef.push_back(std::cos(g.op[0]));
+                coef.push_back(std::sin(g.op[0]));
+            } else if (g.type == OP_ROTATE_Z) {
+                op.kind = KOP_Z2;
+                coef.push_back(std::cos(g.op[0]));
+                coef.push_back(std::sin(g.op[0]));
+                const Split s = splitMask(g.targetMask, tm);
+                if (s.tileLocal) {
+                    const uint8_t r = regSpace(s.tileLocal, L);
+                    if (r)
+                        op.selReg = r;
+                    else
+                        op.selLoc = (uint16_t) s.tileLocal;
+                } else {
+                    op.selCta = (int8_t) __builtin_ctz(s.cta);
+                }
+            } else if (g.type == OP_MULTI_UNITARY) {
+                op.kind = KOP_DENSE;
+                op.k = (uint8_t) g.numMultiTargets;
+                const auto &m = pool.mats[(size_t) g.multiIndex];
+                coef.insert(coef.end(), m.begin(), m.end());
+            } else {
+                const int k = targetReg(g.targetMask);
+                if (k < 0) {
+                    if (err) *err = "internal: pair-gate target is not a register bit";
+                    return false;
+                }
+                op.k = (uint8_t) k;
+                switch (g.type) {
+                    case OP_PAULI_X: op.kind = KOP_X; break;
+                    case OP_PAULI_Y: op.kind = KOP_Y; break;
+                    case OP_PAULI_Y_CONJ: op.kind = KOP_YC; break;
+                    case OP_HADAMARD:
+                        op.kind = KOP_M2R;
+                        coef.insert(coef.end(), {kRsqrt2, kRsqrt2, kRsqrt2, -kRsqrt2});
+                        break;
+                    case OP_ROTATE_X: {
+                        op.kind = KOP_M2I;
+                        const double cs = std::cos(g.op[0]), sn = std::sin(g.op[0]);
+                        coef.insert(coef.end(), {cs, -sn, -sn, cs});
+                        break;
+                    }
+                    case OP_ROTATE_Y: {
+                        op.kind = KOP_M2R;
+                        const double cs = std::cos(g.op[0]), sn = std::sin(g.op[0]);
+                        coef.insert(coef.end(), {cs, -sn, sn, cs});
+                        break;
+                    }
+                    default: {
+                        double m[8];
+                        gateMatrix(g, m);
+                        if (isZero(m[1]) && isZero(m[3]) && isZero(m[5]) && isZero(m[7])) {
+                            op.kind = KOP_M2R;
+                            coef.insert(coef.end(), {m[0], m[2], m[4], m[6]});
+                        } else if (isZero(m[1]) && isZero(m[2]) && isZero(m[4]) && isZero(m[7])) {
+                            op.kind = KOP_M2I;
+                            coef.insert(coef.end(), {m[0], m[3], m[5], m[6]});
+                        } else {
+                            op.kind = KOP_M2C;
+                            coef.insert(coef.end(), m, m + 8);
+                        }
+                        break;
+                    }
+                }
+            }
+            if (emit) ops.push_back(op);
+        }
+        if (ops.size() > (size_t) kMaxOps || coef.size() > (size_t) kMaxCoef) {
+            if (err) *err = "a single register phase exceeds the tile program capacity";
+            return false;
+        }
+        // start a new program (one more sweep over the same tile) when full
+        if (prog->numPhases + 1 > kMaxPhases || prog->numOps + (int) ops.size() > kMaxOps ||
+            numCoef + (int) coef.size() > kMaxCoef) {
+            prog = newProgram(false);
+            numCoef = 0;
+        }
+        KPhase &kp = prog->phases[prog->numPhases++];
+        std::memset(&kp, 0, sizeof(kp));
+        for (int i = 0; i < tileBits - kRegBits; i++) kp.thrPos[i] = (uint8_t) L.thrPos[i];
+        kp.opBegin = (uint16_t) prog->numOps;
+        for (KOp o : ops) {
+            o.coef = (uint16_t) (o.coef + numCoef);
+            prog->ops[prog->numOps++] = o;
+            if (stats) {
+                stats->ops++;
+                stats->flopsPerAmp += opFlopsPerAmp(o);
+            }
+        }
+        kp.opEnd = (uint16_t) prog->numOps;
+        for (int j = 0; j < kRegs; j++) {
+            uint32_t loc = 0;
+            for (int b = 0; b < kRegBits; b++)
+                if ((j >> b) & 1) loc |= 1u << L.regPos[b];
+            kp.regOff[j] = (uint16_t) tileSwizzle(loc);
+        }
+        for (double c : coef) prog->coef[numCoef++] = c;
+        if (stats) stats->phases++;
+    }
+    if (stats) stats->gates += (int) block.gates.size();
+    return true;
+}
+
+}  // namespace dgq

@@ -1,0 +1,65 @@
+// planner.h -- cuts a recorded gate list into state sweeps ("fused blocks")
+// and encodes each sweep as a TileProgram for the tile kernel.
+//
+// dgQuEST cuts its circuit twice with the same greedy DAG selection
+// (src/cpp/QuEST_backend.cpp:118-141,152-182): into sections that fit a task
+// and into 11-qubit fused gates seeded with the 5 coalesced low bits, then
+// re-DAGs each fused gate with budget 1 to group gates by target
+// (src/cpp/QuEST_gpu_kernel.cu:529-562). On one GPU with the state resident
+// in HBM there are no sections: the planner takes blocks of W tile bits
+// (seeded with the 5 low bits, padded from bit 5 upward like
+// QuEST_gpu_kernel.cu:504-509), then phases of 4 register bits.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "ir.h"
+#include "tile_program.h"
+
+namespace dgq {
+
+struct BlockPlan {
+    u64 tileMask = 0;         // W address bits, bits 0..4 always included
+    std::vector<Gate> gates;  // dependency order
+};
+
+struct PlanStats {
+    int sweeps = 0;     // kernel launches (state read+write passes)
+    int phases = 0;     // register layouts summed over sweeps
+    int ops = 0;        // kernel ops summed over sweeps
+    int gates = 0;      // gates after merging
+    double flopsPerAmp = 0;  // algorithmic FP64 flops per amplitude, summed over ops
+};
+
+// Multi-qubit unitary matrices referenced by OP_MULTI_UNITARY gates.
+struct MatrixPool {
+    std::vector<std::vector<double>> mats;  // row-major 2^k x 2^k, (re, im) interleaved
+};
+
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits);
+
+// Encodes one block. The gate list may not fit one TileProgram; then the
+// block is emitted as several programs over the same tile (each one more
+// sweep). Only the first program carries `first` (init / lazy collapse).
+struct SweepHeader {
+    int32_t initKind = INIT_NONE;
+    uint64_t initIndex = 0;
+    double initAmp = 0.0;
+    bool hasRestrict = false;
+    uint64_t restrictMask = 0, restrictValue = 0;
+    double restrictScale = 1.0;
+};
+
+bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits, const MatrixPool &pool,
+                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err);
+
+// A program that only applies the header (init and/or lazy collapse).
+void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out);
+
+// Algorithmic FP64 flops per amplitude of one kernel op (formulas of
+// QuEST_gpu_kernel.cu:17-170 counted as multiplies + adds per amplitude,
+// averaged over the amplitudes it touches when uncontrolled).
+double opFlopsPerAmp(const KOp &op);
+
+}  // namespace dgq

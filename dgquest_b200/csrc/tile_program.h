@@ -1,0 +1,107 @@
+// tile_program.h -- the per-launch program of the fused tile kernel.
+//
+// One launch = one sweep of the state: every CTA owns one tile of 2^W
+// amplitudes whose indices range over W "tile" address bits (always
+// including the 5 lowest bits, so each warp moves 512-byte runs) with the
+// other bits fixed by blockIdx. Inside the CTA each thread keeps 16
+// amplitudes in registers. The gate list of the fused block is cut into
+// phases; in a phase the 4 register bits cover every non-diagonal target,
+// so all of the phase's gates run in registers, and phases change layout
+// through shared memory. Diagonal gates need no register placement (they
+// read the index bits), which is dgQuEST's treatment of diagonal gates and
+// of Rz on a non-local target (QuEST_gpu_kernel.cu:300-311).
+//
+// The program is passed by value as a __grid_constant__ kernel parameter
+// (constant bank; uniform loads), so no per-launch host-to-device copy is
+// needed and the launch can be captured in a CUDA graph as is.
+#pragma once
+
+#include <cstdint>
+
+namespace dgq {
+
+constexpr int kRegBits = 4;
+constexpr int kRegs = 1 << kRegBits;
+constexpr int kCoalescedBits = 5;
+constexpr int kMinTileBits = 9;   // >= 32 threads (one full warp)
+constexpr int kMaxTileBits = 13;  // 2^13 x 16 B = 128 KiB of shared memory
+constexpr int kMaxThreadBits = kMaxTileBits - kRegBits;
+constexpr int kMaxStateBits = 40;
+constexpr int kMaxPhases = 56;
+constexpr int kMaxOps = 640;
+constexpr int kMaxCoef = 1500;
+
+enum KOpKind : uint8_t {
+    KOP_M2R = 0,   // real 2x2 [[a, b], [c, d]] on a register pair
+    KOP_M2I = 1,   // [[a, i b], [i c, d]] (a, b, c, d real): the Rx family
+    KOP_M2C = 2,   // general complex 2x2 (8 coefficients, row-major re/im)
+    KOP_X = 3,     // swap
+    KOP_Y = 4,     // Pauli-Y
+    KOP_YC = 5,    // conjugated Pauli-Y
+    KOP_NEG = 6,   // multiply by -1
+    KOP_MULI = 7,  // multiply by +i
+    KOP_MULNI = 8, // multiply by -i
+    KOP_PH = 9,    // multiply by (c + i s)
+    KOP_Z2 = 10,   // multiply by (c - i s) when the selector bit is 0, (c + i s) when 1
+    KOP_DENSE = 11 // dense 2^k x 2^k on register bits 0..k-1 (k = op.k), coefficients re/im
+};
+
+// 16 bytes; every field is read uniformly by all threads of the CTA.
+struct KOp {
+    uint8_t kind;
+    uint8_t k;         // target register bit (pair ops) or k (dense)
+    uint8_t ctrlReg;   // control bits in register-index space
+    uint8_t selReg;    // KOP_Z2 selector when it is a register bit
+    uint16_t ctrlLoc;  // control bits among the thread (non-register) tile bits
+    uint16_t selLoc;   // KOP_Z2 selector when it is a thread tile bit
+    uint32_t ctrlCta;  // control bits in blockIdx space (non-tile address bits)
+    uint16_t coef;     // offset into TileProgram::coef
+    int8_t selCta;     // KOP_Z2 selector bit index in blockIdx space, -1 if none
+    uint8_t pad;
+};
+
+struct KPhase {
+    uint8_t thrPos[kMaxThreadBits];  // tile-local bit of thread-index bit i
+    uint8_t pad[3];
+    uint16_t opBegin, opEnd;
+    uint16_t regOff[kRegs];  // swizzled shared-memory offset of register j
+};
+
+enum InitKind : int32_t {
+    INIT_NONE = 0,       // read the state
+    INIT_CLASSICAL = 1,  // |initIndex>
+    INIT_PLUS = 2,       // initAmp on every index below 2^numReal
+    INIT_BLANK = 3,      // all zero
+};
+
+struct TileProgram {
+    int32_t numPhases;
+    int32_t numOps;
+    int32_t numBits;   // address bits of the state buffer
+    int32_t numReal;   // qubits the user sees (<= numBits)
+    int32_t initKind;
+    int32_t hasRestrict;
+    uint64_t initIndex;
+    double initAmp;
+    uint64_t restrictMask;   // lazy measurement collapse applied at load:
+    uint64_t restrictValue;  //   amp = (idx & mask) == value ? amp * scale : 0
+    double restrictScale;
+    uint8_t highPos[kMaxTileBits - kCoalescedBits];  // address bit of tile-local bit 5 + i
+    uint8_t ctaPos[kMaxStateBits];                   // address bit of blockIdx bit i
+    uint8_t pad0[4];
+    KPhase phases[kMaxPhases];
+    KOp ops[kMaxOps];
+    double coef[kMaxCoef];
+};
+
+static_assert(sizeof(KOp) == 16, "KOp layout");
+static_assert(sizeof(TileProgram) <= 32000, "TileProgram must fit the kernel parameter space");
+
+// Shared-memory swizzle of a tile-local index: the low 3 bits (the 16-byte
+// bank group) are XOR-ed with the higher bit triples. Linear over GF(2),
+// so swz(a | b) = swz(a) ^ swz(b) for disjoint a, b.
+static inline constexpr uint32_t tileSwizzle(uint32_t x) {
+    return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u);
+}
+
+}  // namespace dgq

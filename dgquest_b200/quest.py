@@ -1,0 +1,244 @@
+"""Python mirror of the QuEST C API exported by libdgq.so.
+
+Names, argument order and meaning follow dgQuEST's include/QuEST.h (each
+C declaration in include/QuEST.h cites its dgQuEST prototype). Structures
+are passed by value exactly as in C. The C library's default on invalid
+input is QuEST's: print and exit(code) (src/QuEST_validation.c:82-91).
+This mirror switches the library to status recording and raises
+``QuESTError(code, message)`` instead, so a Python process survives bad
+input; ``code`` is QuEST's error code.
+"""
+import ctypes
+from ctypes import POINTER, Structure, c_double, c_int, c_int64, c_longlong, c_ulong, c_ulonglong, c_void_p
+
+import numpy as np
+
+from . import load_library
+
+qreal = c_double
+
+
+class Complex(Structure):
+    _fields_ = [("real", qreal), ("imag", qreal)]
+
+
+class ComplexMatrix2(Structure):
+    _fields_ = [("r0c0", Complex), ("r0c1", Complex), ("r1c0", Complex), ("r1c1", Complex)]
+
+
+class Vector(Structure):
+    _fields_ = [("x", qreal), ("y", qreal), ("z", qreal)]
+
+
+class QuESTEnv(Structure):
+    _fields_ = [("value", c_void_p), ("rank", c_int)]
+
+
+class Qureg(Structure):
+    _fields_ = [
+        ("isDensityMatrix", c_int),
+        ("numQubitsRepresented", c_ulonglong),
+        ("numQubitsInStateVec", c_ulonglong),
+        ("numAmpsTotal", c_ulonglong),
+        ("env", QuESTEnv),
+        ("state", c_void_p),
+    ]
+
+
+class ComplexMatrixN(Structure):
+    _fields_ = [("numQubits", c_int), ("real", POINTER(POINTER(qreal))), ("imag", POINTER(POINTER(qreal)))]
+
+
+class PlanStats(Structure):
+    _fields_ = [
+        ("sweeps", ctypes.c_int32),
+        ("phases", ctypes.c_int32),
+        ("ops", ctypes.c_int32),
+        ("gates", ctypes.c_int32),
+        ("tileBits", ctypes.c_int32),
+        ("numBits", ctypes.c_int32),
+        ("flopsPerAmp", c_double),
+        ("planMillis", c_double),
+    ]
+
+
+class QuESTError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+I, D, Q, E, P = c_int, c_double, Qureg, QuESTEnv, POINTER
+_SIGS = {
+    # name: (restype, argtypes)
+    "createQuESTEnv": (QuESTEnv, []),
+    "destroyQuESTEnv": (None, [E]),
+    "seedQuESTDefault": (None, []),
+    "seedQuEST": (None, [P(c_ulong), I]),
+    "getQuEST_PREC": (I, []),
+    "createQureg": (Qureg, [I, E]),
+    "searchQuregTaskPartitions": (None, [Q, E]),
+    "destroyQureg": (None, [Q, E]),
+    "getNumQubits": (I, [Q]),
+    "getNumAmps": (I, [Q]),
+    "initZeroState": (None, [Q]),
+    "initPlusState": (None, [Q]),
+    "initClassicalState": (None, [Q, c_longlong]),
+    "initStateFromAmps": (None, [Q, P(D), P(D)]),
+    "phaseShift": (None, [Q, I, D]),
+    "controlledPhaseShift": (None, [Q, I, I, D]),
+    "multiControlledPhaseShift": (None, [Q, P(I), I, D]),
+    "controlledPhaseFlip": (None, [Q, I, I]),
+    "multiControlledPhaseFlip": (None, [Q, P(I), I]),
+    "sGate": (None, [Q, I]),
+    "tGate": (None, [Q, I]),
+    "compactUnitary": (None, [Q, I, Complex, Complex]),
+    "unitary": (None, [Q, I, ComplexMatrix2]),
+    "rotateX": (None, [Q, I, D]),
+    "rotateY": (None, [Q, I, D]),
+    "rotateZ": (None, [Q, I, D]),
+    "rotateAroundAxis": (None, [Q, I, D, Vector]),
+    "controlledRotateX": (None, [Q, I, I, D]),
+    "controlledRotateY": (None, [Q, I, I, D]),
+    "controlledRotateZ": (None, [Q, I, I, D]),
+    "controlledRotateAroundAxis": (None, [Q, I, I, D, Vector]),
+    "controlledCompactUnitary": (None, [Q, I, I, Complex, Complex]),
+    "controlledUnitary": (None, [Q, I, I, ComplexMatrix2]),
+    "multiControlledUnitary": (None, [Q, P(I), I, I, ComplexMatrix2]),
+    "pauliX": (None, [Q, I]),
+    "pauliY": (None, [Q, I]),
+    "pauliZ": (None, [Q, I]),
+    "hadamard": (None, [Q, I]),
+    "controlledNot": (None, [Q, I, I]),
+    "controlledPauliY": (None, [Q, I, I]),
+    "swapGate": (None, [Q, I, I]),
+    "u1Gate": (None, [Q, I, D]),
+    "u2Gate": (None, [Q, I, D, D]),
+    "u3Gate": (None, [Q, I, D, D, D]),
+    "SqX": (None, [Q, I]),
+    "SqY": (None, [Q, I]),
+    "SqW": (None, [Q, I]),
+    "fSim": (None, [Q, I, I, D, D]),
+    "multiQubitUnitary": (None, [Q, P(I), I, ComplexMatrixN]),
+    "createComplexMatrixN": (ComplexMatrixN, [I]),
+    "destroyComplexMatrixN": (None, [ComplexMatrixN]),
+    "getAmp": (Complex, [Q, c_longlong]),
+    "getRealAmp": (D, [Q, c_longlong]),
+    "getImagAmp": (D, [Q, c_longlong]),
+    "getProbAmp": (D, [Q, c_longlong]),
+    "calcTotalProb": (D, [Q]),
+    "calcProbOfOutcome": (D, [Q, I, I]),
+    "collapseToOutcome": (D, [Q, I, I]),
+    "measure": (I, [Q, I]),
+    "measureWithStats": (I, [Q, I, P(D)]),
+    # extensions (include/dgq.h)
+    "dgq_setErrorMode": (I, [I]),
+    "dgq_getLastError": (I, [ctypes.c_char_p, I]),
+    "dgq_setTileBits": (I, [Q, I]),
+    "dgq_getPlanStats": (I, [Q, P(PlanStats)]),
+    "dgq_planPending": (I, [Q]),
+    "dgq_launchPlanned": (I, [Q]),
+    "dgq_sync": (I, [Q]),
+    "dgq_getStream": (c_void_p, [Q]),
+    "dgq_getDeviceState": (c_void_p, [Q, P(I)]),
+    "dgq_getStateVector": (I, [Q, P(D), P(D)]),
+    "dgq_getLaunchCount": (c_int64, []),
+    "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
+}
+
+_lib = None
+
+
+def _library():
+    global _lib
+    if _lib is None:
+        lib = load_library()
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        lib.dgq_setErrorMode(1)
+        _lib = lib
+    return _lib
+
+
+def _check():
+    lib = _library()
+    buf = ctypes.create_string_buffer(512)
+    code = lib.dgq_getLastError(buf, 512)
+    if code:
+        raise QuESTError(code, buf.value.decode(errors="replace"))
+
+
+def _wrap(name):
+    def call(*args):
+        out = getattr(_library(), name)(*args)
+        _check()
+        return out
+
+    call.__name__ = name
+    call.__doc__ = f"QuEST API `{name}` (see include/QuEST.h)."
+    return call
+
+
+for _name in _SIGS:
+    globals()[_name] = _wrap(_name)
+
+
+# ---------------------------------------------------------------- helpers
+def mat2(m):
+    """ComplexMatrix2 from a 2x2 array-like of complex numbers."""
+    m = np.asarray(m, dtype=np.complex128)
+    return ComplexMatrix2(*(Complex(float(m[r, c].real), float(m[r, c].imag)) for r in range(2) for c in range(2)))
+
+
+def int_array(values):
+    arr = (c_int * len(values))(*[int(v) for v in values])
+    return arr
+
+
+def matrixN(u):
+    """ComplexMatrixN (library-allocated) filled from a square complex array."""
+    u = np.asarray(u, dtype=np.complex128)
+    k = int(round(np.log2(u.shape[0])))
+    m = createComplexMatrixN(k)
+    for r in range(u.shape[0]):
+        for c in range(u.shape[1]):
+            m.real[r][c] = float(u[r, c].real)
+            m.imag[r][c] = float(u[r, c].imag)
+    return m
+
+
+def state_vector(q):
+    """All amplitudes of q in logical order, as a complex128 numpy array."""
+    n = int(q.numQubitsRepresented)
+    re = np.empty(1 << n, dtype=np.float64)
+    im = np.empty(1 << n, dtype=np.float64)
+    dgq_getStateVector(q, re.ctypes.data_as(POINTER(c_double)), im.ctypes.data_as(POINTER(c_double)))
+    return re + 1j * im
+
+
+def prob_all_zero(q):
+    n = int(q.numQubitsRepresented)
+    out = np.empty(n, dtype=np.float64)
+    dgq_calcProbOfAllZero(q, out.ctypes.data_as(POINTER(c_double)))
+    return out
+
+
+def plan_stats(q):
+    st = PlanStats()
+    dgq_getPlanStats(q, ctypes.byref(st))
+    return st
+
+
+def seed(keys):
+    arr = (c_ulong * len(keys))(*[int(k) for k in keys])
+    seedQuEST(arr, len(keys))
+
+
+def init_from_amps(q, amps):
+    amps = np.ascontiguousarray(amps, dtype=np.complex128)
+    re = np.ascontiguousarray(amps.real)
+    im = np.ascontiguousarray(amps.imag)
+    initStateFromAmps(q, re.ctypes.data_as(POINTER(c_double)), im.ctypes.data_as(POINTER(c_double)))

@@ -1,0 +1,90 @@
+/*
+ * dgq.h -- libdgq extensions beyond the QuEST C API (include/QuEST.h).
+ *
+ * None of these has a counterpart in dgQuEST unless a citation says so.
+ * They cover: error-status mode, tile-width (block width) choice, the plan
+ * and launch split used for device timing, plan statistics, bulk state
+ * read-out, and kernel launch accounting.
+ */
+#ifndef DGQ_EXT_H
+#define DGQ_EXT_H
+
+#include <stdint.h>
+
+#include "QuEST.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error handling. Mode 0 (default) prints QuEST's message and exits with
+ * its code, as dgQuEST does (src/QuEST_validation.c:82-91). Mode 1 records
+ * the error instead: the failing call returns without effect (a zero or
+ * default value where it returns one) and dgq_getLastError() reports it. */
+#define DGQ_ERRORS_EXIT 0
+#define DGQ_ERRORS_RECORD 1
+int dgq_setErrorMode(int mode);
+/* Returns the last error code (0 = none) and clears it; copies the message
+ * into msg (if msg != NULL and len > 0). */
+int dgq_getLastError(char *msg, int len);
+
+/* Tile width W (address bits per CTA tile, 9..13) used for this register.
+ * 0 selects it with the cost model (the recast of dgQuEST's time predictor,
+ * src/cpp/time_predictor.cpp:343-395). Returns the previous setting. */
+int dgq_setTileBits(Qureg qureg, int tileBits);
+
+/* Plan statistics of the most recent execution of pending gates. */
+typedef struct dgq_plan_stats {
+    int32_t sweeps;        /* tile-kernel launches (state read + write passes) */
+    int32_t phases;        /* register layouts over all sweeps */
+    int32_t ops;           /* kernel ops over all sweeps */
+    int32_t gates;         /* gates after peephole merging */
+    int32_t tileBits;      /* W used */
+    int32_t numBits;       /* address bits of the state buffer */
+    double flopsPerAmp;    /* algorithmic FP64 flops per amplitude, whole plan */
+    double planMillis;     /* host planning time */
+} dgq_plan_stats;
+int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
+
+/* Plans the pending gates (and pending initialisation / collapse) into
+ * sweep programs and keeps them; dgq_launchPlanned launches them on the
+ * register's stream without waiting. A kept plan can be launched again:
+ * every launch recomputes the whole plan from its initial state, so it is
+ * only meaningful for plans that start from an initialisation. */
+int dgq_planPending(Qureg qureg);
+int dgq_launchPlanned(Qureg qureg);
+/* Runs everything pending and waits for the GPU. */
+int dgq_sync(Qureg qureg);
+
+/* The CUDA stream (cudaStream_t) all of this register's kernels run on. */
+void *dgq_getStream(Qureg qureg);
+/* Device pointer of the state buffer (interleaved re/im doubles) and its
+ * number of address bits (>= numQubits; extra bits are always |0>). The
+ * state is in virtual order; see dgq_getStateVector for logical order. */
+void *dgq_getDeviceState(Qureg qureg, int *numBits);
+
+/* Copies all 2^n amplitudes, in logical index order, into re[] and im[]. */
+int dgq_getStateVector(Qureg qureg, qreal *re, qreal *im);
+
+/* Kernel launches issued by this library since the process started. */
+int64_t dgq_getLaunchCount(void);
+
+/* P(qubit = 0) for every qubit in one pass (the reduction behind
+ * calcProbOfOutcome, src/cpp/QuEST_gpu_kernel.cu:769-807). */
+int dgq_calcProbOfAllZero(Qureg qureg, qreal *probs);
+
+/* Host-only planning (no GPU call): plans `count` gates given in dgQuEST's
+ * IR encoding (type numbers of src/cpp/QuEST_backend.h:89-114, target and
+ * control bit masks, operand[8] per gate with rotations carrying angle/2)
+ * on a register of numQubits with tile width tileBits (0 = cost model), and
+ * reports the plan. Merged gates are returned through mergedTypes (may be
+ * NULL, else room for `count` entries) with *numMerged set. */
+int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
+                  const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
+                  int32_t *numMerged);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGQ_EXT_H */
