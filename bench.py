@@ -245,6 +245,9 @@ def run_gpu(args, world, rank, local):
     avg_launch_s = (ms_step / 1000.0) / st.sweeps
     achieved = bytes_per_launch / avg_launch_s / 1e9
     flops = st.flopsPerAmp * (1 << n)
+    pk = ctypes.c_double(0.0)
+    Q.dgq_measureFp64Peak(ctypes.byref(pk))
+    fp64_peak = pk.value
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -269,6 +272,11 @@ def run_gpu(args, world, rank, local):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic,
                              "peak_source": hbm_kind, "kernel": f"tileKernel<{st.tileBits}>"},
+                "fp64_roofline": {"achieved_tflops": flops / (ms_step / 1000.0) / 1e12,
+                                  "peak_tflops": fp64_peak, "frac": flops / (ms_step / 1000.0) / 1e12 / fp64_peak,
+                                  "peak_source": "measured live (DFMA loop, dgq_measureFp64Peak)",
+                                  "circuit_floor_ms": max(flops / (fp64_peak * 1e12),
+                                                          st.sweeps * bytes_per_launch / (hbm * 1e9)) * 1e3},
                 "e2e": {"value": world / e2e_t, "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t * 1000.0,
                         "plan_ms": st2.planMillis},

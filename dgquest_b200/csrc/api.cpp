@@ -276,17 +276,10 @@ bool planPending(QuregState &s, const char *func) {
         h.restrictScale = s.rScale;
     }
     dgq::PlanStats st;
-    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(s.pending, s.numBits, W);
-    size_t planned = 0;
-    for (const auto &b : blocks) planned += b.gates.size();
-    {
-        // gates left unplanned would be wider than a tile
-        dgq::GateDag check(s.numBits, true);
-        for (const Gate &g : s.pending) check.add(g);
-        if (planned != check.size()) {
-            return raise(E_UNSUPPORTED, func, "a multi-qubit gate is wider than the register tile (max 4 targets)");
-        }
-    }
+    bool complete = true;
+    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(s.pending, s.numBits, W, &complete);
+    if (!complete)
+        return raise(E_UNSUPPORTED, func, "a multi-qubit gate is wider than the register tile (max 4 targets)");
     std::string err;
     bool first = true;
     for (const auto &b : blocks) {
@@ -1060,7 +1053,7 @@ int dgq_setTileBits(Qureg q, int tileBits) {
     QuregState &s = *stateOf(q);
     const int prev = s.tileBitsSetting;
     if (tileBits != 0 && (tileBits < dgq::kMinTileBits || tileBits > dgq::kMaxTileBits)) {
-        raise(E_INVALID_ARGUMENT, __func__, "tile bits must be 0 or in [9, 13]");
+        raise(E_INVALID_ARGUMENT, __func__, "tile bits must be 0 or in [9, 12]");
         return prev;
     }
     s.tileBitsSetting = tileBits;
@@ -1144,6 +1137,39 @@ int dgq_calcProbOfAllZero(Qureg q, qreal *probs) {
     QuregState &s = *stateOf(q);
     if (!ensureProbs(s, __func__)) return -1;
     for (int i = 0; i < s.numQubits; i++) probs[i] = s.p0[(size_t) s.l2v[i]];
+    return 0;
+}
+
+int dgq_measureFp64Peak(double *tflops) {
+    if (!tflops) return -1;
+    int dev = 0, sms = 0;
+    if (!cudaOk(cudaGetDevice(&dev), __func__) ||
+        !cudaOk(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), __func__))
+        return -1;
+    const int blocks = sms * 8, iters = 4096;
+    double *out = nullptr;
+    cudaEvent_t e0, e1;
+    if (!cudaOk(cudaMalloc(&out, sizeof(double) * (size_t) blocks * 256), __func__)) return -1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    bool ok = cudaOk(dgq::launchFp64Peak(out, blocks, iters / 4, 0), __func__);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; ok && r < 3; r++) {
+        cudaEventRecord(e0, 0);
+        ok = cudaOk(dgq::launchFp64Peak(out, blocks, iters, 0), __func__);
+        cudaEventRecord(e1, 0);
+        ok = ok && cudaOk(cudaEventSynchronize(e1), __func__);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+        g_launches++;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (!ok) return -1;
+    const double fmas = (double) blocks * 256.0 * iters * 16.0 * 8.0;
+    *tflops = 2.0 * fmas / (best * 1e-3) / 1e12;
     return 0;
 }
 

@@ -163,7 +163,8 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, doubl
         }
         case KOP_Z2: {
             const double cs = c[0], sn = c[1];
-            const uint32_t sr = op.selReg;
+            const bool regSel = op.code < KC_Z2T;
+            const uint32_t sr = regSel ? (1u << op.k) : 0u;
             const bool thrBit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
             forAll(a, cr, [&](double2 &x, int j) {
                 const bool bit = sr ? ((j & sr) != 0u) : thrBit;
@@ -285,7 +286,6 @@ cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaS
         case 10: return launchTileW<10>(st, prog, s);
         case 11: return launchTileW<11>(st, prog, s);
         case 12: return launchTileW<12>(st, prog, s);
-        case 13: return launchTileW<13>(st, prog, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -493,6 +493,38 @@ cudaError_t launchInterleave(const double *re, const double *im, uint64_t count,
     uint64_t blocks = (total + 255) / 256;
     if (blocks > 148ULL * 32) blocks = 148ULL * 32;
     interleaveKernel<<<(unsigned) blocks, 256, 0, s>>>(re, im, count, total, out);
+    return cudaGetLastError();
+}
+
+}  // namespace dgq
+
+namespace dgq {
+
+// ------------------------------------------------ FP64 pipe microbenchmark
+// Eight independent DFMA chains per thread; the result is written so the
+// work cannot be removed. Used to state the FP64 roofline next to HBM.
+__global__ void __launch_bounds__(256) fp64PeakKernel(double *out, int iters, double seed) {
+    double x0 = seed + threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+           x7 = x0 + 7;
+    const double m = 0.999999, c = 1e-7;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            x0 = fma(x0, m, c);
+            x1 = fma(x1, m, c);
+            x2 = fma(x2, m, c);
+            x3 = fma(x3, m, c);
+            x4 = fma(x4, m, c);
+            x5 = fma(x5, m, c);
+            x6 = fma(x6, m, c);
+            x7 = fma(x7, m, c);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s) {
+    fp64PeakKernel<<<blocks, 256, 0, s>>>(out, iters, 1.0);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,7 @@ cudaError_t launchProb(const double2 *st, const ProbArgs &args, double *partial,
 int probNumCtas(const ProbArgs &args);
 cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s);
 cudaError_t launchGather(const double2 *st, const GatherArgs &args, double2 *out, cudaStream_t s);
+cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s);
 cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, double2 *out,
                              cudaStream_t s);
 

@@ -11,8 +11,9 @@ namespace dgq {
 
 static const double kRsqrt2 = 0.7071067811865475244008443621;
 
-std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits) {
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete) {
     std::vector<BlockPlan> blocks;
+    if (complete) *complete = true;
     GateDag dag(numBits, true);
     for (const Gate &g : gates) dag.add(g);
     const u64 seed = (1ULL << kCoalescedBits) - 1;
@@ -26,6 +27,7 @@ std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, i
         b.tileMask = mask & all;
         if (b.gates.empty()) {
             // only a gate wider than the tile is left: not plannable here
+            if (complete) *complete = false;
             break;
         }
         blocks.push_back(std::move(b));
@@ -261,6 +263,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                 return -1;
             };
             bool emit = true;
+            bool selIsReg = false;
             const int t = (int) g.type;
             if (t < 8) {
                 switch (t) {
@@ -289,10 +292,12 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                 const Split s = splitMask(g.targetMask, tm);
                 if (s.tileLocal) {
                     const uint8_t r = regSpace(s.tileLocal, L);
-                    if (r)
-                        op.selReg = r;
-                    else
+                    if (r) {
+                        op.k = (uint8_t) __builtin_ctz(r);
+                        selIsReg = true;
+                    } else {
                         op.selLoc = (uint16_t) s.tileLocal;
+                    }
                 } else {
                     op.selCta = (int8_t) __builtin_ctz(s.cta);
                 }
@@ -345,7 +350,26 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     }
                 }
             }
-            if (emit) ops.push_back(op);
+            if (emit) {
+                const int rc = op.ctrlReg ? 1 : 0;
+                op.thrCtl = (op.ctrlLoc || op.ctrlCta) ? 1 : 0;
+                switch (op.kind) {
+                    case KOP_M2R: op.code = (uint8_t) (KC_M2R + op.k + 4 * rc); break;
+                    case KOP_M2I: op.code = (uint8_t) (KC_M2I + op.k + 4 * rc); break;
+                    case KOP_M2C: op.code = (uint8_t) (KC_M2C + op.k + 4 * rc); break;
+                    case KOP_X: op.code = (uint8_t) (KC_X + op.k + 4 * rc); break;
+                    case KOP_Y: op.code = (uint8_t) (KC_Y + op.k + 4 * rc); break;
+                    case KOP_YC: op.code = (uint8_t) (KC_YC + op.k + 4 * rc); break;
+                    case KOP_Z2: op.code = (uint8_t) (selIsReg ? KC_Z2R + op.k + 4 * rc : KC_Z2T + rc); break;
+                    case KOP_PH: op.code = (uint8_t) (KC_PH + rc); break;
+                    case KOP_NEG: op.code = (uint8_t) (KC_NEG + rc); break;
+                    case KOP_MULI: op.code = (uint8_t) (KC_MULI + rc); break;
+                    case KOP_MULNI: op.code = (uint8_t) (KC_MULNI + rc); break;
+                    case KOP_DENSE: op.code = (uint8_t) (KC_DENSE + op.k - 1); break;
+                    default: break;
+                }
+                ops.push_back(op);
+            }
         }
         if (ops.size() > (size_t) kMaxOps || coef.size() > (size_t) kMaxCoef) {
             if (err) *err = "a single register phase exceeds the tile program capacity";

@@ -37,7 +37,9 @@ struct MatrixPool {
     std::vector<std::vector<double>> mats;  // row-major 2^k x 2^k, (re, im) interleaved
 };
 
-std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits);
+// `complete` (if given) is set to false when gates are left that no tile
+// can hold (a gate with more non-diagonal targets than the tile width).
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete = nullptr);
 
 // Encodes one block. The gate list may not fit one TileProgram; then the
 // block is emitted as several programs over the same tile (each one more

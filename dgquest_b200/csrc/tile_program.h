@@ -24,7 +24,7 @@ constexpr int kRegBits = 4;
 constexpr int kRegs = 1 << kRegBits;
 constexpr int kCoalescedBits = 5;
 constexpr int kMinTileBits = 9;   // >= 32 threads (one full warp)
-constexpr int kMaxTileBits = 13;  // 2^13 x 16 B = 128 KiB of shared memory
+constexpr int kMaxTileBits = 12;  // 2^12 x 16 B = 64 KiB per tile buffer
 constexpr int kMaxThreadBits = kMaxTileBits - kRegBits;
 constexpr int kMaxStateBits = 40;
 constexpr int kMaxPhases = 56;
@@ -46,18 +46,38 @@ enum KOpKind : uint8_t {
     KOP_DENSE = 11 // dense 2^k x 2^k on register bits 0..k-1 (k = op.k), coefficients re/im
 };
 
+// Dispatch codes of the tile kernel: one straight-line case per
+// (operation, target register bit, register-control present). Pair
+// operations: base + k (+4 when some control bit is a register bit).
+enum KCode : uint8_t {
+    KC_M2R = 0,
+    KC_M2I = 8,
+    KC_M2C = 16,
+    KC_X = 24,
+    KC_Y = 32,
+    KC_YC = 40,
+    KC_Z2R = 48,   // Rz-like, selector = register bit k (+4 controlled)
+    KC_Z2T = 56,   // selector is a thread/CTA bit (+1 controlled)
+    KC_PH = 58,    // +1 controlled
+    KC_NEG = 60,   // +1 controlled
+    KC_MULI = 62,  // +1 controlled
+    KC_MULNI = 64, // +1 controlled
+    KC_DENSE = 66, // + (k - 1), k = 1..4
+    KC_COUNT = 70
+};
+
 // 16 bytes; every field is read uniformly by all threads of the CTA.
 struct KOp {
-    uint8_t kind;
-    uint8_t k;         // target register bit (pair ops) or k (dense)
+    uint8_t kind;      // KOpKind (accounting)
+    uint8_t code;      // KCode (dispatch)
+    uint8_t thrCtl;    // 1 when ctrlLoc or ctrlCta is non-zero
     uint8_t ctrlReg;   // control bits in register-index space
-    uint8_t selReg;    // KOP_Z2 selector when it is a register bit
     uint16_t ctrlLoc;  // control bits among the thread (non-register) tile bits
-    uint16_t selLoc;   // KOP_Z2 selector when it is a thread tile bit
+    uint16_t selLoc;   // KC_Z2T selector when it is a thread tile bit
     uint32_t ctrlCta;  // control bits in blockIdx space (non-tile address bits)
     uint16_t coef;     // offset into TileProgram::coef
-    int8_t selCta;     // KOP_Z2 selector bit index in blockIdx space, -1 if none
-    uint8_t pad;
+    int8_t selCta;     // KC_Z2T selector bit index in blockIdx space, -1 if none
+    uint8_t k;         // target register bit (pair ops), selector register bit (KC_Z2R), k (dense)
 };
 
 struct KPhase {

@@ -66,12 +66,8 @@ def ops_to_ir(ops, n):
 def plan(ops, n, tile_bits=0, want_merged=False):
     """Host-only plan statistics of an op list (no GPU needed)."""
     from .quest import PlanStats, _check, _library
-    lib = _library()
-    fn = lib.dgq_planGates
+    fn = _library().dgq_planGates
     P = ctypes.POINTER
-    fn.restype = ctypes.c_int
-    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_uint64),
-                   P(ctypes.c_uint64), P(ctypes.c_double), P(PlanStats), P(ctypes.c_int32), P(ctypes.c_int32)]
     t, tm, cm, o = ops_to_ir(ops, n)
     st = PlanStats()
     merged = np.zeros(max(1, len(t)), dtype=np.int32)

@@ -145,6 +145,9 @@ _SIGS = {
     "dgq_getStateVector": (I, [Q, P(D), P(D)]),
     "dgq_getLaunchCount": (c_int64, []),
     "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
+    "dgq_measureFp64Peak": (I, [P(D)]),
+    "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
+                          P(ctypes.c_int32), P(ctypes.c_int32)]),
 }
 
 _lib = None

@@ -28,7 +28,7 @@ int dgq_setErrorMode(int mode);
  * into msg (if msg != NULL and len > 0). */
 int dgq_getLastError(char *msg, int len);
 
-/* Tile width W (address bits per CTA tile, 9..13) used for this register.
+/* Tile width W (address bits per CTA tile, 9..12) used for this register.
  * 0 selects it with the cost model (the recast of dgQuEST's time predictor,
  * src/cpp/time_predictor.cpp:343-395). Returns the previous setting. */
 int dgq_setTileBits(Qureg qureg, int tileBits);
@@ -72,6 +72,10 @@ int64_t dgq_getLaunchCount(void);
 /* P(qubit = 0) for every qubit in one pass (the reduction behind
  * calcProbOfOutcome, src/cpp/QuEST_gpu_kernel.cu:769-807). */
 int dgq_calcProbOfAllZero(Qureg qureg, qreal *probs);
+
+/* Measures the FP64 FMA throughput of the current device (TFLOP/s, an FMA
+ * counted as two flops) with a register-resident DFMA loop over all SMs. */
+int dgq_measureFp64Peak(double *tflops);
 
 /* Host-only planning (no GPU call): plans `count` gates given in dgQuEST's
  * IR encoding (type numbers of src/cpp/QuEST_backend.h:89-114, target and

@@ -43,7 +43,7 @@ def test_mixed_ops_every_call(quest, env, n):
     check(amps, p0, ref_amps, ref_p0)
 
 
-@pytest.mark.parametrize("tile_bits", [9, 10, 11, 12, 13])
+@pytest.mark.parametrize("tile_bits", [9, 10, 11, 12])
 def test_random_layers_every_tile_width(quest, env, tile_bits):
     n = 16
     ops = C.random_layers(n, 10, C.config_seed(2, tile_bits))
