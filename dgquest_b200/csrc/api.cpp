@@ -138,6 +138,12 @@ double nowMillis() {
 
 }  // namespace
 
+namespace dgq {
+// Error reporting for entry points defined in other translation units:
+// follows the library's error mode (exit with QuEST's message, or record).
+bool raiseExternal(int code, const char *func, const char *detail) { return raise(code, func, detail); }
+}  // namespace dgq
+
 // ====================================================================
 // environment and register state
 // ====================================================================

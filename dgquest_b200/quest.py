@@ -146,6 +146,7 @@ _SIGS = {
     "dgq_getLaunchCount": (c_int64, []),
     "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
     "dgq_measureFp64Peak": (I, [P(D)]),
+    "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),
 }
