@@ -236,7 +236,7 @@ def run_gpu(args, world, rank, local):
     e2e_t = max_over_ranks(float(np.mean(e2e_times)), world)
     st2 = Q.plan_stats(q)
     from dgquest_b200.quest import ctypes as _ct  # noqa: F401
-    prog_bytes = 25048  # sizeof(TileProgram): the kernel parameter block of one launch
+    prog_bytes = 25296  # sizeof(TileProgram): the kernel parameter block of one launch
     h2d = st2.sweeps * prog_bytes
     d2h = 16 + (n + 1) * 8
 
@@ -271,7 +271,9 @@ def run_gpu(args, world, rank, local):
                 "norm_error": abs(norm - 1.0),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic,
-                             "peak_source": hbm_kind, "kernel": f"tileKernel<{st.tileBits}>"},
+                             "peak_source": hbm_kind,
+                             "kernel": (f"dgq_sweep (runtime-specialised tile kernel, W={st.tileBits})"
+                                        if st.jitCompiled + st.jitReused else f"tileKernel<{st.tileBits}>")},
                 "fp64_roofline": {"achieved_tflops": flops / (ms_step / 1000.0) / 1e12,
                                   "peak_tflops": fp64_peak, "frac": flops / (ms_step / 1000.0) / 1e12 / fp64_peak,
                                   "peak_source": "measured live (DFMA loop, dgq_measureFp64Peak)",
@@ -279,7 +281,10 @@ def run_gpu(args, world, rank, local):
                                                           st.sweeps * bytes_per_launch / (hbm * 1e9)) * 1e3},
                 "e2e": {"value": world / e2e_t, "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t * 1000.0,
-                        "plan_ms": st2.planMillis},
+                        "plan_ms": st2.planMillis,
+                        "cold_specialisation_ms": st.jitMillis,
+                        "note": "steady state: the sweep kernels specialised for this circuit's structure are "
+                                "compiled once (cold_specialisation_ms, first planning) and reused"},
                 "gpu_launches": int(launches), "clocks": clk}
     return line
 

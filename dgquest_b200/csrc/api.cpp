@@ -27,6 +27,7 @@
 #include "dgq.h"
 #include "dag.h"
 #include "ir.h"
+#include "jit.h"
 #include "kernels.h"
 #include "planner.h"
 #include "rng.h"
@@ -184,6 +185,7 @@ struct QuregState {
 
     int tileBitsSetting = 0;  // 0 = cost model
     std::vector<dgq::TileProgram> planned;
+    std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)
     int plannedTileBits = 0;
     dgq_plan_stats stats{};
 };
@@ -265,7 +267,22 @@ int chooseTileBits(QuregState &s) {
 }
 
 // ---------------------------------------------------------------- execution
-bool planPending(QuregState &s, const char *func) {
+// Registers with at least this many address bits get runtime-specialised
+// sweep kernels (DGQ_JIT_MIN_BITS overrides): below it a sweep takes
+// microseconds and the generic tile kernel beats a compile.
+std::atomic<int> g_jitMinBits{-1};
+
+int jitMinBits() {
+    int v = g_jitMinBits.load();
+    if (v < 0) {
+        const char *e = getenv("DGQ_JIT_MIN_BITS");
+        v = e ? atoi(e) : 22;
+        g_jitMinBits.store(v);
+    }
+    return v;
+}
+
+bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.planned.clear();
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
@@ -300,6 +317,22 @@ bool planPending(QuregState &s, const char *func) {
         st.sweeps = 1;
     }
     s.plannedTileBits = W;
+    s.plannedFns.assign(s.planned.size(), nullptr);
+    s.stats.jitCompiled = 0;
+    s.stats.jitReused = 0;
+    s.stats.jitMillis = 0.0;
+    if (specialise && dgq::jitEnabled() && s.numBits >= jitMinBits()) {
+        std::vector<std::string> sources;
+        sources.reserve(s.planned.size());
+        for (const auto &p : s.planned) sources.push_back(dgq::generateSweepSource(p, W));
+        dgq::JitStats js;
+        std::string jerr;
+        if (!dgq::jitGetKernels(sources, s.plannedFns, &js, &jerr))
+            return raise(E_UNSUPPORTED, func, jerr.c_str());
+        s.stats.jitCompiled = js.compiled;
+        s.stats.jitReused = js.reused;
+        s.stats.jitMillis = js.compileMillis;
+    }
     s.stats.sweeps = st.sweeps;
     s.stats.phases = st.phases;
     s.stats.ops = st.ops;
@@ -319,8 +352,11 @@ bool planPending(QuregState &s, const char *func) {
 }
 
 bool launchPlanned(QuregState &s, const char *func) {
-    for (const auto &p : s.planned) {
-        if (!cudaOk(dgq::launchTile(s.dState, s.plannedTileBits, p, s.stream), func)) return false;
+    for (size_t i = 0; i < s.planned.size(); i++) {
+        const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+        const cudaError_t e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, s.planned[i], s.stream)
+                                 : dgq::launchTile(s.dState, s.plannedTileBits, s.planned[i], s.stream);
+        if (!cudaOk(e, func)) return false;
         g_launches++;
     }
     return true;
@@ -1210,9 +1246,57 @@ int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, 
     }
     s.initPending = true;
     s.initKind = dgq::INIT_CLASSICAL;
-    if (!planPending(s, __func__)) return -1;
+    if (!planPending(s, __func__, false)) return -1;
     *out = s.stats;
     return 0;
+}
+
+int dgq_setSpecialisationMinBits(int minBits) {
+    const int prev = jitMinBits();
+    g_jitMinBits.store(minBits < 0 ? 22 : minBits);
+    return prev;
+}
+
+int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
+                    const uint64_t *controlMasks, const double *operands, int sweep, char *buf, int len) {
+    if (numQubits < 1 || numQubits > dgq::kMaxStateBits - 2 || count < 0 || !buf || len <= 0) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
+    }
+    QuregState s;
+    s.numQubits = numQubits;
+    s.numBits = std::max(numQubits, dgq::kMinTileBits);
+    resetMapping(s);
+    s.tileBitsSetting = tileBits;
+    for (int i = 0; i < count; i++) {
+        Gate g;
+        g.type = (dgq::GateType) types[i];
+        g.targetMask = targetMasks[i];
+        g.controlMask = controlMasks[i];
+        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
+        s.pending.push_back(g);
+    }
+    s.initPending = true;
+    s.initKind = dgq::INIT_CLASSICAL;
+    const bool ok = planPending(s, __func__, false);
+    if (!ok) return -1;
+    if (sweep < 0 || sweep >= (int) s.planned.size()) return (int) s.planned.size();
+    const std::string src = dgq::generateSweepSource(s.planned[(size_t) sweep], s.plannedTileBits);
+    std::strncpy(buf, src.c_str(), (size_t) len - 1);
+    buf[len - 1] = '\0';
+    return (int) src.size() < len ? (int) s.planned.size() : -2;
+}
+
+int dgq_compileSweepSource(const char *source, char *log, int len) {
+    if (!source) return -1;
+    std::vector<char> cubin;
+    std::string lg;
+    const bool ok = dgq::jitCompileOnly(source, cubin, lg);
+    if (log && len > 0) {
+        std::strncpy(log, lg.c_str(), (size_t) len - 1);
+        log[len - 1] = '\0';
+    }
+    return ok ? (int) cubin.size() : -1;
 }
 
 }  // extern "C"

@@ -1,0 +1,369 @@
+// jit.cpp -- see jit.h.
+#include "jit.h"
+
+#include <nvrtc.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <mutex>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+
+namespace dgq {
+
+// Embedded texts of tile_program.h and jit_prelude.cuh (generated at build
+// time into jit_sources.inc as kTileProgramSource / kJitPreludeSource).
+#include "jit_sources.inc"
+
+namespace {
+
+const char *kernelKindName(int code) {
+    if (code < KC_M2I) return "jM2R";
+    if (code < KC_M2C) return "jM2I";
+    if (code < KC_X) return "jM2C";
+    if (code < KC_Y) return "jX";
+    if (code < KC_YC) return "jY";
+    if (code < KC_Z2R) return "jYC";
+    return "jZ2R";
+}
+
+void emitOp(std::ostringstream &o, const KOp &op) {
+    const unsigned cr = op.ctrlReg;
+    const int off = op.coef;
+    std::ostringstream body;
+    if (op.code < KC_Z2T) {
+        const int base = (op.code / 8) * 8;
+        const int kk = op.code - base;
+        const int k = kk & 3;
+        const bool ctrl = kk >= 4;
+        const char *fn = kernelKindName(op.code);
+        const bool coef = !(op.code >= KC_X && op.code < KC_Z2R);
+        body << "dgq::" << fn << "<" << k << ", " << (ctrl ? "true" : "false") << ", " << cr << "u>(a"
+             << (coef ? ", prog.coef + " + std::to_string(off) : std::string()) << ");";
+    } else if (op.code == KC_Z2T || op.code == KC_Z2T + 1) {
+        const bool ctrl = op.code == KC_Z2T + 1;
+        std::ostringstream sel;
+        bool any = false;
+        if (op.selLoc) {
+            sel << "((loc & " << op.selLoc << "u) != 0u)";
+            any = true;
+        }
+        if (op.selCta >= 0) {
+            sel << (any ? " || " : "") << "(((cta >> " << (int) op.selCta << ") & 1u) != 0u)";
+            any = true;
+        }
+        if (!any) sel << "false";
+        body << "{ const bool b_ = " << sel.str() << "; dgq::jPH<" << (ctrl ? "true" : "false") << ", " << cr
+             << "u>(a, prog.coef[" << off << "], b_ ? prog.coef[" << off + 1 << "] : -prog.coef[" << off + 1
+             << "]); }";
+    } else if (op.code == KC_PH || op.code == KC_PH + 1) {
+        body << "dgq::jPH<" << (op.code == KC_PH + 1 ? "true" : "false") << ", " << cr << "u>(a, prog.coef[" << off
+             << "], prog.coef[" << off + 1 << "]);";
+    } else if (op.code == KC_NEG || op.code == KC_NEG + 1) {
+        body << "dgq::jNEG<" << (op.code == KC_NEG + 1 ? "true" : "false") << ", " << cr << "u>(a);";
+    } else if (op.code == KC_MULI || op.code == KC_MULI + 1) {
+        body << "dgq::jMULI<" << (op.code == KC_MULI + 1 ? "true" : "false") << ", " << cr << "u>(a);";
+    } else if (op.code == KC_MULNI || op.code == KC_MULNI + 1) {
+        body << "dgq::jMULNI<" << (op.code == KC_MULNI + 1 ? "true" : "false") << ", " << cr << "u>(a);";
+    } else if (op.code >= KC_DENSE && op.code < KC_DENSE + 4) {
+        body << "dgq::jDense<" << (op.code - KC_DENSE + 1) << ", " << cr << "u>(a, prog.coef + " << off << ");";
+    } else if (op.code >= KC_RY1 && op.code < KC_H1) {
+        static const char *names[4] = {"jRY1", "jRY2", "jRX1", "jRX2"};
+        body << "dgq::" << names[(op.code - KC_RY1) / 4] << "<" << (op.code - KC_RY1) % 4 << ">(a, prog.coef + " << off
+             << ");";
+    } else if (op.code >= KC_H1 && op.code < KC_H1 + 4) {
+        body << "dgq::jH1<" << op.code - KC_H1 << ">(a);";
+    } else if (op.code >= KC_PH1R && op.code < KC_PH1R + 4) {
+        body << "dgq::jPH1R<" << op.code - KC_PH1R << ">(a, prog.coef + " << off << ");";
+    } else if (op.code == KC_PH1T) {
+        std::ostringstream sel;
+        bool any = false;
+        if (op.selLoc) {
+            sel << "((loc & " << op.selLoc << "u) != 0u)";
+            any = true;
+        }
+        if (op.selCta >= 0) {
+            sel << (any ? " || " : "") << "(((cta >> " << (int) op.selCta << ") & 1u) != 0u)";
+            any = true;
+        }
+        body << "if (" << (any ? sel.str() : std::string("false")) << ") dgq::jPH<false, 0u>(a, prog.coef[" << off
+             << "], prog.coef[" << off + 1 << "]);";
+    }
+    if (op.thrCtl) {
+        std::ostringstream cond;
+        bool any = false;
+        if (op.ctrlLoc) {
+            cond << "((loc & " << op.ctrlLoc << "u) == " << op.ctrlLoc << "u)";
+            any = true;
+        }
+        if (op.ctrlCta) {
+            cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+            any = true;
+        }
+        o << "    if (" << (any ? cond.str() : std::string("true")) << ") { " << body.str() << " }\n";
+    } else {
+        o << "    " << body.str() << "\n";
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// Address of thread `tid`'s element 0 and of the 4 register bits in a
+// direct phase layout (thread bits 0..4 = address bits 0..4).
+void emitDirectAddressing(std::ostringstream &o, const KPhase &ph, int W, const char *gt, const char *rb) {
+    o << "    const uint64_t " << gt << " = dgq::jCtaBase(prog, cta, W) | (uint64_t) (tid & 31u)";
+    for (int i = kCoalescedBits; i < W - kRegBits; i++)
+        o << " | ((uint64_t) ((tid >> " << i << ") & 1u) << prog.highPos[" << (int) ph.thrPos[i] - kCoalescedBits << "])";
+    o << ";\n";
+    o << "    const uint64_t " << rb << "[4] = {";
+    for (int b = 0; b < kRegBits; b++)
+        o << (b ? ", " : "") << "1ULL << prog.highPos[" << (int) ph.regPos[b] - kCoalescedBits << "]";
+    o << "};\n";
+}
+
+}  // namespace
+
+std::string generateSweepSource(const TileProgram &prog, int W) {
+    const int T = 1 << (W - kRegBits);
+    const int minBlocks = 65536 / (128 * T) > 0 ? 65536 / (128 * T) : 1;
+    std::ostringstream o;
+    o << "#include \"jit_prelude.cuh\"\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << minBlocks
+      << ") dgq_sweep(double2 *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
+    o << "    constexpr int W = " << W << ";\n";
+    o << "    extern __shared__ double2 sm[];\n";
+    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x;\n";
+    o << "    (void) cta;\n";
+    o << "    double2 a[dgq::kRegs];\n";
+    const int np = prog.numPhases;
+    const bool firstDirect = np > 0 && prog.phases[0].direct;
+    const bool lastDirect = np > 0 && prog.phases[np - 1].direct;
+    if (firstDirect) {
+        emitDirectAddressing(o, prog.phases[0], W, "gIn", "rbIn");
+        o << "    dgq::jLoadDirect<" << prog.initKind << ", " << (prog.hasRestrict ? "true" : "false")
+          << ">(st, prog, gIn, rbIn, a);\n";
+    } else {
+        o << "    dgq::jLoad<W, " << prog.initKind << ", " << (prog.hasRestrict ? "true" : "false")
+          << ">(st, prog, tid, cta, a);\n";
+        if (np > 0) o << "    dgq::jToSmem<W>(sm, tid, a);\n    __syncthreads();\n";
+    }
+    for (int p = 0; p < np; p++) {
+        const KPhase &ph = prog.phases[p];
+        const bool readSmem = !(p == 0 && firstDirect);
+        const bool writeSmem = !(p == np - 1 && lastDirect);
+        o << "  {\n    const uint32_t loc = 0u";
+        for (int i = 0; i < W - kRegBits; i++) o << " | (((tid >> " << i << ") & 1u) << " << (int) ph.thrPos[i] << ")";
+        o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc);\n    (void) sb;\n";
+        if (readSmem)
+            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = sm[sb ^ " << ph.regOff[j] << "u];\n";
+        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOp(o, prog.ops[k]);
+        if (writeSmem) {
+            for (int j = 0; j < kRegs; j++) o << "    sm[sb ^ " << ph.regOff[j] << "u] = a[" << j << "];\n";
+            o << "    __syncthreads();\n";
+        }
+        o << "  }\n";
+    }
+    if (np > 0 && !lastDirect) o << "    dgq::jFromSmem<W>(sm, tid, a);\n";
+    if (prog.hasGlobal) o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";
+    if (lastDirect) {
+        emitDirectAddressing(o, prog.phases[np - 1], W, "gOut", "rbOut");
+        o << "    dgq::jStoreDirect(st, gOut, rbOut, a);\n}\n";
+    } else {
+        o << "    dgq::jStore<W>(st, prog, tid, cta, a);\n}\n";
+    }
+    return o.str();
+}
+
+bool jitEnabled() {
+    static int enabled = -1;
+    if (enabled < 0) {
+        const char *e = getenv("DGQ_JIT");
+        enabled = (e && e[0] == '0') ? 0 : 1;
+    }
+    return enabled == 1;
+}
+
+namespace {
+
+// Driver entry points through the runtime (no link-time dependency on the
+// driver library, so the library also loads on hosts without a GPU).
+struct Driver {
+    CUresult (*moduleLoadData)(CUmodule *, const void *) = nullptr;
+    CUresult (*moduleGetFunction)(CUfunction *, CUmodule, const char *) = nullptr;
+    CUresult (*funcSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+    CUresult (*launchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                             CUstream, void **, void **) = nullptr;
+    CUresult (*getErrorString)(CUresult, const char **) = nullptr;
+    bool ok = false;
+};
+
+const Driver &driver() {
+    static Driver d;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        auto get = [](const char *name, void **fn) {
+            cudaDriverEntryPointQueryResult q;
+            return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess && *fn != nullptr;
+        };
+        d.ok = get("cuModuleLoadData", (void **) &d.moduleLoadData) &&
+               get("cuModuleGetFunction", (void **) &d.moduleGetFunction) &&
+               get("cuFuncSetAttribute", (void **) &d.funcSetAttribute) &&
+               get("cuLaunchKernel", (void **) &d.launchKernel) &&
+               get("cuGetErrorString", (void **) &d.getErrorString);
+    });
+    return d;
+}
+
+struct CacheEntry {
+    std::string source;
+    CUmodule module;
+    CUfunction fn;
+};
+
+std::mutex g_cacheMutex;
+std::unordered_map<size_t, std::vector<CacheEntry>> g_cache;
+
+CUfunction cacheFind(const std::string &src) {
+    std::lock_guard<std::mutex> lk(g_cacheMutex);
+    auto it = g_cache.find(std::hash<std::string>()(src));
+    if (it == g_cache.end()) return nullptr;
+    for (const auto &e : it->second)
+        if (e.source == src) return e.fn;
+    return nullptr;
+}
+
+bool compileOne(const std::string &src, std::vector<char> &cubin, std::string &log) {
+    nvrtcProgram prog;
+    const char *headers[2] = {kTileProgramSource, kJitPreludeSource};
+    const char *names[2] = {"tile_program.h", "jit_prelude.cuh"};
+    if (nvrtcCreateProgram(&prog, src.c_str(), "dgq_sweep.cu", 2, headers, names) != NVRTC_SUCCESS) {
+        log = "nvrtcCreateProgram failed";
+        return false;
+    }
+    const char *opts[] = {"-arch=sm_100a", "--std=c++17", "-default-device", "-lineinfo"};
+    const nvrtcResult r = nvrtcCompileProgram(prog, 4, opts);
+    size_t logSize = 0;
+    nvrtcGetProgramLogSize(prog, &logSize);
+    if (logSize > 1) {
+        log.resize(logSize);
+        nvrtcGetProgramLog(prog, &log[0]);
+    }
+    if (r != NVRTC_SUCCESS) {
+        nvrtcDestroyProgram(&prog);
+        return false;
+    }
+    size_t n = 0;
+    nvrtcGetCUBINSize(prog, &n);
+    cubin.resize(n);
+    nvrtcGetCUBIN(prog, cubin.data());
+    nvrtcDestroyProgram(&prog);
+    return true;
+}
+
+}  // namespace
+
+bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log) {
+    return compileOne(src, cubin, log);
+}
+
+bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfunction> &out, JitStats *stats,
+                   std::string *err) {
+    const auto t0 = std::chrono::steady_clock::now();
+    out.assign(sources.size(), nullptr);
+    std::vector<size_t> todo;
+    // identical sources in one batch compile once
+    std::unordered_map<std::string, size_t> firstOf;
+    std::vector<size_t> dupOf(sources.size(), (size_t) -1);
+    int reused = 0;
+    for (size_t i = 0; i < sources.size(); i++) {
+        out[i] = cacheFind(sources[i]);
+        if (out[i]) {
+            reused++;
+            continue;
+        }
+        auto it = firstOf.find(sources[i]);
+        if (it != firstOf.end()) {
+            dupOf[i] = it->second;
+            continue;
+        }
+        firstOf[sources[i]] = i;
+        todo.push_back(i);
+    }
+    std::vector<std::vector<char>> cubins(sources.size());
+    std::vector<std::string> logs(sources.size());
+    std::vector<char> ok(sources.size(), 0);
+    if (!todo.empty()) {
+        unsigned hw = std::thread::hardware_concurrency();
+        if (hw == 0) hw = 4;
+        const unsigned nthreads = std::min<unsigned>(hw, (unsigned) todo.size());
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t t; (t = next.fetch_add(1)) < todo.size();) {
+                const size_t i = todo[t];
+                ok[i] = compileOne(sources[i], cubins[i], logs[i]) ? 1 : 0;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nthreads; t++) pool.emplace_back(worker);
+        worker();
+        for (auto &th : pool) th.join();
+    }
+    bool allOk = true;
+    const Driver &drv = driver();
+    if (!todo.empty() && !drv.ok) {
+        if (err) *err = "CUDA driver entry points unavailable";
+        return false;
+    }
+    for (size_t i : todo) {
+        if (!ok[i]) {
+            if (err) *err = "NVRTC compile failed: " + logs[i].substr(0, 2000);
+            allOk = false;
+            continue;
+        }
+        CUmodule mod = nullptr;
+        CUfunction fn = nullptr;
+        CUresult r = drv.moduleLoadData(&mod, cubins[i].data());
+        if (r == CUDA_SUCCESS) r = drv.moduleGetFunction(&fn, mod, "dgq_sweep");
+        if (r != CUDA_SUCCESS) {
+            const char *msg = nullptr;
+            drv.getErrorString(r, &msg);
+            if (err) *err = std::string("loading a specialised kernel failed: ") + (msg ? msg : "?");
+            allOk = false;
+            continue;
+        }
+        out[i] = fn;
+        std::lock_guard<std::mutex> lk(g_cacheMutex);
+        g_cache[std::hash<std::string>()(sources[i])].push_back({sources[i], mod, fn});
+    }
+    for (size_t i = 0; i < sources.size(); i++)
+        if (dupOf[i] != (size_t) -1) out[i] = out[dupOf[i]];
+    if (stats) {
+        stats->compiled = (int) todo.size();
+        stats->reused = reused;
+        stats->compileMillis = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return allOk;
+}
+
+cudaError_t launchJitSweep(CUfunction fn, double2 *st, int W, const TileProgram &prog, cudaStream_t s) {
+    const int T = 1 << (W - kRegBits);
+    const unsigned smem = (unsigned) (sizeof(double2) << W);
+    // one attribute call per function: cheap and idempotent
+    const Driver &drv = driver();
+    if (!drv.ok) return cudaErrorNotSupported;
+    CUresult r = drv.funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int) smem);
+    if (r != CUDA_SUCCESS) return cudaErrorLaunchFailure;
+    const unsigned grid = 1u << (prog.numBits - W);
+    void *args[2] = {(void *) &st, (void *) &prog};
+    r = drv.launchKernel(fn, grid, 1, 1, (unsigned) T, 1, 1, smem, (CUstream) s, args, nullptr);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+}  // namespace dgq

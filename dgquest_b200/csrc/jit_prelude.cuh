@@ -1,0 +1,356 @@
+// jit_prelude.cuh -- device code shared by the runtime-specialised sweep
+// kernels (codegen.cpp writes one kernel per sweep program and NVRTC
+// compiles it for sm_100a together with this header and tile_program.h).
+//
+// The generated kernel is the tile kernel of kernels.cu with everything
+// that is fixed by the plan turned into compile-time constants: the phase
+// layouts (register and thread bits, shared-memory offsets), the sequence
+// of operations with their target register bits and control masks, and the
+// positions of their coefficients in the parameter block. The amplitudes
+// then flow from one operation to the next as plain SSA values, with no
+// dispatch and no merge points, and the coefficients are read straight from
+// the constant bank. Only values that change between runs of the same
+// structure (coefficients, address-bit positions, initial index, collapse
+// mask) stay in the TileProgram parameter.
+#pragma once
+
+#include "tile_program.h"
+
+namespace dgq {
+
+__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u); }
+
+// ---------------------------------------------------------------- operations
+#define DGQJ_PAIR_LOOP(K, CTRL, cr, ...)                                        \
+    _Pragma("unroll") for (int p_ = 0; p_ < kRegs / 2; p_++) {                  \
+        const int j0 = ((p_ >> (K)) << ((K) + 1)) | (p_ & ((1 << (K)) - 1));    \
+        const int j1 = j0 | (1 << (K));                                         \
+        if ((CTRL) && (j0 & (cr)) != (cr)) continue;                            \
+        double2 &x = a[j0];                                                     \
+        double2 &y = a[j1];                                                     \
+        __VA_ARGS__                                                             \
+    }
+
+#define DGQJ_AMP_LOOP(CTRL, cr, ...)                                            \
+    _Pragma("unroll") for (int j = 0; j < kRegs; j++) {                         \
+        if ((CTRL) && (j & (cr)) != (cr)) continue;                             \
+        double2 &x = a[j];                                                      \
+        __VA_ARGS__                                                             \
+    }
+
+// [[m0, m1], [m2, m3]] real
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jM2R(double2 (&a)[kRegs], const double *c) {
+    const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        const double t0 = m2 * x.x, t1 = m2 * x.y, u0 = m1 * y.x, u1 = m1 * y.y;
+        x.x = fma(m0, x.x, u0);
+        x.y = fma(m0, x.y, u1);
+        y.x = fma(m3, y.x, t0);
+        y.y = fma(m3, y.y, t1);
+    })
+}
+
+// [[m0, i m1], [i m2, m3]] with m real
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jM2I(double2 (&a)[kRegs], const double *c) {
+    const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        const double t0 = m2 * x.y, t1 = m2 * x.x, u0 = m1 * y.y, u1 = m1 * y.x;
+        x.x = fma(m0, x.x, -u0);
+        x.y = fma(m0, x.y, u1);
+        y.x = fma(m3, y.x, -t0);
+        y.y = fma(m3, y.y, t1);
+    })
+}
+
+// general complex 2x2, row-major (re, im)
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jM2C(double2 (&a)[kRegs], const double *c) {
+    const double u0 = c[0], u1 = c[1], u2 = c[2], u3 = c[3], u4 = c[4], u5 = c[5], u6 = c[6], u7 = c[7];
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        double xr = u0 * x.x;
+        xr = fma(-u1, x.y, xr);
+        xr = fma(u2, y.x, xr);
+        xr = fma(-u3, y.y, xr);
+        double xi = u0 * x.y;
+        xi = fma(u1, x.x, xi);
+        xi = fma(u2, y.y, xi);
+        xi = fma(u3, y.x, xi);
+        double yr = u4 * x.x;
+        yr = fma(-u5, x.y, yr);
+        yr = fma(u6, y.x, yr);
+        yr = fma(-u7, y.y, yr);
+        double yi = u4 * x.y;
+        yi = fma(u5, x.x, yi);
+        yi = fma(u6, y.y, yi);
+        yi = fma(u7, y.x, yi);
+        x = make_double2(xr, xi);
+        y = make_double2(yr, yi);
+    })
+}
+
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jX(double2 (&a)[kRegs]) {
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        const double2 t = x;
+        x = y;
+        y = t;
+    })
+}
+
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jY(double2 (&a)[kRegs]) {
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        const double2 t = x;
+        x = make_double2(y.y, -y.x);
+        y = make_double2(-t.y, t.x);
+    })
+}
+
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jYC(double2 (&a)[kRegs]) {
+    DGQJ_PAIR_LOOP(K, CTRL, CR, {
+        const double2 t = x;
+        x = make_double2(-y.y, y.x);
+        y = make_double2(t.y, -t.x);
+    })
+}
+
+__device__ __forceinline__ void jPhaseMul(double2 &x, double cs, double sn) {
+    const double t = sn * x.y, u = sn * x.x;
+    x.x = fma(cs, x.x, -t);
+    x.y = fma(cs, x.y, u);
+}
+
+// diag(c - i s, c + i s) selected by register bit K
+template <int K, bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jZ2R(double2 (&a)[kRegs], const double *c) {
+    const double cs = c[0], sn = c[1];
+    DGQJ_AMP_LOOP(CTRL, CR, { jPhaseMul(x, cs, ((j >> K) & 1) ? sn : -sn); })
+}
+
+template <bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jPH(double2 (&a)[kRegs], double cs, double sn) {
+    DGQJ_AMP_LOOP(CTRL, CR, { jPhaseMul(x, cs, sn); })
+}
+
+template <bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jNEG(double2 (&a)[kRegs]) {
+    DGQJ_AMP_LOOP(CTRL, CR, { x = make_double2(-x.x, -x.y); })
+}
+
+template <bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jMULI(double2 (&a)[kRegs]) {
+    DGQJ_AMP_LOOP(CTRL, CR, { x = make_double2(-x.y, x.x); })
+}
+
+template <bool CTRL, uint32_t CR>
+__device__ __forceinline__ void jMULNI(double2 (&a)[kRegs]) {
+    DGQJ_AMP_LOOP(CTRL, CR, { x = make_double2(x.y, -x.x); })
+}
+
+// Factored uncontrolled gates (the scalar factor is applied once per sweep)
+template <int K>
+__device__ __forceinline__ void jRY1(double2 (&a)[kRegs], const double *c) {
+    const double t = c[0];
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const double2 x0 = x;
+        x = make_double2(fma(-t, y.x, x0.x), fma(-t, y.y, x0.y));
+        y = make_double2(fma(t, x0.x, y.x), fma(t, x0.y, y.y));
+    })
+}
+template <int K>
+__device__ __forceinline__ void jRY2(double2 (&a)[kRegs], const double *c) {
+    const double u = c[0];
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const double2 x0 = x;
+        x = make_double2(fma(u, x0.x, -y.x), fma(u, x0.y, -y.y));
+        y = make_double2(fma(u, y.x, x0.x), fma(u, y.y, x0.y));
+    })
+}
+template <int K>
+__device__ __forceinline__ void jRX1(double2 (&a)[kRegs], const double *c) {
+    const double t = c[0];
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const double2 x0 = x;
+        x = make_double2(fma(t, y.y, x0.x), fma(-t, y.x, x0.y));
+        y = make_double2(fma(t, x0.y, y.x), fma(-t, x0.x, y.y));
+    })
+}
+template <int K>
+__device__ __forceinline__ void jRX2(double2 (&a)[kRegs], const double *c) {
+    const double u = c[0];
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const double2 x0 = x;
+        x = make_double2(fma(u, x0.x, y.y), fma(u, x0.y, -y.x));
+        y = make_double2(fma(u, y.x, x0.y), fma(u, y.y, -x0.x));
+    })
+}
+template <int K>
+__device__ __forceinline__ void jH1(double2 (&a)[kRegs]) {
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const double2 x0 = x;
+        x = make_double2(x0.x + y.x, x0.y + y.y);
+        y = make_double2(x0.x - y.x, x0.y - y.y);
+    })
+}
+// phase (cs + i sn) on the amplitudes whose register bit K is 1
+template <int K>
+__device__ __forceinline__ void jPH1R(double2 (&a)[kRegs], const double *c) {
+    const double cs = c[0], sn = c[1];
+#pragma unroll
+    for (int j = 0; j < kRegs; j++)
+        if ((j >> K) & 1) jPhaseMul(a[j], cs, sn);
+}
+__device__ __forceinline__ void jGlobal(double2 (&a)[kRegs], double gr, double gi) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const double2 x = a[j];
+        a[j] = make_double2(fma(gr, x.x, -gi * x.y), fma(gr, x.y, gi * x.x));
+    }
+}
+
+template <int KK, uint32_t CR>
+__device__ __forceinline__ void jDense(double2 (&a)[kRegs], const double *m) {
+    constexpr int D = 1 << KK;
+#pragma unroll
+    for (int g = 0; g < (kRegs >> KK); g++) {
+        const int base = g << KK;
+        if ((base & CR) != CR) continue;
+        double2 v[D];
+#pragma unroll
+        for (int c = 0; c < D; c++) v[c] = a[base + c];
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+            double re = 0.0, im = 0.0;
+#pragma unroll
+            for (int c = 0; c < D; c++) {
+                const double mr = m[2 * (r * D + c)], mi = m[2 * (r * D + c) + 1];
+                re = fma(mr, v[c].x, re);
+                re = fma(-mi, v[c].y, re);
+                im = fma(mr, v[c].y, im);
+                im = fma(mi, v[c].x, im);
+            }
+            a[base + r] = make_double2(re, im);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tile I/O
+// Canonical element (tid, j) of the tile sits at tile-local index
+// tid + T * j: lanes cover the 5 lowest address bits, j the top 4 tile bits.
+template <int W>
+__device__ __forceinline__ uint64_t jBase(const TileProgram &prog, uint32_t tid, uint32_t cta) {
+    uint64_t t = tid & 31u;
+    const int nCta = prog.numBits - W;
+    for (int i = 0; i < nCta; i++) t |= (uint64_t) ((cta >> i) & 1u) << prog.ctaPos[i];
+#pragma unroll
+    for (int i = 0; i < W - 9; i++) t |= (uint64_t) ((tid >> (5 + i)) & 1u) << prog.highPos[i];
+    return t;
+}
+
+template <int W>
+__device__ __forceinline__ uint64_t jIndex(const TileProgram &prog, uint64_t base, int j) {
+    uint64_t g = base;
+    if (j & 1) g |= 1ULL << prog.highPos[W - 9];
+    if (j & 2) g |= 1ULL << prog.highPos[W - 8];
+    if (j & 4) g |= 1ULL << prog.highPos[W - 7];
+    if (j & 8) g |= 1ULL << prog.highPos[W - 6];
+    return g;
+}
+
+template <int W, int INIT, bool RESTRICT>
+__device__ __forceinline__ void jLoad(const double2 *__restrict__ st, const TileProgram &prog, uint32_t tid,
+                                      uint32_t cta, double2 (&a)[kRegs]) {
+    const uint64_t base = jBase<W>(prog, tid, cta);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const uint64_t g = jIndex<W>(prog, base, j);
+        double2 v;
+        if (INIT == INIT_NONE) {
+            v = st[g];
+        } else if (INIT == INIT_CLASSICAL) {
+            v = make_double2(g == prog.initIndex ? 1.0 : 0.0, 0.0);
+        } else if (INIT == INIT_PLUS) {
+            v = make_double2((g >> prog.numReal) == 0ULL ? prog.initAmp : 0.0, 0.0);
+        } else {
+            v = make_double2(0.0, 0.0);
+        }
+        if (RESTRICT) {
+            const bool keep = (g & prog.restrictMask) == prog.restrictValue;
+            const double sc = prog.restrictScale;
+            v = keep ? make_double2(v.x * sc, v.y * sc) : make_double2(0.0, 0.0);
+        }
+        a[j] = v;
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void jStore(double2 *__restrict__ st, const TileProgram &prog, uint32_t tid, uint32_t cta,
+                                       const double2 (&a)[kRegs]) {
+    const uint64_t base = jBase<W>(prog, tid, cta);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) st[jIndex<W>(prog, base, j)] = a[j];
+}
+
+// Direct layouts: thread bits 0..4 are address bits 0..4; the other
+// thread bits and the 4 register bits are given as address-bit values.
+template <int INIT, bool RESTRICT>
+__device__ __forceinline__ void jLoadDirect(const double2 *__restrict__ st, const TileProgram &prog, uint64_t gt,
+                                            const uint64_t (&rb)[kRegBits], double2 (&a)[kRegs]) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const uint64_t g = gt | ((j & 1) ? rb[0] : 0ULL) | ((j & 2) ? rb[1] : 0ULL) | ((j & 4) ? rb[2] : 0ULL) |
+                           ((j & 8) ? rb[3] : 0ULL);
+        double2 v;
+        if (INIT == INIT_NONE) {
+            v = st[g];
+        } else if (INIT == INIT_CLASSICAL) {
+            v = make_double2(g == prog.initIndex ? 1.0 : 0.0, 0.0);
+        } else if (INIT == INIT_PLUS) {
+            v = make_double2((g >> prog.numReal) == 0ULL ? prog.initAmp : 0.0, 0.0);
+        } else {
+            v = make_double2(0.0, 0.0);
+        }
+        if (RESTRICT) {
+            const bool keep = (g & prog.restrictMask) == prog.restrictValue;
+            const double sc = prog.restrictScale;
+            v = keep ? make_double2(v.x * sc, v.y * sc) : make_double2(0.0, 0.0);
+        }
+        a[j] = v;
+    }
+}
+
+__device__ __forceinline__ void jStoreDirect(double2 *__restrict__ st, uint64_t gt, const uint64_t (&rb)[kRegBits],
+                                             const double2 (&a)[kRegs]) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const uint64_t g = gt | ((j & 1) ? rb[0] : 0ULL) | ((j & 2) ? rb[1] : 0ULL) | ((j & 4) ? rb[2] : 0ULL) |
+                           ((j & 8) ? rb[3] : 0ULL);
+        st[g] = a[j];
+    }
+}
+
+__device__ __forceinline__ uint64_t jCtaBase(const TileProgram &prog, uint32_t cta, int W) {
+    uint64_t t = 0;
+    const int nCta = prog.numBits - W;
+    for (int i = 0; i < nCta; i++) t |= (uint64_t) ((cta >> i) & 1u) << prog.ctaPos[i];
+    return t;
+}
+
+template <int W>
+__device__ __forceinline__ void jToSmem(double2 *sm, uint32_t tid, const double2 (&a)[kRegs]) {
+    constexpr uint32_t T = 1u << (W - kRegBits);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) sm[swz(tid + T * (uint32_t) j)] = a[j];
+}
+
+template <int W>
+__device__ __forceinline__ void jFromSmem(const double2 *sm, uint32_t tid, double2 (&a)[kRegs]) {
+    constexpr uint32_t T = 1u << (W - kRegBits);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) a[j] = sm[swz(tid + T * (uint32_t) j)];
+}
+
+}  // namespace dgq

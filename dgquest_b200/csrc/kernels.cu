@@ -173,6 +173,60 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, doubl
             });
             break;
         }
+        case KOP_RY1: {
+            const double t = c[0];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
+                const double2 x0 = x;
+                x = make_double2(fma(-t, y.x, x0.x), fma(-t, y.y, x0.y));
+                y = make_double2(fma(t, x0.x, y.x), fma(t, x0.y, y.y));
+            }));
+            break;
+        }
+        case KOP_RY2: {
+            const double u = c[0];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
+                const double2 x0 = x;
+                x = make_double2(fma(u, x0.x, -y.x), fma(u, x0.y, -y.y));
+                y = make_double2(fma(u, y.x, x0.x), fma(u, y.y, x0.y));
+            }));
+            break;
+        }
+        case KOP_RX1: {
+            const double t = c[0];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
+                const double2 x0 = x;
+                x = make_double2(fma(t, y.y, x0.x), fma(-t, y.x, x0.y));
+                y = make_double2(fma(t, x0.y, y.x), fma(-t, x0.x, y.y));
+            }));
+            break;
+        }
+        case KOP_RX2: {
+            const double u = c[0];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
+                const double2 x0 = x;
+                x = make_double2(fma(u, x0.x, y.y), fma(u, x0.y, -y.x));
+                y = make_double2(fma(u, y.x, x0.y), fma(u, y.y, -x0.x));
+            }));
+            break;
+        }
+        case KOP_H1:
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
+                const double2 x0 = x;
+                x = make_double2(x0.x + y.x, x0.y + y.y);
+                y = make_double2(x0.x - y.x, x0.y - y.y);
+            }));
+            break;
+        case KOP_PH1: {
+            const double cs = c[0], sn = c[1];
+            if (op.code == KC_PH1T) {
+                const bool bit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
+                if (bit) forAll(a, 0u, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
+            } else {
+                const uint32_t sr = 1u << op.k;
+                forAll(a, sr, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
+            }
+            break;
+        }
         case KOP_DENSE:
             switch (op.k) {
                 case 1: denseApply<1>(a, cr, c); break;
@@ -261,6 +315,11 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
         }
 #pragma unroll
         for (int j = 0; j < kRegs; j++) a[j] = sm[swz(tid + (uint32_t) (T * j))];
+    }
+    if (prog.hasGlobal) {
+        const double gr = prog.globalRe, gi = prog.globalIm;
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) a[j] = make_double2(gr * a[j].x - gi * a[j].y, gr * a[j].y + gi * a[j].x);
     }
 #pragma unroll
     for (int j = 0; j < kRegs; j++) st[gidx(j)] = a[j];

@@ -83,6 +83,7 @@ struct PhaseLayout {
     int regPos[kRegBits];
     int thrPos[kMaxThreadBits];
     uint32_t regLocalMask = 0;
+    bool direct = false;
 };
 
 // Register bits: `front` first (dense-gate target order), then the other
@@ -113,6 +114,15 @@ PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int
     std::vector<int> thr;
     for (int p = 0; p < tileBits; p++)
         if (!((used >> p) & 1u)) thr.push_back(p);
+    L.direct = (used & ((1u << kCoalescedBits) - 1)) == 0;
+    if (L.direct) {
+        // lanes on tile bits 0..4 (address bits 0..4): the phase can read and
+        // write HBM directly in 512-byte runs; bits 0..2 have distinct
+        // classes mod 3, so its shared-memory accesses stay conflict-free
+        int i = 0;
+        for (int p : thr) L.thrPos[i++] = p;
+        return L;
+    }
     std::vector<int> lanes, rest;
     int classes = 0;
     for (int p : thr) {
@@ -149,6 +159,12 @@ double opFlopsPerAmp(const KOp &op) {
         case KOP_Z2: f = 6.0; break;
         case KOP_M2C: f = 14.0; break;
         case KOP_DENSE: f = 8.0 * (double) (1 << op.k) - 2.0; break;
+        case KOP_RY1:
+        case KOP_RY2:
+        case KOP_RX1:
+        case KOP_RX2: f = 4.0; break;   // one FMA per output component
+        case KOP_H1: f = 2.0; break;    // one add per output component
+        case KOP_PH1: f = 3.0; break;   // a complex multiply on half of the amplitudes
         default: f = 0.0; break;
     }
     const int c = __builtin_popcount(op.ctrlReg) + __builtin_popcount(op.ctrlLoc) + __builtin_popcount(op.ctrlCta);
@@ -157,6 +173,7 @@ double opFlopsPerAmp(const KOp &op) {
 
 void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out) {
     std::memset(&out, 0, sizeof(out));
+    out.globalRe = 1.0;
     out.numBits = numBits;
     out.numReal = numReal;
     out.initKind = hdr.initKind;
@@ -222,6 +239,9 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         std::memset(&p, 0, sizeof(p));
         p.numBits = numBits;
         p.numReal = numReal;
+        p.globalRe = 1.0;
+        p.globalIm = 0.0;
+        p.hasGlobal = 0;
         if (isFirst) {
             p.initKind = first.initKind;
             p.initIndex = first.initIndex;
@@ -244,9 +264,16 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
 
     for (const Phase &ph : phases) {
         const PhaseLayout L = makeLayout(ph.front, ph.targetsLocal, tileBits);
-        // encode the phase's ops into a scratch list first
+        // encode the phase's ops into a scratch list first; uncontrolled
+        // rotations leave their scalar factor in (phRe, phIm)
         std::vector<KOp> ops;
         std::vector<double> coef;
+        double phRe = 1.0, phIm = 0.0;
+        auto scaleBy = [&](double fr, double fi) {
+            const double r = phRe * fr - phIm * fi, i = phRe * fi + phIm * fr;
+            phRe = r;
+            phIm = i;
+        };
         for (const Gate &g : ph.gates) {
             KOp op;
             std::memset(&op, 0, sizeof(op));
@@ -285,6 +312,24 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                 op.kind = KOP_PH;
                 coef.push_back(std::cos(g.op[0]));
                 coef.push_back(std::sin(g.op[0]));
+            } else if (g.type == OP_ROTATE_Z && g.controlMask == 0) {
+                // diag(e^{-ia}, e^{ia}) = e^{-ia} diag(1, e^{2ia})
+                op.kind = KOP_PH1;
+                coef.push_back(std::cos(2.0 * g.op[0]));
+                coef.push_back(std::sin(2.0 * g.op[0]));
+                scaleBy(std::cos(g.op[0]), -std::sin(g.op[0]));
+                const Split s = splitMask(g.targetMask, tm);
+                if (s.tileLocal) {
+                    const uint8_t r = regSpace(s.tileLocal, L);
+                    if (r) {
+                        op.k = (uint8_t) __builtin_ctz(r);
+                        selIsReg = true;
+                    } else {
+                        op.selLoc = (uint16_t) s.tileLocal;
+                    }
+                } else {
+                    op.selCta = (int8_t) __builtin_ctz(s.cta);
+                }
             } else if (g.type == OP_ROTATE_Z) {
                 op.kind = KOP_Z2;
                 coef.push_back(std::cos(g.op[0]));
@@ -313,26 +358,41 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     return false;
                 }
                 op.k = (uint8_t) k;
+                const bool free = g.controlMask == 0;
                 switch (g.type) {
+                    case OP_HADAMARD:
+                        if (!free) {
+                            op.kind = KOP_M2R;
+                            coef.insert(coef.end(), {kRsqrt2, kRsqrt2, kRsqrt2, -kRsqrt2});
+                        } else {
+                            op.kind = KOP_H1;
+                            scaleBy(kRsqrt2, 0.0);
+                        }
+                        break;
+                    case OP_ROTATE_Y:
+                    case OP_ROTATE_X: {
+                        const double cs = std::cos(g.op[0]), sn = std::sin(g.op[0]);
+                        const bool isY = g.type == OP_ROTATE_Y;
+                        if (!free) {
+                            op.kind = isY ? KOP_M2R : KOP_M2I;
+                            if (isY)
+                                coef.insert(coef.end(), {cs, -sn, sn, cs});
+                            else
+                                coef.insert(coef.end(), {cs, -sn, -sn, cs});
+                        } else if (std::fabs(cs) >= std::fabs(sn)) {
+                            op.kind = isY ? KOP_RY1 : KOP_RX1;
+                            coef.push_back(sn / cs);
+                            scaleBy(cs, 0.0);
+                        } else {
+                            op.kind = isY ? KOP_RY2 : KOP_RX2;
+                            coef.push_back(cs / sn);
+                            scaleBy(sn, 0.0);
+                        }
+                        break;
+                    }
                     case OP_PAULI_X: op.kind = KOP_X; break;
                     case OP_PAULI_Y: op.kind = KOP_Y; break;
                     case OP_PAULI_Y_CONJ: op.kind = KOP_YC; break;
-                    case OP_HADAMARD:
-                        op.kind = KOP_M2R;
-                        coef.insert(coef.end(), {kRsqrt2, kRsqrt2, kRsqrt2, -kRsqrt2});
-                        break;
-                    case OP_ROTATE_X: {
-                        op.kind = KOP_M2I;
-                        const double cs = std::cos(g.op[0]), sn = std::sin(g.op[0]);
-                        coef.insert(coef.end(), {cs, -sn, -sn, cs});
-                        break;
-                    }
-                    case OP_ROTATE_Y: {
-                        op.kind = KOP_M2R;
-                        const double cs = std::cos(g.op[0]), sn = std::sin(g.op[0]);
-                        coef.insert(coef.end(), {cs, -sn, sn, cs});
-                        break;
-                    }
                     default: {
                         double m[8];
                         gateMatrix(g, m);
@@ -366,6 +426,12 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     case KOP_MULI: op.code = (uint8_t) (KC_MULI + rc); break;
                     case KOP_MULNI: op.code = (uint8_t) (KC_MULNI + rc); break;
                     case KOP_DENSE: op.code = (uint8_t) (KC_DENSE + op.k - 1); break;
+                    case KOP_RY1: op.code = (uint8_t) (KC_RY1 + op.k); break;
+                    case KOP_RY2: op.code = (uint8_t) (KC_RY2 + op.k); break;
+                    case KOP_RX1: op.code = (uint8_t) (KC_RX1 + op.k); break;
+                    case KOP_RX2: op.code = (uint8_t) (KC_RX2 + op.k); break;
+                    case KOP_H1: op.code = (uint8_t) (KC_H1 + op.k); break;
+                    case KOP_PH1: op.code = (uint8_t) (selIsReg ? KC_PH1R + op.k : KC_PH1T); break;
                     default: break;
                 }
                 ops.push_back(op);
@@ -381,9 +447,17 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             prog = newProgram(false);
             numCoef = 0;
         }
+        if (phRe != 1.0 || phIm != 0.0) {
+            const double gr = prog->globalRe, gi = prog->globalIm;
+            prog->globalRe = gr * phRe - gi * phIm;
+            prog->globalIm = gr * phIm + gi * phRe;
+            prog->hasGlobal = 1;
+        }
         KPhase &kp = prog->phases[prog->numPhases++];
         std::memset(&kp, 0, sizeof(kp));
         for (int i = 0; i < tileBits - kRegBits; i++) kp.thrPos[i] = (uint8_t) L.thrPos[i];
+        for (int b = 0; b < kRegBits; b++) kp.regPos[b] = (uint8_t) L.regPos[b];
+        kp.direct = L.direct ? 1 : 0;
         kp.opBegin = (uint16_t) prog->numOps;
         for (KOp o : ops) {
             o.coef = (uint16_t) (o.coef + numCoef);

@@ -43,7 +43,15 @@ enum KOpKind : uint8_t {
     KOP_MULNI = 8, // multiply by -i
     KOP_PH = 9,    // multiply by (c + i s)
     KOP_Z2 = 10,   // multiply by (c - i s) when the selector bit is 0, (c + i s) when 1
-    KOP_DENSE = 11 // dense 2^k x 2^k on register bits 0..k-1 (k = op.k), coefficients re/im
+    KOP_DENSE = 11, // dense 2^k x 2^k on register bits 0..k-1 (k = op.k), coefficients re/im
+    // Uncontrolled gates with their scalar factor moved into the sweep's
+    // global factor (TileProgram::globalRe/Im), leaving unit entries:
+    KOP_RY1 = 12,  // [[1, -t], [t, 1]]        (Ry with |cos| >= |sin|, t = tan)
+    KOP_RY2 = 13,  // [[u, -1], [1, u]]        (Ry with |sin| > |cos|, u = cot)
+    KOP_RX1 = 14,  // [[1, -i t], [-i t, 1]]   (Rx, t = tan)
+    KOP_RX2 = 15,  // [[u, -i], [-i, u]]       (Rx, u = cot)
+    KOP_H1 = 16,   // [[1, 1], [1, -1]]        (Hadamard without 1/sqrt 2)
+    KOP_PH1 = 17   // multiply by (c + i s) where the selector bit is 1 (Rz without e^{-i a})
 };
 
 // Dispatch codes of the tile kernel: one straight-line case per
@@ -63,7 +71,14 @@ enum KCode : uint8_t {
     KC_MULI = 62,  // +1 controlled
     KC_MULNI = 64, // +1 controlled
     KC_DENSE = 66, // + (k - 1), k = 1..4
-    KC_COUNT = 70
+    KC_RY1 = 70,   // + k; never controlled
+    KC_RY2 = 74,
+    KC_RX1 = 78,
+    KC_RX2 = 82,
+    KC_H1 = 86,
+    KC_PH1R = 90,  // + k: selector = register bit k
+    KC_PH1T = 94,  // selector is a thread/CTA bit
+    KC_COUNT = 95
 };
 
 // 16 bytes; every field is read uniformly by all threads of the CTA.
@@ -82,7 +97,9 @@ struct KOp {
 
 struct KPhase {
     uint8_t thrPos[kMaxThreadBits];  // tile-local bit of thread-index bit i
-    uint8_t pad[3];
+    uint8_t direct;                  // 1: thread bits 0..4 are tile bits 0..4 (coalesced global I/O)
+    uint8_t regPos[kRegBits];        // tile-local bit of register bit b
+    uint8_t pad[2];
     uint16_t opBegin, opEnd;
     uint16_t regOff[kRegs];  // swizzled shared-memory offset of register j
 };
@@ -101,6 +118,9 @@ struct TileProgram {
     int32_t numReal;   // qubits the user sees (<= numBits)
     int32_t initKind;
     int32_t hasRestrict;
+    int32_t hasGlobal;       // multiply every amplitude by (globalRe + i globalIm) before the store
+    int32_t pad1;
+    double globalRe, globalIm;
     uint64_t initIndex;
     double initAmp;
     uint64_t restrictMask;   // lazy measurement collapse applied at load:

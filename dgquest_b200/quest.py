@@ -59,6 +59,9 @@ class PlanStats(Structure):
         ("numBits", ctypes.c_int32),
         ("flopsPerAmp", c_double),
         ("planMillis", c_double),
+        ("jitCompiled", ctypes.c_int32),
+        ("jitReused", ctypes.c_int32),
+        ("jitMillis", c_double),
     ]
 
 
@@ -146,6 +149,10 @@ _SIGS = {
     "dgq_getLaunchCount": (c_int64, []),
     "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
     "dgq_measureFp64Peak": (I, [P(D)]),
+    "dgq_sweepSource": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I,
+                            ctypes.c_char_p, I]),
+    "dgq_compileSweepSource": (I, [ctypes.c_char_p, ctypes.c_char_p, I]),
+    "dgq_setSpecialisationMinBits": (I, [I]),
     "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),

@@ -42,7 +42,10 @@ typedef struct dgq_plan_stats {
     int32_t tileBits;      /* W used */
     int32_t numBits;       /* address bits of the state buffer */
     double flopsPerAmp;    /* algorithmic FP64 flops per amplitude, whole plan */
-    double planMillis;     /* host planning time */
+    double planMillis;     /* host planning time (including kernel specialisation) */
+    int32_t jitCompiled;   /* sweep kernels compiled for this plan */
+    int32_t jitReused;     /* sweep kernels found already compiled */
+    double jitMillis;      /* time spent specialising kernels */
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
@@ -104,6 +107,20 @@ int dgq_calcProbOfAllZeroNoAlloc(const void *deviceState, int numBits, double *d
 int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
                   const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
                   int32_t *numMerged);
+
+/* Registers with at least minBits address bits run runtime-specialised
+ * sweep kernels (default 22, or DGQ_JIT_MIN_BITS; DGQ_JIT=0 disables
+ * specialisation). Negative restores the default. Returns the previous value. */
+int dgq_setSpecialisationMinBits(int minBits);
+
+/* Host-only view of the runtime specialisation: the CUDA source generated
+ * for sweep `sweep` of the plan of the given gates (same encoding as
+ * dgq_planGates; returns the number of sweeps, -2 if buf is too small), and
+ * an NVRTC compile of such a source for sm_100a (returns the cubin size, or
+ * -1 with the compiler log in `log`). Neither needs a GPU. */
+int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
+                    const uint64_t *controlMasks, const double *operands, int sweep, char *buf, int len);
+int dgq_compileSweepSource(const char *source, char *log, int len);
 
 #ifdef __cplusplus
 }

@@ -187,3 +187,45 @@ def test_plan_fuses_and_counts(quest, env):
     assert st.gates <= len(ops)
     assert st.numBits == n
     quest.destroyQureg(q, env)
+
+
+@pytest.fixture
+def specialised(quest):
+    prev = quest.dgq_setSpecialisationMinBits(1)
+    yield
+    quest.dgq_setSpecialisationMinBits(prev)
+
+
+@pytest.mark.parametrize("tile_bits", [9, 10, 11, 12])
+def test_specialised_kernels_match_oracle(quest, env, specialised, tile_bits):
+    n = 15
+    ops = np.concatenate([C.mixed_ops(n, 250, 500 + tile_bits), C.random_layers(n, 4, 7)])
+    amps, p0, _, st = run_product(quest, env, n, ops, tile_bits=tile_bits)
+    assert st.jitCompiled + st.jitReused == st.sweeps
+    ref_amps, ref_p0, _ = oracle.run(n, ops)
+    check(amps, p0, ref_amps, ref_p0)
+
+
+def test_specialised_dense_and_measure(quest, env, specialised):
+    n = 13
+    gen = np.random.default_rng(11)
+    u = C.random_unitary(gen, 16)
+    pre = C.mixed_ops(n, 80, 12)
+    post = np.concatenate([C.mixed_ops(n, 80, 13), C.OpList().add(C.MEASURE, 2).add(C.MEASURE, 9).array()])
+    q = quest.createQureg(n, env)
+    quest.seed([5, 6])
+    C.replay(q, pre)
+    m = quest.matrixN(u)
+    quest.multiQubitUnitary(q, quest.int_array([1, 7, 3, 12]), 4, m)
+    quest.destroyComplexMatrixN(m)
+    out = C.replay(q, post)
+    amps = quest.state_vector(q)
+    st = quest.plan_stats(q)
+    quest.destroyQureg(q, env)
+    o = oracle.Oracle(n)
+    o.seed([5, 6])
+    o.apply(pre)
+    o.multi_qubit_unitary([1, 7, 3, 12], u)
+    ref_out = o.apply(post)
+    assert out == ref_out
+    assert np.abs(amps - o.amps()).max() <= TOL

@@ -1,0 +1,63 @@
+"""CPU tests of the host planner and the runtime specialisation: plans for
+the headline circuits, DAG merge rules, and NVRTC compiles of generated
+sweep kernels for sm_100a (no GPU is used)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from dgquest_b200 import circuits as C
+from dgquest_b200 import ir
+from dgquest_b200 import quest as Q
+
+P = ctypes.POINTER
+
+
+def test_random_circuit_plan_shape():
+    ops = C.random_layers(30, 20, C.config_seed(2))
+    prev = None
+    for w in (9, 10, 11, 12):
+        st = ir.plan(ops, 30, w)
+        assert st.tileBits == w and st.numBits == 30
+        assert st.gates == 900
+        if prev is not None:
+            assert st.sweeps <= prev  # wider tiles never need more sweeps here
+        prev = st.sweeps
+    assert 15 <= prev <= 30
+
+
+def test_merge_rules():
+    # T T -> S ; S S -> Z ; Z Z -> nothing ; Rx(a) Rx(b) -> Rx(a+b) ; H H -> nothing ; X then U -> U
+    b = C.OpList()
+    b.add(C.T, 0).add(C.T, 0)            # -> S (type 2)
+    b.add(C.H, 1).add(C.H, 1)            # cancel
+    b.add(C.RX, 2, p=(0.3,)).add(C.RX, 2, p=(0.4,))  # one Rx
+    b.add(C.Z, 3).add(C.Z, 3)            # cancel
+    b.add(C.PHASE, 4, p=(0.2,)).add(C.T, 4)  # one phase shift
+    st, merged = ir.plan(b.array(), 10, 9, want_merged=True)
+    assert sorted(merged) == sorted([2, 15, 8])
+
+
+def _sources(ops, n, w):
+    t, tm, cm, o = ir.ops_to_ir(ops, n)
+    buf = ctypes.create_string_buffer(1 << 20)
+    args = (n, w, len(t), t.ctypes.data_as(P(ctypes.c_int32)), tm.ctypes.data_as(P(ctypes.c_uint64)),
+            cm.ctypes.data_as(P(ctypes.c_uint64)), o.ctypes.data_as(P(ctypes.c_double)))
+    count = Q.dgq_sweepSource(*args, 0, buf, len(buf))
+    out = []
+    for s in range(count):
+        Q.dgq_sweepSource(*args, s, buf, len(buf))
+        out.append(buf.value)
+    return out
+
+
+@pytest.mark.parametrize("w", [9, 12])
+def test_generated_sweeps_compile(w):
+    ops = np.concatenate([C.mixed_ops(14, 150, 3, kinds=[k for k in range(26) if k != C.MEASURE]),
+                          C.random_layers(14, 2, 5)])
+    srcs = _sources(ops, 14, w)
+    assert len(srcs) >= 1
+    log = ctypes.create_string_buffer(1 << 16)
+    for s in srcs[:3]:
+        size = Q.dgq_compileSweepSource(s, log, len(log))
+        assert size > 0, log.value.decode()
