@@ -227,6 +227,101 @@ std::vector<Gate> GateDag::takeBlock(int budget, u64 &mask, size_t maxGates) {
     return taken;
 }
 
+// Insertion order is a topological order, so one forward pass decides
+// which gates are reachable inside `allowed`.
+size_t GateDag::countAllowed(u64 allowed) const {
+    std::vector<char> ok(nodes_.size(), 0);
+    size_t count = 0;
+    for (size_t i = 0; i < nodes_.size(); i++) {
+        const Node &nd = nodes_[i];
+        if (!nd.alive) continue;
+        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
+        if (cost & ~allowed) continue;
+        bool all = true;
+        for (int p : nd.prev)
+            if (!ok[(size_t) p]) {
+                all = false;
+                break;
+            }
+        if (!all) continue;
+        ok[i] = 1;
+        count++;
+    }
+    return count;
+}
+
+u64 GateDag::frontierTargets(u64 allowed) const {
+    std::vector<char> ok(nodes_.size(), 0);
+    u64 frontier = 0;
+    for (size_t i = 0; i < nodes_.size(); i++) {
+        const Node &nd = nodes_[i];
+        if (!nd.alive) continue;
+        bool all = true;
+        for (int p : nd.prev)
+            if (!ok[(size_t) p]) {
+                all = false;
+                break;
+            }
+        if (!all) continue;
+        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
+        if (cost & ~allowed) {
+            frontier |= cost & ~allowed;
+            continue;
+        }
+        ok[i] = 1;
+    }
+    return frontier;
+}
+
+std::vector<u64> GateDag::frontierSets(u64 allowed) const {
+    std::vector<char> ok(nodes_.size(), 0);
+    std::vector<u64> sets;
+    for (size_t i = 0; i < nodes_.size(); i++) {
+        const Node &nd = nodes_[i];
+        if (!nd.alive) continue;
+        bool all = true;
+        for (int p : nd.prev)
+            if (!ok[(size_t) p]) {
+                all = false;
+                break;
+            }
+        if (!all) continue;
+        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
+        const u64 missing = cost & ~allowed;
+        if (missing) {
+            if (std::find(sets.begin(), sets.end(), missing) == sets.end()) sets.push_back(missing);
+            continue;
+        }
+        ok[i] = 1;
+    }
+    return sets;
+}
+
+std::vector<Gate> GateDag::takeAllowed(u64 allowed) {
+    std::vector<char> ok(nodes_.size(), 0);
+    std::vector<Gate> taken, rest;
+    for (size_t i = 0; i < nodes_.size(); i++) {
+        const Node &nd = nodes_[i];
+        if (!nd.alive) continue;
+        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
+        bool all = (cost & ~allowed) == 0;
+        for (int p : nd.prev)
+            if (all && !ok[(size_t) p]) all = false;
+        if (all) {
+            ok[i] = 1;
+            taken.push_back(nd.g);
+        } else {
+            rest.push_back(nd.g);
+        }
+    }
+    nodes_.clear();
+    front_.clear();
+    alive_ = 0;
+    for (auto &st : qubitStack_) st.clear();
+    for (const Gate &g : rest) add(g);
+    return taken;
+}
+
 std::vector<Gate> GateDag::gatesInOrder() const {
     std::vector<Gate> out;
     for (const auto &n : nodes_)

@@ -39,6 +39,16 @@ public:
 
     std::vector<Gate> gatesInOrder() const;
 
+    // Gates of the largest dependency-closed set whose non-diagonal targets
+    // all lie in `allowed` (count only / remove and return them).
+    size_t countAllowed(u64 allowed) const;
+    std::vector<Gate> takeAllowed(u64 allowed);
+    // Non-diagonal target bits of the gates that could run next if their
+    // targets were allowed (frontier of the allowed-closed set).
+    u64 frontierTargets(u64 allowed) const;
+    // The distinct sets of missing target bits of those next gates.
+    std::vector<u64> frontierSets(u64 allowed) const;
+
 private:
     struct Node {
         Gate g;

@@ -114,6 +114,25 @@ void emitOp(std::ostringstream &o, const KOp &op) {
 
 namespace {
 
+// Address bit of tile-local bit l, as a CUDA expression.
+std::string addrBitExpr(int l) {
+    if (l < kCoalescedBits) return std::to_string(l);
+    return "prog.highPos[" + std::to_string(l - kCoalescedBits) + "]";
+}
+
+// Address bits of this thread's element 0 and of the 4 register bits in
+// the layout of phase ph (any layout).
+void emitLayoutAddressing(std::ostringstream &o, const KPhase &ph, int W, const char *ctaExpr, const char *gt,
+                          const char *rb) {
+    o << "    const uint64_t " << gt << " = dgq::jCtaBase(prog, " << ctaExpr << ", W)";
+    for (int i = 0; i < W - kRegBits; i++)
+        o << " | ((uint64_t) ((tid >> " << i << ") & 1u) << " << addrBitExpr(ph.thrPos[i]) << ")";
+    o << ";\n";
+    o << "    const uint64_t " << rb << "[4] = {";
+    for (int b = 0; b < kRegBits; b++) o << (b ? ", " : "") << "1ULL << " << addrBitExpr(ph.regPos[b]);
+    o << "};\n";
+}
+
 // Address of thread `tid`'s element 0 and of the 4 register bits in a
 // direct phase layout (thread bits 0..4 = address bits 0..4).
 void emitDirectAddressing(std::ostringstream &o, const KPhase &ph, int W, const char *gt, const char *rb) {
@@ -129,9 +148,101 @@ void emitDirectAddressing(std::ostringstream &o, const KPhase &ph, int W, const 
 
 }  // namespace
 
-std::string generateSweepSource(const TileProgram &prog, int W) {
+// CTAs per SM the kernel is compiled for: 16 warps per SM at 128 registers
+// a thread by default; DGQ_JIT_CTAS_PER_SM overrides (register cap
+// 65536 / (threads x CTAs)).
+static int ctasPerSm(int T) {
+    static int env = -2;
+    if (env == -2) {
+        const char *e = getenv("DGQ_JIT_CTAS_PER_SM");
+        env = e ? atoi(e) : -1;
+    }
+    if (env > 0) return env;
+    return 65536 / (128 * T) > 0 ? 65536 / (128 * T) : 1;
+}
+
+// Off by default: measured on B200 at 30 qubits, one 256-thread CTA per SM
+// with two 64 KiB buffers hides less latency than two plain CTAs per SM
+// (204 ms vs 158 ms per circuit). DGQ_JIT_PERSISTENT=1 selects it.
+bool jitPersistent() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("DGQ_JIT_PERSISTENT");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
+
+// Persistent form: each CTA walks tiles blockIdx.x, +gridDim.x, ...; the
+// next tile streams into the other of two shared buffers by cp.async while
+// the current one runs its phases, so HBM reads overlap the FP64 work.
+static std::string generatePersistent(const TileProgram &prog, int W) {
     const int T = 1 << (W - kRegBits);
-    const int minBlocks = 65536 / (128 * T) > 0 ? 65536 / (128 * T) : 1;
+    const int np = prog.numPhases;
+    const bool load = prog.initKind == INIT_NONE;
+    const bool lastDirect = prog.phases[np - 1].direct;
+    std::ostringstream o;
+    o << "#include \"jit_prelude.cuh\"\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", 1"
+      << ") dgq_sweep(double2 *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
+    o << "    constexpr int W = " << W << ";\n";
+    o << "    constexpr uint32_t TILE = 1u << W;\n";
+    o << "    extern __shared__ double2 smAll[];\n";
+    o << "    const uint32_t tid = threadIdx.x;\n";
+    o << "    const uint32_t numTiles = 1u << (prog.numBits - W);\n";
+    o << "    double2 a[dgq::kRegs];\n";
+    if (load) o << "    if (blockIdx.x < numTiles) dgq::jPrefetch<W>(st, prog, tid, blockIdx.x, smAll);\n    dgq::jCpAsyncCommit();\n";
+    o << "    int it = 0;\n";
+    o << "    for (uint32_t cta = blockIdx.x; cta < numTiles; cta += gridDim.x, it++) {\n";
+    o << "    double2 *sm = smAll + (size_t) (it & 1) * TILE;\n";
+    o << "    __syncthreads();\n";
+    if (load) {
+        o << "    { const uint32_t nx = cta + gridDim.x; if (nx < numTiles) dgq::jPrefetch<W>(st, prog, tid, nx, smAll + "
+             "(size_t) ((it + 1) & 1) * TILE); }\n";
+        o << "    dgq::jCpAsyncCommit();\n    dgq::jCpAsyncWait1();\n    __syncthreads();\n";
+    }
+    for (int p = 0; p < np; p++) {
+        const KPhase &ph = prog.phases[p];
+        const bool writeSmem = !(p == np - 1 && lastDirect);
+        o << "  {\n    const uint32_t loc = 0u";
+        for (int i = 0; i < W - kRegBits; i++) o << " | (((tid >> " << i << ") & 1u) << " << (int) ph.thrPos[i] << ")";
+        o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc);\n";
+        if (p == 0 && !load) {
+            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = make_double2(0.0, 0.0);\n";
+        } else {
+            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = sm[sb ^ " << ph.regOff[j] << "u];\n";
+        }
+        if (p == 0 && (!load || prog.hasRestrict)) {
+            emitLayoutAddressing(o, ph, W, "cta", "gF", "rbF");
+            o << "    dgq::jFixup<" << prog.initKind << ", " << (prog.hasRestrict ? "true" : "false")
+              << ">(prog, gF, rbF, a);\n";
+        }
+        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOp(o, prog.ops[k]);
+        if (writeSmem) {
+            for (int j = 0; j < kRegs; j++) o << "    sm[sb ^ " << ph.regOff[j] << "u] = a[" << j << "];\n";
+            o << "    __syncthreads();\n";
+        }
+        o << "  }\n";
+    }
+    if (!lastDirect) o << "    dgq::jFromSmem<W>(sm, tid, a);\n";
+    if (prog.hasGlobal) o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";
+    if (lastDirect) {
+        o << "  {\n";
+        emitDirectAddressing(o, prog.phases[np - 1], W, "gOut", "rbOut");
+        o << "    dgq::jStoreDirect(st, gOut, rbOut, a);\n  }\n";
+    } else {
+        o << "    dgq::jStore<W>(st, prog, tid, cta, a);\n";
+    }
+    o << "    }\n";
+    if (load) o << "    dgq::jCpAsyncWait0();\n";
+    o << "}\n";
+    return o.str();
+}
+
+std::string generateSweepSource(const TileProgram &prog, int W) {
+    if (jitPersistent() && prog.numPhases > 0) return generatePersistent(prog, W);
+    const int T = 1 << (W - kRegBits);
+    const int minBlocks = ctasPerSm(T);
     std::ostringstream o;
     o << "#include \"jit_prelude.cuh\"\n";
     o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << minBlocks
@@ -200,6 +311,7 @@ struct Driver {
     CUresult (*launchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                              CUstream, void **, void **) = nullptr;
     CUresult (*getErrorString)(CUresult, const char **) = nullptr;
+    CUresult (*occupancy)(int *, CUfunction, int, size_t) = nullptr;
     bool ok = false;
 };
 
@@ -216,7 +328,8 @@ const Driver &driver() {
                get("cuModuleGetFunction", (void **) &d.moduleGetFunction) &&
                get("cuFuncSetAttribute", (void **) &d.funcSetAttribute) &&
                get("cuLaunchKernel", (void **) &d.launchKernel) &&
-               get("cuGetErrorString", (void **) &d.getErrorString);
+               get("cuGetErrorString", (void **) &d.getErrorString) &&
+               get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void **) &d.occupancy);
     });
     return d;
 }
@@ -354,13 +467,22 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
 
 cudaError_t launchJitSweep(CUfunction fn, double2 *st, int W, const TileProgram &prog, cudaStream_t s) {
     const int T = 1 << (W - kRegBits);
-    const unsigned smem = (unsigned) (sizeof(double2) << W);
+    const bool persistent = jitPersistent() && prog.numPhases > 0;
+    const unsigned smem = (unsigned) ((sizeof(double2) << W) * (persistent ? 2 : 1));
     // one attribute call per function: cheap and idempotent
     const Driver &drv = driver();
     if (!drv.ok) return cudaErrorNotSupported;
     CUresult r = drv.funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int) smem);
     if (r != CUDA_SUCCESS) return cudaErrorLaunchFailure;
-    const unsigned grid = 1u << (prog.numBits - W);
+    unsigned grid = 1u << (prog.numBits - W);
+    if (persistent) {
+        int perSm = 0, dev = 0, sms = 0;
+        if (drv.occupancy(&perSm, fn, T, smem) != CUDA_SUCCESS || perSm < 1) perSm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned cap = (unsigned) (perSm * sms);
+        if (grid > cap) grid = cap;
+    }
     void *args[2] = {(void *) &st, (void *) &prog};
     r = drv.launchKernel(fn, grid, 1, 1, (unsigned) T, 1, 1, smem, (CUstream) s, args, nullptr);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;

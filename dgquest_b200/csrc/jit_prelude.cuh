@@ -339,6 +339,55 @@ __device__ __forceinline__ uint64_t jCtaBase(const TileProgram &prog, uint32_t c
     return t;
 }
 
+// Global index of element j for a thread whose own address bits are gt and
+// whose register bits have the address-bit values rb (any layout).
+__device__ __forceinline__ uint64_t jIdx(uint64_t gt, const uint64_t (&rb)[kRegBits], int j) {
+    return gt | ((j & 1) ? rb[0] : 0ULL) | ((j & 2) ? rb[1] : 0ULL) | ((j & 4) ? rb[2] : 0ULL) | ((j & 8) ? rb[3] : 0ULL);
+}
+
+// In-register initial state / lazy collapse for elements whose global
+// indices are given by (gt, rb).
+template <int INIT, bool RESTRICT>
+__device__ __forceinline__ void jFixup(const TileProgram &prog, uint64_t gt, const uint64_t (&rb)[kRegBits],
+                                       double2 (&a)[kRegs]) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const uint64_t g = jIdx(gt, rb, j);
+        double2 v = a[j];
+        if (INIT == INIT_CLASSICAL) {
+            v = make_double2(g == prog.initIndex ? 1.0 : 0.0, 0.0);
+        } else if (INIT == INIT_PLUS) {
+            v = make_double2((g >> prog.numReal) == 0ULL ? prog.initAmp : 0.0, 0.0);
+        } else if (INIT == INIT_BLANK) {
+            v = make_double2(0.0, 0.0);
+        }
+        if (RESTRICT) {
+            const bool keep = (g & prog.restrictMask) == prog.restrictValue;
+            const double sc = prog.restrictScale;
+            v = keep ? make_double2(v.x * sc, v.y * sc) : make_double2(0.0, 0.0);
+        }
+        a[j] = v;
+    }
+}
+
+__device__ __forceinline__ void jCpAsync16(void *smemPtr, const void *gptr) {
+    const uint32_t s = (uint32_t) __cvta_generic_to_shared(smemPtr);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gptr) : "memory");
+}
+__device__ __forceinline__ void jCpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void jCpAsyncWait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void jCpAsyncWait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// cp.async of tile `cta`'s canonical elements into buffer buf
+template <int W>
+__device__ __forceinline__ void jPrefetch(const double2 *__restrict__ st, const TileProgram &prog, uint32_t tid,
+                                          uint32_t cta, double2 *buf) {
+    constexpr uint32_t T = 1u << (W - kRegBits);
+    const uint64_t base = jBase<W>(prog, tid, cta);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) jCpAsync16(&buf[swz(tid + T * (uint32_t) j)], st + jIndex<W>(prog, base, j));
+}
+
 template <int W>
 __device__ __forceinline__ void jToSmem(double2 *sm, uint32_t tid, const double2 (&a)[kRegs]) {
     constexpr uint32_t T = 1u << (W - kRegBits);

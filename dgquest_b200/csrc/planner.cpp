@@ -11,6 +11,44 @@ namespace dgq {
 
 static const double kRsqrt2 = 0.7071067811865475244008443621;
 
+// Block selection. dgQuEST's rule (DAG.cpp:219-259) walks the DAG depth
+// first and admits gates while the target union fits; the tile bits then
+// follow from the order of the walk. Here the tile's free bits are chosen
+// first: starting from the 5 coalesced bits, add one at a time the bit that
+// lets the most gates run (dependency-closed, non-diagonal targets inside
+// the tile), considering only bits some runnable-next gate targets, then
+// take every gate that fits. Phases inside a block use the same rule with
+// the 4 register bits.
+// Grows `mask` up to `budget` bits: each step adds the missing target bits
+// of one runnable-next gate, choosing the addition that lets the most gates
+// run (ties: fewer new bits; with preferHigh, bits above the 5 coalesced).
+static void growMask(const GateDag &dag, u64 &mask, int budget, bool preferHigh) {
+    const u64 low = (1ULL << kCoalescedBits) - 1;
+    while (popcount64(mask) < budget) {
+        const std::vector<u64> cands = dag.frontierSets(mask);
+        size_t best = 0;
+        u64 bestAdd = 0;
+        for (u64 add : cands) {
+            if (popcount64(mask | add) > budget) continue;
+            const size_t c = dag.countAllowed(mask | add);
+            bool better = c > best;
+            if (!better && c == best && bestAdd) {
+                const int pa = popcount64(add), pb = popcount64(bestAdd);
+                if (pa < pb)
+                    better = true;
+                else if (pa == pb && preferHigh && (bestAdd & low) && !(add & low))
+                    better = true;
+            }
+            if (better) {
+                best = c;
+                bestAdd = add;
+            }
+        }
+        if (!bestAdd) break;
+        mask |= bestAdd;
+    }
+}
+
 std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete) {
     std::vector<BlockPlan> blocks;
     if (complete) *complete = true;
@@ -20,11 +58,12 @@ std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, i
     const u64 all = numBits >= 64 ? ~0ULL : ((1ULL << numBits) - 1);
     while (!dag.empty()) {
         BlockPlan b;
-        u64 mask = seed;
-        b.gates = dag.takeBlock(tileBits, mask, 1u << 20);
+        u64 mask = seed & all;
+        growMask(dag, mask, tileBits, false);
         // pad to tileBits with the lowest unused bits from bit 5 upward
         for (int bit = kCoalescedBits; popcount64(mask) < tileBits && bit < numBits; bit++) mask |= 1ULL << bit;
         b.tileMask = mask & all;
+        b.gates = dag.takeAllowed(b.tileMask);
         if (b.gates.empty()) {
             // only a gate wider than the tile is left: not plannable here
             if (complete) *complete = false;
@@ -204,7 +243,13 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         for (const Gate &g : block.gates) dag.add(g);
         while (!dag.empty()) {
             u64 mask = 0;
-            std::vector<Gate> gs = dag.takeBlock(kRegBits, mask, 1u << 20);
+            growMask(dag, mask, kRegBits, true);
+            std::vector<Gate> gs = dag.takeAllowed(mask);
+            if (gs.empty()) {
+                // a multi-target gate wider than the register bits
+                u64 m2 = 0;
+                gs = dag.takeBlock(kRegBits, m2, 1u << 20);
+            }
             if (gs.empty()) {
                 if (err) *err = "a gate has more non-diagonal targets than the register tile holds";
                 return false;
