@@ -253,6 +253,35 @@ def run_gpu(args, world, rank, local):
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("tile_kernel_bytes_per_launch_n30")
+    # precision form: the same circuit on a complex64 register (8 GiB)
+    fp32 = None
+    if not args.no_fp32:
+        q32 = Q.dgq_createQuregF32(n, env)
+        s32 = torch.cuda.ExternalStream(Q.dgq_getStream(q32))
+        Q.initZeroState(q32)
+        C.replay(q32, ops)
+        Q.dgq_planPending(q32)
+        st32 = Q.plan_stats(q32)
+        for _ in range(args.warmup):
+            Q.dgq_launchPlanned(q32)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(s32)
+        for _ in range(args.steps):
+            Q.dgq_launchPlanned(q32)
+        f1.record(s32)
+        torch.cuda.synchronize()
+        ms32 = max_over_ranks(f0.elapsed_time(f1), world) / args.steps
+        # both registers now hold the circuit's final state (fresh run of the FP64 plan)
+        Q.initZeroState(q)
+        C.replay(q, ops)
+        fid = Q.calcFidelity(q, q32)
+        fp32 = {"ms_per_step": ms32, "circuits_per_s": world * 1000.0 / ms32, "speedup_vs_fp64": ms_step / ms32,
+                "fidelity_vs_fp64": fid, "dtype": "complex64 amplitudes, FP32 arithmetic (SIMT)",
+                "tile_bits": st32.tileBits, "sweeps": st32.sweeps,
+                "hbm_gbs": 2.0 * (1 << n) * 8 * st32.sweeps / (ms32 / 1000.0) / 1e9}
+        Q.destroyQureg(q32, env)
     Q.destroyQureg(q, env)
     Q.destroyQuESTEnv(env)
 
@@ -285,8 +314,28 @@ def run_gpu(args, world, rank, local):
                         "cold_specialisation_ms": st.jitMillis,
                         "note": "steady state: the sweep kernels specialised for this circuit's structure are "
                                 "compiled once (cold_specialisation_ms, first planning) and reused"},
-                "gpu_launches": int(launches), "clocks": clk}
+                "gpu_launches": int(launches), "clocks": clk, "fp32_form": fp32}
     return line
+
+
+def run_ncu_case(args):
+    """One plan of the random circuit on a small register, run twice (ncu: -s skips the first)."""
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    env = Q.createQuESTEnv()
+    q = Q.dgq_createQuregF32(args.qubits, env) if args.precision == 1 else Q.createQureg(args.qubits, env)
+    if args.tile_bits:
+        Q.dgq_setTileBits(q, args.tile_bits)
+    Q.dgq_setSpecialisationMinBits(1)
+    for _ in range(2):
+        Q.initZeroState(q)
+        C.replay(q, C.random_layers(args.qubits, args.depth, C.config_seed(2)))
+        Q.dgq_sync(q)
+    st = Q.plan_stats(q)
+    print(json.dumps({"case": "random", "qubits": args.qubits, "depth": args.depth, "tile_bits": st.tileBits,
+                      "sweeps": st.sweeps, "norm": Q.calcTotalProb(q)}))
+    Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
 
 
 def main():
@@ -302,7 +351,14 @@ def main():
     ap.add_argument("--ref-gates", type=int, default=8)
     ap.add_argument("--cpu-gates", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--precision", type=int, default=2, choices=[1, 2], help="--ncu-case register precision")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="run one small case once (for ncu captures): --qubits/--depth/--tile-bits, specialised kernels")
     args = ap.parse_args()
+    if args.ncu_case:
+        run_ncu_case(args)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "dgq" else args.warmup
 
     world, rank, local = dist_setup(args.gpus)

@@ -96,6 +96,7 @@ const char *errorMessage(int code) {
         case E_COLLAPSE_STATE_ZERO_PROB: return "Can't collapse to state with zero probability.";
         case E_INVALID_QUBIT_OUTCOME: return "Invalid measurement outcome -- must be either 0 or 1.";
         case E_DEFINED_ONLY_FOR_STATEVECS: return "Operation valid only for state-vectors.";
+        case E_MISMATCHING_QUREG_DIMENSIONS: return "Dimensions of the qubit registers don't match.";
         case E_INVALID_NUM_TARGETS: return "Invalid number of target qubits. Must be >0 and <=numQubits, and unique.";
         case E_SYS_TOO_BIG_FOR_DEVICE: return "The state-vector does not fit in free GPU memory.";
         case E_UNSUPPORTED: return "Operation not supported by this build.";
@@ -155,7 +156,8 @@ struct QuESTEnvValue {
 struct QuregState {
     int numQubits = 0;  // user-visible qubits
     int numBits = 0;    // address bits of the buffer (>= numQubits, >= kMinTileBits)
-    double2 *dState = nullptr;
+    bool single = false;  // complex64 amplitudes (float2) instead of complex128
+    void *dState = nullptr;
     cudaStream_t stream = nullptr;
 
     // recorded, not yet executed
@@ -182,6 +184,7 @@ struct QuregState {
     double *dPartial = nullptr;
     size_t partialCap = 0;
     double *dProbOut = nullptr;
+    double *dNorm = nullptr;  // complex64 renormalisation: two running sums of |a|^2
 
     int tileBitsSetting = 0;  // 0 = cost model
     std::vector<dgq::TileProgram> planned;
@@ -193,6 +196,8 @@ struct QuregState {
 namespace {
 
 QuregState *stateOf(const Qureg &q) { return q.state; }
+
+size_t ampBytes(const QuregState &s) { return s.single ? sizeof(float2) : sizeof(double2); }
 
 void resetMapping(QuregState &s) {
     for (int i = 0; i < 64; i++) {
@@ -247,7 +252,7 @@ double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, co
 }
 
 int chooseTileBits(QuregState &s) {
-    const int hi = std::min(dgq::kMaxTileBits, s.numBits);
+    const int hi = std::min(s.single ? dgq::kMaxTileBits : dgq::kMaxTileBitsF64, s.numBits);
     const int lo = dgq::kMinTileBits;
     if (s.tileBitsSetting > 0) return std::max(lo, std::min(hi, s.tileBitsSetting));
     if (const char *env = getenv("DGQ_TILE_BITS")) {
@@ -317,11 +322,24 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
         st.sweeps = 1;
     }
     s.plannedTileBits = W;
+    for (size_t i = 0; i < s.planned.size(); i++) {
+        dgq::TileProgram &p = s.planned[i];
+        p.isSingle = s.single ? 1 : 0;
+        if (s.single && p.numPhases > 0) {
+            // renormalise every sweep: sweep i divides by the norm sweep i-1 measured
+            p.renormOut = 1;
+            p.normOut = s.dNorm + (i & 1);
+            p.renormIn = (i > 0 && s.planned[i - 1].renormOut) ? 1 : 0;
+            p.normIn = s.dNorm + ((i + 1) & 1);
+        }
+    }
     s.plannedFns.assign(s.planned.size(), nullptr);
+    if (s.single && specialise && !dgq::jitEnabled())
+        return raise(E_UNSUPPORTED, func, "complex64 registers need runtime-specialised kernels (DGQ_JIT=0 is set)");
     s.stats.jitCompiled = 0;
     s.stats.jitReused = 0;
     s.stats.jitMillis = 0.0;
-    if (specialise && dgq::jitEnabled() && s.numBits >= jitMinBits()) {
+    if (specialise && dgq::jitEnabled() && (s.single || s.numBits >= jitMinBits())) {
         std::vector<std::string> sources;
         sources.reserve(s.planned.size());
         for (const auto &p : s.planned) sources.push_back(dgq::generateSweepSource(p, W));
@@ -354,8 +372,11 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
 bool launchPlanned(QuregState &s, const char *func) {
     for (size_t i = 0; i < s.planned.size(); i++) {
         const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+        if (s.planned[i].renormOut &&
+            !cudaOk(cudaMemsetAsync(s.planned[i].normOut, 0, sizeof(double), s.stream), func))
+            return false;
         const cudaError_t e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, s.planned[i], s.stream)
-                                 : dgq::launchTile(s.dState, s.plannedTileBits, s.planned[i], s.stream);
+                                 : dgq::launchTile((double2 *) s.dState, s.plannedTileBits, s.planned[i], s.stream);
         if (!cudaOk(e, func)) return false;
         g_launches++;
     }
@@ -388,7 +409,7 @@ bool ensureProbs(QuregState &s, const char *func) {
         if (!cudaOk(cudaMalloc(&s.dPartial, need * sizeof(double)), func)) return false;
         s.partialCap = need;
     }
-    if (!cudaOk(dgq::launchProb(s.dState, a, s.dPartial, s.dProbOut, s.stream), func)) return false;
+    if (!cudaOk(dgq::launchProb(s.dState, s.single, a, s.dPartial, s.dProbOut, s.stream), func)) return false;
     g_launches += 2;
     std::vector<double> out((size_t) nf + 1);
     if (!cudaOk(cudaMemcpyAsync(out.data(), s.dProbOut, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s.stream),
@@ -548,35 +569,39 @@ void destroyQuESTEnv(QuESTEnv env) { delete env.value; }
 int getQuEST_PREC(void) { return (int) (sizeof(qreal) / 4); }
 
 // ---------------------------------------------------------------- registers
-Qureg createQureg(int numQubits, QuESTEnv env) {
+}  // extern "C"
+
+static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const char *func) {
     Qureg q;
     std::memset(&q, 0, sizeof(q));
     if (numQubits <= 0) {
-        raise(E_INVALID_NUM_QUBITS, __func__);
+        raise(E_INVALID_NUM_QUBITS, func);
         return q;
     }
     if (numQubits > dgq::kMaxStateBits - 2) {
-        raise(E_SYS_TOO_BIG_FOR_DEVICE, __func__);
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, func);
         return q;
     }
     auto *s = new QuregState();
     s->numQubits = numQubits;
     s->numBits = std::max(numQubits, dgq::kMinTileBits);
+    s->single = single;
     resetMapping(*s);
-    const size_t bytes = sizeof(double2) << s->numBits;
+    const size_t bytes = ampBytes(*s) << s->numBits;
     size_t freeB = 0, totalB = 0;
-    if (!cudaOk(cudaMemGetInfo(&freeB, &totalB), __func__)) {
+    if (!cudaOk(cudaMemGetInfo(&freeB, &totalB), func)) {
         delete s;
         return q;
     }
     if (bytes + (64u << 20) > freeB) {
         delete s;
-        raise(E_SYS_TOO_BIG_FOR_DEVICE, __func__);
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, func);
         return q;
     }
-    if (!cudaOk(cudaMalloc(&s->dState, bytes), __func__) ||
-        !cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), __func__) ||
-        !cudaOk(cudaMalloc(&s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1)), __func__)) {
+    if (!cudaOk(cudaMalloc(&s->dState, bytes), func) ||
+        !cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func) ||
+        !cudaOk(cudaMalloc(&s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1)), func) ||
+        !cudaOk(cudaMalloc(&s->dNorm, sizeof(double) * 2), func)) {
         if (s->dState) cudaFree(s->dState);
         delete s;
         return q;
@@ -589,6 +614,17 @@ Qureg createQureg(int numQubits, QuESTEnv env) {
     q.state = s;
     initZeroState(q);
     return q;
+}
+
+extern "C" {
+
+Qureg createQureg(int numQubits, QuESTEnv env) { return createQuregWith(numQubits, env, false, __func__); }
+
+Qureg dgq_createQuregF32(int numQubits, QuESTEnv env) { return createQuregWith(numQubits, env, true, __func__); }
+
+int dgq_getPrecision(Qureg qureg) {
+    if (!vQureg(qureg, __func__)) return 0;
+    return stateOf(qureg)->single ? 1 : 2;
 }
 
 void searchQuregTaskPartitions(Qureg qureg, QuESTEnv env) {
@@ -608,6 +644,7 @@ void destroyQureg(Qureg qureg, QuESTEnv env) {
     if (s->dState) cudaFree(s->dState);
     if (s->dPartial) cudaFree(s->dPartial);
     if (s->dProbOut) cudaFree(s->dProbOut);
+    if (s->dNorm) cudaFree(s->dNorm);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -672,13 +709,13 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
         return;
     }
     if (total > n) {
-        cudaOk(cudaMemsetAsync(s.dState + n, 0, (total - n) * sizeof(double2), s.stream), __func__);
+        cudaOk(cudaMemsetAsync((char *) s.dState + n * ampBytes(s), 0, (total - n) * ampBytes(s), s.stream), __func__);
     }
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint64_t c = std::min(chunk, n - off);
         cudaOk(cudaMemcpyAsync(dRe, reals + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
         cudaOk(cudaMemcpyAsync(dIm, imags + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
-        cudaOk(dgq::launchInterleave(dRe, dIm, c, c, s.dState + off, s.stream), __func__);
+        cudaOk(dgq::launchInterleave(dRe, dIm, c, c, (char *) s.dState + off * ampBytes(s), s.single, s.stream), __func__);
         g_launches++;
     }
     cudaOk(cudaStreamSynchronize(s.stream), __func__);
@@ -1014,8 +1051,19 @@ Complex getAmp(Qureg q, long long int index) {
         return out;
     }
     double2 a;
-    if (!cudaOk(cudaMemcpyAsync(&a, s.dState + v, sizeof(a), cudaMemcpyDeviceToHost, s.stream), __func__)) return out;
-    if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+    if (s.single) {
+        float2 f;
+        if (!cudaOk(cudaMemcpyAsync(&f, (const float2 *) s.dState + v, sizeof(f), cudaMemcpyDeviceToHost, s.stream),
+                    __func__))
+            return out;
+        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+        a = make_double2(f.x, f.y);
+    } else {
+        if (!cudaOk(cudaMemcpyAsync(&a, (const double2 *) s.dState + v, sizeof(a), cudaMemcpyDeviceToHost, s.stream),
+                    __func__))
+            return out;
+        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+    }
     const double sc = s.restrictActive ? s.rScale : 1.0;
     out.real = a.x * sc;
     out.imag = a.y * sc;
@@ -1074,10 +1122,12 @@ int measureWithStats(Qureg q, int measureQubit, qreal *outcomeProb) {
     if (!ensureProbs(s, __func__)) return 0;
     const int v = s.l2v[measureQubit];
     const double zeroProb = s.p0[(size_t) v];
+    // QuEST's REAL_EPS for the register's precision (1e-13 double, 1e-5 single)
+    const double eps = s.single ? 1e-5 : REAL_EPS;
     int outcome;
-    if (zeroProb < REAL_EPS)
+    if (zeroProb < eps)
         outcome = 1;
-    else if (1 - zeroProb < REAL_EPS)
+    else if (1 - zeroProb < eps)
         outcome = 0;
     else
         outcome = (g_rng.real1() > zeroProb);
@@ -1160,7 +1210,7 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
     for (uint64_t off = 0; off < n && ok; off += chunk) {
         ga.begin = off;
         ga.count = std::min(chunk, n - off);
-        ok = cudaOk(dgq::launchGather(s.dState, ga, dOut, s.stream), __func__) &&
+        ok = cudaOk(dgq::launchGather(s.dState, s.single, ga, dOut, s.stream), __func__) &&
              cudaOk(cudaMemcpyAsync(host.data(), dOut, ga.count * sizeof(double2), cudaMemcpyDeviceToHost, s.stream),
                     __func__) &&
              cudaOk(cudaStreamSynchronize(s.stream), __func__);
@@ -1258,7 +1308,8 @@ int dgq_setSpecialisationMinBits(int minBits) {
 }
 
 int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
-                    const uint64_t *controlMasks, const double *operands, int sweep, char *buf, int len) {
+                    const uint64_t *controlMasks, const double *operands, int sweep, int precision, char *buf,
+                    int len) {
     if (numQubits < 1 || numQubits > dgq::kMaxStateBits - 2 || count < 0 || !buf || len <= 0) {
         raise(E_INVALID_ARGUMENT, __func__);
         return -1;
@@ -1266,6 +1317,7 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
     QuregState s;
     s.numQubits = numQubits;
     s.numBits = std::max(numQubits, dgq::kMinTileBits);
+    s.single = precision == 1;
     resetMapping(s);
     s.tileBitsSetting = tileBits;
     for (int i = 0; i < count; i++) {
@@ -1279,6 +1331,7 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
     s.initPending = true;
     s.initKind = dgq::INIT_CLASSICAL;
     const bool ok = planPending(s, __func__, false);
+    for (auto &p : s.planned) p.isSingle = s.single ? 1 : 0;
     if (!ok) return -1;
     if (sweep < 0 || sweep >= (int) s.planned.size()) return (int) s.planned.size();
     const std::string src = dgq::generateSweepSource(s.planned[(size_t) sweep], s.plannedTileBits);
@@ -1297,6 +1350,57 @@ int dgq_compileSweepSource(const char *source, char *log, int len) {
         log[len - 1] = '\0';
     }
     return ok ? (int) cubin.size() : -1;
+}
+
+// src/QuEST.h:1306 (declared, no body in dgQuEST): <bra|ket> for state-vectors
+Complex calcInnerProduct(Qureg bra, Qureg ket) {
+    Complex out{0.0, 0.0};
+    if (!vQureg(bra, __func__) || !vQureg(ket, __func__)) return out;
+    QuregState &b = *stateOf(bra);
+    QuregState &k = *stateOf(ket);
+    if (b.numQubits != k.numQubits) {
+        raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
+        return out;
+    }
+    if (!flush(b, __func__) || !flush(k, __func__)) return out;
+    if (!cudaOk(cudaStreamSynchronize(b.stream), __func__) || !cudaOk(cudaStreamSynchronize(k.stream), __func__))
+        return out;
+    dgq::InnerArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.numReal = b.numQubits;
+    a.identity = 1;
+    for (int i = 0; i < b.numQubits; i++) {
+        a.l2vBra[i] = (uint8_t) b.l2v[i];
+        a.l2vKet[i] = (uint8_t) k.l2v[i];
+        if (b.l2v[i] != i || k.l2v[i] != i) a.identity = 0;
+    }
+    a.braRestrict = b.restrictActive;
+    a.braMask = b.rMask;
+    a.braValue = b.rValue;
+    a.braScale = b.rScale;
+    a.ketRestrict = k.restrictActive;
+    a.ketMask = k.rMask;
+    a.ketValue = k.rValue;
+    a.ketScale = k.rScale;
+    double2 *dPart = nullptr, *dOut = nullptr;
+    if (!cudaOk(cudaMalloc(&dPart, sizeof(double2) * (size_t) (dgq::innerNumCtas() + 1)), __func__)) return out;
+    dOut = dPart + dgq::innerNumCtas();
+    double2 h{0.0, 0.0};
+    const bool ok = cudaOk(dgq::launchInner(b.dState, b.single, k.dState, k.single, a, dPart, dOut, b.stream), __func__) &&
+                    cudaOk(cudaMemcpyAsync(&h, dOut, sizeof(h), cudaMemcpyDeviceToHost, b.stream), __func__) &&
+                    cudaOk(cudaStreamSynchronize(b.stream), __func__);
+    g_launches += 2;
+    cudaFree(dPart);
+    if (!ok) return out;
+    out.real = h.x;
+    out.imag = h.y;
+    return out;
+}
+
+// src/QuEST.h:1539 (declared, no body in dgQuEST): |<pure|qureg>|^2 for state-vectors
+qreal calcFidelity(Qureg qureg, Qureg pureState) {
+    const Complex ip = calcInnerProduct(qureg, pureState);
+    return ip.real * ip.real + ip.imag * ip.imag;
 }
 
 }  // extern "C"

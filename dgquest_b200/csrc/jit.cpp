@@ -183,18 +183,19 @@ static std::string generatePersistent(const TileProgram &prog, int W) {
     const bool lastDirect = prog.phases[np - 1].direct;
     std::ostringstream o;
     o << "#include \"jit_prelude.cuh\"\n";
+    o << "typedef " << (prog.isSingle ? "float2" : "double2") << " V;\n";
     o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", 1"
-      << ") dgq_sweep(double2 *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
+      << ") dgq_sweep(V *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
     o << "    constexpr int W = " << W << ";\n";
     o << "    constexpr uint32_t TILE = 1u << W;\n";
-    o << "    extern __shared__ double2 smAll[];\n";
+    o << "    extern __shared__ V smAll[];\n";
     o << "    const uint32_t tid = threadIdx.x;\n";
     o << "    const uint32_t numTiles = 1u << (prog.numBits - W);\n";
-    o << "    double2 a[dgq::kRegs];\n";
+    o << "    V a[dgq::kRegs];\n";
     if (load) o << "    if (blockIdx.x < numTiles) dgq::jPrefetch<W>(st, prog, tid, blockIdx.x, smAll);\n    dgq::jCpAsyncCommit();\n";
     o << "    int it = 0;\n";
     o << "    for (uint32_t cta = blockIdx.x; cta < numTiles; cta += gridDim.x, it++) {\n";
-    o << "    double2 *sm = smAll + (size_t) (it & 1) * TILE;\n";
+    o << "    V *sm = smAll + (size_t) (it & 1) * TILE;\n";
     o << "    __syncthreads();\n";
     if (load) {
         o << "    { const uint32_t nx = cta + gridDim.x; if (nx < numTiles) dgq::jPrefetch<W>(st, prog, tid, nx, smAll + "
@@ -208,7 +209,7 @@ static std::string generatePersistent(const TileProgram &prog, int W) {
         for (int i = 0; i < W - kRegBits; i++) o << " | (((tid >> " << i << ") & 1u) << " << (int) ph.thrPos[i] << ")";
         o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc);\n";
         if (p == 0 && !load) {
-            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = make_double2(0.0, 0.0);\n";
+            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "].x = 0; a[" << j << "].y = 0;\n";
         } else {
             for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = sm[sb ^ " << ph.regOff[j] << "u];\n";
         }
@@ -239,19 +240,26 @@ static std::string generatePersistent(const TileProgram &prog, int W) {
     return o.str();
 }
 
+// The persistent form has no renormalisation step, so complex64 programs
+// (which renormalise every sweep) always use the plain form.
+static bool usePersistent(const TileProgram &prog) {
+    return jitPersistent() && prog.numPhases > 0 && !prog.renormIn && !prog.renormOut;
+}
+
 std::string generateSweepSource(const TileProgram &prog, int W) {
-    if (jitPersistent() && prog.numPhases > 0) return generatePersistent(prog, W);
+    if (usePersistent(prog)) return generatePersistent(prog, W);
     const int T = 1 << (W - kRegBits);
     const int minBlocks = ctasPerSm(T);
     std::ostringstream o;
     o << "#include \"jit_prelude.cuh\"\n";
+    o << "typedef " << (prog.isSingle ? "float2" : "double2") << " V;\n";
     o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << minBlocks
-      << ") dgq_sweep(double2 *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
+      << ") dgq_sweep(V *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
     o << "    constexpr int W = " << W << ";\n";
-    o << "    extern __shared__ double2 sm[];\n";
+    o << "    extern __shared__ V sm[];\n";
     o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x;\n";
     o << "    (void) cta;\n";
-    o << "    double2 a[dgq::kRegs];\n";
+    o << "    V a[dgq::kRegs];\n";
     const int np = prog.numPhases;
     const bool firstDirect = np > 0 && prog.phases[0].direct;
     const bool lastDirect = np > 0 && prog.phases[np - 1].direct;
@@ -281,7 +289,12 @@ std::string generateSweepSource(const TileProgram &prog, int W) {
         o << "  }\n";
     }
     if (np > 0 && !lastDirect) o << "    dgq::jFromSmem<W>(sm, tid, a);\n";
-    if (prog.hasGlobal) o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";
+    if (prog.renormIn) {
+        o << "    { const double sc_ = rsqrt(*prog.normIn); dgq::jGlobal(a, prog.globalRe * sc_, prog.globalIm * sc_); }\n";
+    } else if (prog.hasGlobal) {
+        o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";
+    }
+    if (prog.renormOut) o << "    dgq::jNormAccumulate(a, prog.normOut);\n";
     if (lastDirect) {
         emitDirectAddressing(o, prog.phases[np - 1], W, "gOut", "rbOut");
         o << "    dgq::jStoreDirect(st, gOut, rbOut, a);\n}\n";
@@ -465,10 +478,10 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
     return allOk;
 }
 
-cudaError_t launchJitSweep(CUfunction fn, double2 *st, int W, const TileProgram &prog, cudaStream_t s) {
+cudaError_t launchJitSweep(CUfunction fn, void *st, int W, const TileProgram &prog, cudaStream_t s) {
     const int T = 1 << (W - kRegBits);
-    const bool persistent = jitPersistent() && prog.numPhases > 0;
-    const unsigned smem = (unsigned) ((sizeof(double2) << W) * (persistent ? 2 : 1));
+    const bool persistent = usePersistent(prog);
+    const unsigned smem = (unsigned) (((prog.isSingle ? sizeof(float2) : sizeof(double2)) << W) * (persistent ? 2 : 1));
     // one attribute call per function: cheap and idempotent
     const Driver &drv = driver();
     if (!drv.ok) return cudaErrorNotSupported;

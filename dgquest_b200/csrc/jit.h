@@ -30,7 +30,7 @@ struct JitStats {
 bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfunction> &out, JitStats *stats,
                    std::string *err);
 
-cudaError_t launchJitSweep(CUfunction fn, double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s);
+cudaError_t launchJitSweep(CUfunction fn, void *st, int tileBits, const TileProgram &prog, cudaStream_t s);
 
 // NVRTC compile only (no GPU needed).
 bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log);

@@ -356,7 +356,8 @@ cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaS
 // the CTA, the rest = blockIdx. Each CTA writes 17 partial sums:
 // [0..7] zero-sums of the thread bits, [8..11] of the j bits,
 // [12..15] of the unit bits, [16] the CTA total.
-__global__ void __launch_bounds__(256) probKernel(const double2 *__restrict__ st, const __grid_constant__ ProbArgs args, double *partial) {
+template <class V>
+__global__ void __launch_bounds__(256) probKernel(const V *__restrict__ st, const __grid_constant__ ProbArgs args, double *partial) {
     const uint32_t tid = threadIdx.x;
     const uint32_t cta = blockIdx.x;
     const int nFree = args.nFree;
@@ -388,8 +389,9 @@ __global__ void __launch_bounds__(256) probKernel(const double2 *__restrict__ st
             const uint64_t g = gbase | ((j & 1) ? j0 : 0ULL) | ((j & 2) ? j1 : 0ULL) | ((j & 4) ? j2 : 0ULL) | ((j & 8) ? j3 : 0ULL);
             double p = 0.0;
             if (s < limit) {
-                const double2 v = st[g];
-                p = v.x * v.x + v.y * v.y;
+                const V v = st[g];
+                const double re = (double) v.x, im = (double) v.y;
+                p = re * re + im * im;
             }
             ut += p;
             if (!(j & 1)) zj0 += p;
@@ -457,9 +459,13 @@ __global__ void __launch_bounds__(256) probFinalize(const double *__restrict__ p
     }
 }
 
-cudaError_t launchProb(const double2 *st, const ProbArgs &args, double *partial, double *out, cudaStream_t s) {
+cudaError_t launchProb(const void *st, bool single, const ProbArgs &args, double *partial, double *out,
+                       cudaStream_t s) {
     const int grid = args.nFree > 12 + args.kappa ? (1 << (args.nFree - 12 - args.kappa)) : 1;
-    probKernel<<<grid, 256, 0, s>>>(st, args, partial);
+    if (single)
+        probKernel<float2><<<grid, 256, 0, s>>>((const float2 *) st, args, partial);
+    else
+        probKernel<double2><<<grid, 256, 0, s>>>((const double2 *) st, args, partial);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     probFinalize<<<args.nFree + 1, 256, 0, s>>>(partial, grid, args.nFree, args.kappa, out);
@@ -508,13 +514,14 @@ cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s) {
 // ------------------------------------------------------------ gather
 // out[l] = st[virt(l)] for logical indices l in [begin, begin + count),
 // with virt() the logical->virtual bit map and the lazy collapse applied.
-__global__ void gatherKernel(const double2 *__restrict__ st, const __grid_constant__ GatherArgs args, double2 *__restrict__ out) {
+template <class V>
+__global__ void gatherKernel(const V *__restrict__ st, const __grid_constant__ GatherArgs args, double2 *__restrict__ out) {
     for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < args.count;
          i += (uint64_t) gridDim.x * blockDim.x) {
         const uint64_t l = args.begin + i;
         uint64_t v = 0;
         for (int b = 0; b < args.numReal; b++) v |= ((l >> b) & 1ULL) << args.l2v[b];
-        double2 x = st[v];
+        double2 x = make_double2((double) st[v].x, (double) st[v].y);
         if (args.hasRestrict) {
             if ((v & args.restrictMask) != args.restrictValue)
                 x = make_double2(0.0, 0.0);
@@ -525,11 +532,14 @@ __global__ void gatherKernel(const double2 *__restrict__ st, const __grid_consta
     }
 }
 
-cudaError_t launchGather(const double2 *st, const GatherArgs &args, double2 *out, cudaStream_t s) {
+cudaError_t launchGather(const void *st, bool single, const GatherArgs &args, double2 *out, cudaStream_t s) {
     uint64_t blocks = (args.count + 255) / 256;
     if (blocks > 148ULL * 32) blocks = 148ULL * 32;
     if (blocks == 0) blocks = 1;
-    gatherKernel<<<(unsigned) blocks, 256, 0, s>>>(st, args, out);
+    if (single)
+        gatherKernel<float2><<<(unsigned) blocks, 256, 0, s>>>((const float2 *) st, args, out);
+    else
+        gatherKernel<double2><<<(unsigned) blocks, 256, 0, s>>>((const double2 *) st, args, out);
     return cudaGetLastError();
 }
 
@@ -539,19 +549,26 @@ namespace dgq {
 
 // ------------------------------------------------- amplitude upload
 // out[i] = (re[i], im[i]) for i < count, zero for count <= i < total.
+template <class V>
 __global__ void interleaveKernel(const double *__restrict__ re, const double *__restrict__ im, uint64_t count,
-                                 uint64_t total, double2 *__restrict__ out) {
+                                 uint64_t total, V *__restrict__ out) {
     for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (uint64_t) gridDim.x * blockDim.x) {
-        out[i] = i < count ? make_double2(re[i], im[i]) : make_double2(0.0, 0.0);
+        V v;
+        v.x = i < count ? re[i] : 0.0;
+        v.y = i < count ? im[i] : 0.0;
+        out[i] = v;
     }
 }
 
-cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, double2 *out,
-                             cudaStream_t s) {
+cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, void *out,
+                             bool single, cudaStream_t s) {
     uint64_t blocks = (total + 255) / 256;
     if (blocks > 148ULL * 32) blocks = 148ULL * 32;
-    interleaveKernel<<<(unsigned) blocks, 256, 0, s>>>(re, im, count, total, out);
+    if (single)
+        interleaveKernel<float2><<<(unsigned) blocks, 256, 0, s>>>(re, im, count, total, (float2 *) out);
+    else
+        interleaveKernel<double2><<<(unsigned) blocks, 256, 0, s>>>(re, im, count, total, (double2 *) out);
     return cudaGetLastError();
 }
 
@@ -584,6 +601,94 @@ __global__ void __launch_bounds__(256) fp64PeakKernel(double *out, int iters, do
 
 cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s) {
     fp64PeakKernel<<<blocks, 256, 0, s>>>(out, iters, 1.0);
+    return cudaGetLastError();
+}
+
+}  // namespace dgq
+
+namespace dgq {
+
+// ------------------------------------------------------ inner product
+// sum over logical indices of conj(bra) * ket, both registers read through
+// their own logical->virtual maps and lazy collapses; FP64 accumulation,
+// fixed reduction order (partials per CTA, then one finalise CTA).
+template <class VB, class VK>
+__global__ void __launch_bounds__(256) innerKernel(const VB *__restrict__ bra, const VK *__restrict__ ket,
+                                                   const __grid_constant__ InnerArgs args, double2 *partial) {
+    double re = 0.0, im = 0.0;
+    const uint64_t n = 1ULL << args.numReal;
+    for (uint64_t l = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (uint64_t) gridDim.x * blockDim.x) {
+        uint64_t vb = l, vk = l;
+        if (!args.identity) {
+            vb = 0;
+            vk = 0;
+            for (int b = 0; b < args.numReal; b++) {
+                const uint64_t bit = (l >> b) & 1ULL;
+                vb |= bit << args.l2vBra[b];
+                vk |= bit << args.l2vKet[b];
+            }
+        }
+        double br = (double) bra[vb].x, bi = (double) bra[vb].y;
+        double kr = (double) ket[vk].x, ki = (double) ket[vk].y;
+        if (args.braRestrict) {
+            const bool keep = (vb & args.braMask) == args.braValue;
+            br = keep ? br * args.braScale : 0.0;
+            bi = keep ? bi * args.braScale : 0.0;
+        }
+        if (args.ketRestrict) {
+            const bool keep = (vk & args.ketMask) == args.ketValue;
+            kr = keep ? kr * args.ketScale : 0.0;
+            ki = keep ? ki * args.ketScale : 0.0;
+        }
+        re += br * kr + bi * ki;
+        im += br * ki - bi * kr;
+    }
+    __shared__ double sre[8], sim[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sre[threadIdx.x >> 5] = re;
+        sim[threadIdx.x >> 5] = im;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < 8; w++) {
+            a += sre[w];
+            b += sim[w];
+        }
+        partial[blockIdx.x] = make_double2(a, b);
+    }
+}
+
+__global__ void innerFinalize(const double2 *__restrict__ partial, int n, double2 *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < n; i++) {
+        a += partial[i].x;
+        b += partial[i].y;
+    }
+    *out = make_double2(a, b);
+}
+
+int innerNumCtas() { return 148 * 8; }
+
+cudaError_t launchInner(const void *bra, bool braSingle, const void *ket, bool ketSingle, const InnerArgs &args,
+                        double2 *partial, double2 *out, cudaStream_t s) {
+    const int grid = innerNumCtas();
+    if (braSingle && ketSingle)
+        innerKernel<float2, float2><<<grid, 256, 0, s>>>((const float2 *) bra, (const float2 *) ket, args, partial);
+    else if (braSingle)
+        innerKernel<float2, double2><<<grid, 256, 0, s>>>((const float2 *) bra, (const double2 *) ket, args, partial);
+    else if (ketSingle)
+        innerKernel<double2, float2><<<grid, 256, 0, s>>>((const double2 *) bra, (const float2 *) ket, args, partial);
+    else
+        innerKernel<double2, double2><<<grid, 256, 0, s>>>((const double2 *) bra, (const double2 *) ket, args, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    innerFinalize<<<1, 32, 0, s>>>(partial, grid, out);
     return cudaGetLastError();
 }
 

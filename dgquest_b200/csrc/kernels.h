@@ -32,13 +32,28 @@ struct GatherArgs {
     uint8_t l2v[kMaxStateBits];
 };
 
+struct InnerArgs {
+    int32_t numReal;
+    int32_t identity;  // both maps are the identity
+    int32_t braRestrict, ketRestrict;
+    uint64_t braMask, braValue, ketMask, ketValue;
+    double braScale, ketScale;
+    uint8_t l2vBra[kMaxStateBits];
+    uint8_t l2vKet[kMaxStateBits];
+};
+
+cudaError_t launchInner(const void *bra, bool braSingle, const void *ket, bool ketSingle, const InnerArgs &args,
+                        double2 *partial, double2 *out, cudaStream_t s);
+int innerNumCtas();
+
 cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s);
-cudaError_t launchProb(const double2 *st, const ProbArgs &args, double *partial, double *out, cudaStream_t s);
+cudaError_t launchProb(const void *st, bool single, const ProbArgs &args, double *partial, double *out,
+                       cudaStream_t s);
 int probNumCtas(const ProbArgs &args);
 cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s);
-cudaError_t launchGather(const double2 *st, const GatherArgs &args, double2 *out, cudaStream_t s);
+cudaError_t launchGather(const void *st, bool single, const GatherArgs &args, double2 *out, cudaStream_t s);
 cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s);
-cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, double2 *out,
-                             cudaStream_t s);
+cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, void *out,
+                             bool single, cudaStream_t s);
 
 }  // namespace dgq

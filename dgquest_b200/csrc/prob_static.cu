@@ -89,7 +89,7 @@ extern "C" int dgq_calcProbOfAllZeroNoAlloc(const void *deviceState, int numBits
         raiseExternal(104, __func__, "state larger than the static scratch holds");
         return -1;
     }
-    e = launchProb((const double2 *) deviceState, a, scratch, deviceProbs, (cudaStream_t) stream);
+    e = launchProb(deviceState, false, a, scratch, deviceProbs, (cudaStream_t) stream);
     if (e != cudaSuccess) {
         raiseExternal(103, __func__, cudaGetErrorString(e));
         return -2;

@@ -24,7 +24,8 @@ constexpr int kRegBits = 4;
 constexpr int kRegs = 1 << kRegBits;
 constexpr int kCoalescedBits = 5;
 constexpr int kMinTileBits = 9;   // >= 32 threads (one full warp)
-constexpr int kMaxTileBits = 12;  // 2^12 x 16 B = 64 KiB per tile buffer
+constexpr int kMaxTileBits = 13;  // complex64: 2^13 x 8 B; complex128 tiles stop at 12 (64 KiB)
+constexpr int kMaxTileBitsF64 = 12;
 constexpr int kMaxThreadBits = kMaxTileBits - kRegBits;
 constexpr int kMaxStateBits = 40;
 constexpr int kMaxPhases = 56;
@@ -119,8 +120,14 @@ struct TileProgram {
     int32_t initKind;
     int32_t hasRestrict;
     int32_t hasGlobal;       // multiply every amplitude by (globalRe + i globalIm) before the store
-    int32_t pad1;
+    int32_t isSingle;        // 1: complex64 state (float2), 0: complex128 (double2)
     double globalRe, globalIm;
+    // complex64 renormalisation (runtime-specialised kernels only): the
+    // sweep scales by 1/sqrt(*normIn) and adds its output's sum of |a|^2
+    // to *normOut (zeroed before the launch)
+    int32_t renormIn, renormOut;
+    const double *normIn;
+    double *normOut;
     uint64_t initIndex;
     double initAmp;
     uint64_t restrictMask;   // lazy measurement collapse applied at load:

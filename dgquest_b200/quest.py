@@ -135,6 +135,8 @@ _SIGS = {
     "collapseToOutcome": (D, [Q, I, I]),
     "measure": (I, [Q, I]),
     "measureWithStats": (I, [Q, I, P(D)]),
+    "calcInnerProduct": (Complex, [Q, Q]),
+    "calcFidelity": (D, [Q, Q]),
     # extensions (include/dgq.h)
     "dgq_setErrorMode": (I, [I]),
     "dgq_getLastError": (I, [ctypes.c_char_p, I]),
@@ -149,7 +151,9 @@ _SIGS = {
     "dgq_getLaunchCount": (c_int64, []),
     "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
     "dgq_measureFp64Peak": (I, [P(D)]),
-    "dgq_sweepSource": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I,
+    "dgq_createQuregF32": (Qureg, [I, E]),
+    "dgq_getPrecision": (I, [Q]),
+    "dgq_sweepSource": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I, I,
                             ctypes.c_char_p, I]),
     "dgq_compileSweepSource": (I, [ctypes.c_char_p, ctypes.c_char_p, I]),
     "dgq_setSpecialisationMinBits": (I, [I]),

@@ -144,6 +144,8 @@ qreal calcProbOfOutcome(Qureg qureg, const int measureQubit, int outcome); /* in
 qreal collapseToOutcome(Qureg qureg, const int measureQubit, int outcome); /* include/QuEST.h:1277 */
 int measure(Qureg qureg, int measureQubit);                   /* include/QuEST.h:1289 */
 int measureWithStats(Qureg qureg, int measureQubit, qreal *outcomeProb); /* include/QuEST.h:1303 */
+Complex calcInnerProduct(Qureg bra, Qureg ket);                 /* include/QuEST.h:1306 (declared only in dgQuEST) */
+qreal calcFidelity(Qureg qureg, Qureg pureState);               /* include/QuEST.h:1539 (declared only in dgQuEST) */
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,14 @@
 extern "C" {
 #endif
 
+/* Precision form: a register whose 2^n amplitudes are complex64 (two
+ * floats, 8 bytes each) with FP32 gate arithmetic; every QuEST call accepts
+ * it. Read-outs return doubles; probabilities are accumulated in FP64.
+ * Its sweeps always run runtime-specialised kernels and may use tiles of
+ * 2^13 amplitudes. dgq_getPrecision returns 1 (complex64) or 2. */
+Qureg dgq_createQuregF32(int numQubits, QuESTEnv env);
+int dgq_getPrecision(Qureg qureg);
+
 /* Error handling. Mode 0 (default) prints QuEST's message and exits with
  * its code, as dgQuEST does (src/QuEST_validation.c:82-91). Mode 1 records
  * the error instead: the failing call returns without effect (a zero or
@@ -115,11 +123,13 @@ int dgq_setSpecialisationMinBits(int minBits);
 
 /* Host-only view of the runtime specialisation: the CUDA source generated
  * for sweep `sweep` of the plan of the given gates (same encoding as
- * dgq_planGates; returns the number of sweeps, -2 if buf is too small), and
+ * dgq_planGates; precision 1 = complex64, 2 = complex128; returns the number
+ * of sweeps, -2 if buf is too small), and
  * an NVRTC compile of such a source for sm_100a (returns the cubin size, or
  * -1 with the compiler log in `log`). Neither needs a GPU. */
 int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
-                    const uint64_t *controlMasks, const double *operands, int sweep, char *buf, int len);
+                    const uint64_t *controlMasks, const double *operands, int sweep, int precision, char *buf,
+                    int len);
 int dgq_compileSweepSource(const char *source, char *log, int len);
 
 #ifdef __cplusplus

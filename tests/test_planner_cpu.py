@@ -38,24 +38,24 @@ def test_merge_rules():
     assert sorted(merged) == sorted([2, 15, 8])
 
 
-def _sources(ops, n, w):
+def _sources(ops, n, w, precision=2):
     t, tm, cm, o = ir.ops_to_ir(ops, n)
     buf = ctypes.create_string_buffer(1 << 20)
     args = (n, w, len(t), t.ctypes.data_as(P(ctypes.c_int32)), tm.ctypes.data_as(P(ctypes.c_uint64)),
             cm.ctypes.data_as(P(ctypes.c_uint64)), o.ctypes.data_as(P(ctypes.c_double)))
-    count = Q.dgq_sweepSource(*args, 0, buf, len(buf))
+    count = Q.dgq_sweepSource(*args, 0, precision, buf, len(buf))
     out = []
     for s in range(count):
-        Q.dgq_sweepSource(*args, s, buf, len(buf))
+        Q.dgq_sweepSource(*args, s, precision, buf, len(buf))
         out.append(buf.value)
     return out
 
 
-@pytest.mark.parametrize("w", [9, 12])
-def test_generated_sweeps_compile(w):
+@pytest.mark.parametrize("w,precision", [(9, 2), (12, 2), (13, 1)])
+def test_generated_sweeps_compile(w, precision):
     ops = np.concatenate([C.mixed_ops(14, 150, 3, kinds=[k for k in range(26) if k != C.MEASURE]),
                           C.random_layers(14, 2, 5)])
-    srcs = _sources(ops, 14, w)
+    srcs = _sources(ops, 14, w, precision)
     assert len(srcs) >= 1
     log = ctypes.create_string_buffer(1 << 16)
     for s in srcs[:3]:
