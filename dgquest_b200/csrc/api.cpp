@@ -252,7 +252,12 @@ double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, co
 }
 
 int chooseTileBits(QuregState &s) {
-    const int hi = std::min(s.single ? dgq::kMaxTileBits : dgq::kMaxTileBitsF64, s.numBits);
+    // complex64 tiles could reach 2^13 amplitudes in 64 KiB, but at 16
+    // amplitudes a thread that is one 512-thread CTA per SM, which hides no
+    // latency; 2^12 keeps three CTAs per SM (override: dgq_setTileBits(13))
+    const int hi = std::min(s.single && s.tileBitsSetting == dgq::kMaxTileBits ? dgq::kMaxTileBits
+                                                                                 : dgq::kMaxTileBitsF64,
+                            s.numBits);
     const int lo = dgq::kMinTileBits;
     if (s.tileBitsSetting > 0) return std::max(lo, std::min(hi, s.tileBitsSetting));
     if (const char *env = getenv("DGQ_TILE_BITS")) {

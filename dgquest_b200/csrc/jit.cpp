@@ -151,14 +151,16 @@ void emitDirectAddressing(std::ostringstream &o, const KPhase &ph, int W, const 
 // CTAs per SM the kernel is compiled for: 16 warps per SM at 128 registers
 // a thread by default; DGQ_JIT_CTAS_PER_SM overrides (register cap
 // 65536 / (threads x CTAs)).
-static int ctasPerSm(int T) {
+static int ctasPerSm(int T, bool single) {
     static int env = -2;
     if (env == -2) {
         const char *e = getenv("DGQ_JIT_CTAS_PER_SM");
         env = e ? atoi(e) : -1;
     }
     if (env > 0) return env;
-    return 65536 / (128 * T) > 0 ? 65536 / (128 * T) : 1;
+    // complex64 amplitudes need half the registers: 3 x 256-thread CTAs per SM
+    const int regs = single ? 85 : 128;
+    return 65536 / (regs * T) > 0 ? 65536 / (regs * T) : 1;
 }
 
 // Off by default: measured on B200 at 30 qubits, one 256-thread CTA per SM
@@ -249,7 +251,7 @@ static bool usePersistent(const TileProgram &prog) {
 std::string generateSweepSource(const TileProgram &prog, int W) {
     if (usePersistent(prog)) return generatePersistent(prog, W);
     const int T = 1 << (W - kRegBits);
-    const int minBlocks = ctasPerSm(T);
+    const int minBlocks = ctasPerSm(T, prog.isSingle != 0);
     std::ostringstream o;
     o << "#include \"jit_prelude.cuh\"\n";
     o << "typedef " << (prog.isSingle ? "float2" : "double2") << " V;\n";
