@@ -235,9 +235,7 @@ def run_gpu(args, world, rank, local):
             e2e_times.append(dt)
     e2e_t = max_over_ranks(float(np.mean(e2e_times)), world)
     st2 = Q.plan_stats(q)
-    from dgquest_b200.quest import ctypes as _ct  # noqa: F401
-    prog_bytes = 25296  # sizeof(TileProgram): the kernel parameter block of one launch
-    h2d = st2.sweeps * prog_bytes
+    h2d = int(st2.launchBytes)  # one sweep program per kernel parameter block
     d2h = 16 + (n + 1) * 8
 
     hbm, hbm_kind = peaks()

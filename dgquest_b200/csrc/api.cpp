@@ -363,6 +363,7 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.stats.tileBits = W;
     s.stats.numBits = s.numBits;
     s.stats.flopsPerAmp = st.flopsPerAmp;
+    s.stats.launchBytes = (int64_t) st.sweeps * (int64_t) sizeof(dgq::TileProgram);
     s.stats.planMillis = nowMillis() - t0;
     s.pending.clear();
     s.pool.mats.clear();

@@ -62,6 +62,7 @@ class PlanStats(Structure):
         ("jitCompiled", ctypes.c_int32),
         ("jitReused", ctypes.c_int32),
         ("jitMillis", c_double),
+        ("launchBytes", ctypes.c_int64),
     ]
 
 

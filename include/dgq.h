@@ -54,6 +54,8 @@ typedef struct dgq_plan_stats {
     int32_t jitCompiled;   /* sweep kernels compiled for this plan */
     int32_t jitReused;     /* sweep kernels found already compiled */
     double jitMillis;      /* time spent specialising kernels */
+    int64_t launchBytes;   /* host->device bytes per launch of the whole plan
+                              (one sweep program per kernel parameter block) */
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
