@@ -336,6 +336,75 @@ def run_ncu_case(args):
     Q.destroyQuESTEnv(env)
 
 
+def run_batch_form(args, world):
+    """Batched form: 4096 ansatz circuits (n in [10, 22], depth in [4, 32]) in
+    one persistent launch per step, complex128 and complex64; tile width and
+    grouping from the autotuner, the launch replayed from a CUDA graph."""
+    import torch
+
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    wl = C.batch_workload(args.batch_circuits)
+    env = Q.createQuESTEnv()
+    out = {"workload": f"{len(wl)} hardware-efficient ansatz circuits, n~U[10,22], depth~U[4,32], <Z_q> of every qubit",
+           "circuits": len(wl), "gates": int(sum(len(o) for _, _, o in wl))}
+    steps = max(1, min(args.steps, 5))
+    for name, single in (("complex128", False), ("complex64", True)):
+        regs = [Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env) for n, _, _ in wl]
+        t0 = time.perf_counter()
+        for q, (n, d, ops) in zip(regs, wl):
+            Q.initZeroState(q)
+            Q.apply_circuit(q, ops)
+        record_ms = (time.perf_counter() - t0) * 1e3
+        b = Q.Batch(regs)
+        st = b.stats()
+        stream = torch.cuda.ExternalStream(b.stream())
+        for _ in range(args.warmup):
+            b.launch()
+        b.wait()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            b.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
+        z = b.expectation_z()
+        b.close()
+        # end to end through the API: record every circuit, plan (tuning
+        # cached), upload, launch, read <Z> back
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for q, (n, d, ops) in zip(regs, wl):
+            Q.initZeroState(q)
+            Q.apply_circuit(q, ops)
+        b2 = Q.Batch(regs)
+        b2.launch()
+        z2 = b2.expectation_z()
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+        st2 = b2.stats()
+        b2.close()
+        for q in regs:
+            Q.destroyQureg(q, env)
+        hbm = peaks()[0]
+        out[name] = {"ms_per_launch": ms, "circuits_per_s": world * len(wl) / (ms / 1e3),
+                     "hbm_gbs_algorithmic": st.sweepBytes / (ms / 1e3) / 1e9,
+                     "roofline_frac": st.sweepBytes / (ms / 1e3) / 1e9 / hbm,
+                     "sweep_bytes": int(st.sweepBytes), "state_bytes": int(st.stateBytes),
+                     "tile_bits": st.tileBits, "group_factor": st.groupFactor, "grid": st.grid,
+                     "ctas_per_sm": st.ctasPerSm, "items": int(st.items), "sweeps": st.sweeps,
+                     "whole_register_items": st.wholeRegisters, "tuned": bool(st.tuned),
+                     "tune_ms": st.tuneMillis, "plan_ms": st.planMillis, "record_ms": record_ms,
+                     "e2e_ms": e2e_ms, "e2e_plan_ms": st2.planMillis,
+                     "e2e_h2d_bytes": int(st2.programBytes), "e2e_d2h_bytes": int(8 * len(z2)),
+                     "z_abs_max": float(np.abs(z).max()), "z_repeat_identical": bool(np.array_equal(z, z2))}
+    Q.destroyQuESTEnv(env)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,6 +419,8 @@ def main():
     ap.add_argument("--cpu-gates", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-circuits", type=int, default=4096)
     ap.add_argument("--precision", type=int, default=2, choices=[1, 2], help="--ncu-case register precision")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run one small case once (for ncu captures): --qubits/--depth/--tile-bits, specialised kernels")
@@ -367,6 +438,10 @@ def main():
             dist.destroy_process_group()
         return
     line = run_gpu(args, world, rank, local)
+    if not args.no_batch:
+        batch = run_batch_form(args, world)
+        if rank == 0:
+            line["batched_form"] = batch
     if rank == 0 and world == 1 and not args.no_cpu:
         from dgquest_b200 import circuits as C
         ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))

@@ -213,19 +213,44 @@ def grid_sqrt(rows, cols, depth, seed):
 
 
 def hea(n, depth, seed):
-    """Hardware-efficient ansatz: per layer Ry(theta), Rz(phi) on each qubit, then CNOT(i, i+1)."""
-    rng = Mt19937(seed)
-    b = OpList()
-    for _ in range(depth):
-        for q in range(n):
-            b.add(RY, q, p=(2.0 * math.pi * rng.uniform(),))
-            b.add(RZ, q, p=(2.0 * math.pi * rng.uniform(),))
-        for q in range(n - 1):
-            b.add(CNOT, q, q + 1)
-    return b.array()
+    """Hardware-efficient ansatz: per layer Ry(theta), Rz(phi) on each qubit, then CNOT(i, i+1).
+
+    Angles are 2 pi x the MT19937 (init_genrand(seed)) 53-bit uniforms in
+    gate order; numpy's RandomState draws the same sequence (two 32-bit
+    outputs per double, a >> 5 and b >> 6), which keeps this vectorised."""
+    per = 2 * n + (n - 1)
+    arr = np.zeros(depth * per, dtype=OP_DTYPE)
+    if depth == 0 or n == 0:
+        return arr
+    ang = 2.0 * math.pi * np.random.RandomState(seed & 0xFFFFFFFF).random_sample(2 * n * depth)
+    layer = np.zeros(per, dtype=OP_DTYPE)
+    layer["kind"][0:2 * n:2] = RY
+    layer["kind"][1:2 * n:2] = RZ
+    layer["q0"][0:2 * n] = np.repeat(np.arange(n), 2)
+    layer["kind"][2 * n:] = CNOT
+    layer["q0"][2 * n:] = np.arange(n - 1)
+    layer["q1"][2 * n:] = np.arange(1, n)
+    for d in range(depth):
+        blk = arr[d * per:(d + 1) * per]
+        blk[:] = layer
+        blk["p"][:2 * n, 0] = ang[d * 2 * n:(d + 1) * 2 * n]
+    return arr
 
 
-# ---------------------------------------------------------------- replay
+def batch_workload(count, seed=None):
+    """The batched workload: `count` hardware-efficient ansatz circuits with
+    qubit counts uniform in [10, 22] and depths uniform in [4, 32]; sizes are
+    drawn from MT19937(seed) (n = 10 + u32 % 13, depth = 4 + u32 % 29) and
+    circuit i uses angle seed config_seed(4, i). Returns [(n, depth, ops)]."""
+    rng = Mt19937(config_seed(4) if seed is None else seed)
+    out = []
+    for i in range(count):
+        n = 10 + rng.below(13)
+        d = 4 + rng.below(29)
+        out.append((n, d, hea(n, d, config_seed(4, i))))
+    return out
+
+
 def replay(q, ops, quest=None):
     """Replays an op list through the QuEST API of libdgq; returns measurement outcomes."""
     if quest is None:

@@ -30,6 +30,7 @@
 #include "jit.h"
 #include "kernels.h"
 #include "planner.h"
+#include "qureg_state.h"
 #include "rng.h"
 
 using dgq::Gate;
@@ -110,6 +111,7 @@ std::mutex g_errMutex;
 int g_errMode = DGQ_ERRORS_EXIT;
 int g_lastError = 0;
 std::string g_lastMessage;
+std::atomic<int64_t> g_errorCount{0};  // errors raised in record mode
 std::atomic<int64_t> g_launches{0};
 dgq::Mt19937 g_rng;
 
@@ -125,6 +127,7 @@ bool raise(int code, const char *func, const char *detail = nullptr) {
     }
     std::lock_guard<std::mutex> lk(g_errMutex);
     g_lastError = code;
+    g_errorCount++;
     g_lastMessage = msg;
     return false;
 }
@@ -153,45 +156,6 @@ struct QuESTEnvValue {
     int device = 0;
 };
 
-struct QuregState {
-    int numQubits = 0;  // user-visible qubits
-    int numBits = 0;    // address bits of the buffer (>= numQubits, >= kMinTileBits)
-    bool single = false;  // complex64 amplitudes (float2) instead of complex128
-    void *dState = nullptr;
-    cudaStream_t stream = nullptr;
-
-    // recorded, not yet executed
-    std::vector<Gate> pending;
-    dgq::MatrixPool pool;
-    bool initPending = false;
-    int32_t initKind = dgq::INIT_NONE;
-    uint64_t initIndex = 0;
-    double initAmp = 0.0;
-
-    // lazy measurement collapse applied to the state in HBM
-    bool restrictActive = false;
-    uint64_t rMask = 0, rValue = 0;
-    double rScale = 1.0;
-
-    // logical qubit -> address bit (swapGate relabels instead of moving data)
-    int l2v[64];
-    int v2l[64];
-
-    // P(bit = 0) per address bit, of the (collapsed, normalised) state
-    bool probsValid = false;
-    std::vector<double> p0;
-    double totalProb = 1.0;
-    double *dPartial = nullptr;
-    size_t partialCap = 0;
-    double *dProbOut = nullptr;
-    double *dNorm = nullptr;  // complex64 renormalisation: two running sums of |a|^2
-
-    int tileBitsSetting = 0;  // 0 = cost model
-    std::vector<dgq::TileProgram> planned;
-    std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)
-    int plannedTileBits = 0;
-    dgq_plan_stats stats{};
-};
 
 namespace {
 
@@ -292,12 +256,13 @@ int jitMinBits() {
     return v;
 }
 
-bool planPending(QuregState &s, const char *func, bool specialise = true) {
-    s.planned.clear();
-    if (s.pending.empty() && !s.initPending) return true;
-    const double t0 = nowMillis();
-    const int W = chooseTileBits(s);
-    dgq::SweepHeader h;
+}  // namespace
+
+namespace dgq {
+
+int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err) {
+    out.clear();
+    SweepHeader h;
     if (s.initPending) {
         h.initKind = s.initKind;
         h.initIndex = s.initIndex;
@@ -308,24 +273,49 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
         h.restrictValue = s.rValue;
         h.restrictScale = s.rScale;
     }
-    dgq::PlanStats st;
     bool complete = true;
-    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(s.pending, s.numBits, W, &complete);
-    if (!complete)
-        return raise(E_UNSUPPORTED, func, "a multi-qubit gate is wider than the register tile (max 4 targets)");
-    std::string err;
+    std::vector<BlockPlan> blocks = planBlocks(s.pending, s.numBits, W, &complete);
+    if (!complete) {
+        err = "a multi-qubit gate is wider than the register tile (max 4 targets)";
+        return E_UNSUPPORTED;
+    }
     bool first = true;
     for (const auto &b : blocks) {
-        dgq::SweepHeader hb = first ? h : dgq::SweepHeader();
-        if (!dgq::encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, s.planned, &st, &err))
-            return raise(E_UNSUPPORTED, func, err.c_str());
+        SweepHeader hb = first ? h : SweepHeader();
+        if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err)) return E_UNSUPPORTED;
         first = false;
     }
     if (blocks.empty()) {
-        s.planned.emplace_back();
-        dgq::encodeHeaderOnly(s.numBits, s.numQubits, W, h, s.planned.back());
+        out.emplace_back();
+        encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back());
         st.sweeps = 1;
     }
+    return 0;
+}
+
+void consumePending(QuregState &s) {
+    s.pending.clear();
+    s.pool.mats.clear();
+    s.initPending = false;
+    s.restrictActive = false;
+    s.rMask = s.rValue = 0;
+    s.rScale = 1.0;
+    s.probsValid = false;
+}
+
+}  // namespace dgq
+
+namespace {
+
+bool planPending(QuregState &s, const char *func, bool specialise = true) {
+    s.planned.clear();
+    if (s.pending.empty() && !s.initPending) return true;
+    const double t0 = nowMillis();
+    const int W = chooseTileBits(s);
+    dgq::PlanStats st;
+    std::string err;
+    const int code = dgq::buildPrograms(s, W, s.planned, st, err);
+    if (code) return raise(code, func, err.c_str());
     s.plannedTileBits = W;
     for (size_t i = 0; i < s.planned.size(); i++) {
         dgq::TileProgram &p = s.planned[i];
@@ -365,13 +355,7 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.stats.flopsPerAmp = st.flopsPerAmp;
     s.stats.launchBytes = (int64_t) st.sweeps * (int64_t) sizeof(dgq::TileProgram);
     s.stats.planMillis = nowMillis() - t0;
-    s.pending.clear();
-    s.pool.mats.clear();
-    s.initPending = false;
-    s.restrictActive = false;
-    s.rMask = s.rValue = 0;
-    s.rScale = 1.0;
-    s.probsValid = false;
+    dgq::consumePending(s);
     return true;
 }
 
@@ -525,6 +509,70 @@ int dgq_setErrorMode(int mode) {
     const int prev = g_errMode;
     g_errMode = mode == DGQ_ERRORS_RECORD ? DGQ_ERRORS_RECORD : DGQ_ERRORS_EXIT;
     return prev;
+}
+
+int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes) {
+    if (!vQureg(q, __func__)) return -1;
+    if (count < 0 || (count > 0 && !r)) return raise(E_INVALID_ARGUMENT, __func__, "null records") ? 0 : -1;
+    int m = 0;
+    for (int i = 0; i < count; i++) {
+        const int64_t before = g_errorCount.load();
+        const dgq_gate_record &g = r[i];
+        const int a = g.q0, b = g.q1;
+        const double *p = g.p;
+        switch (g.kind) {
+            case 0: hadamard(q, a); break;
+            case 1: pauliX(q, a); break;
+            case 2: pauliY(q, a); break;
+            case 3: pauliZ(q, a); break;
+            case 4: sGate(q, a); break;
+            case 5: tGate(q, a); break;
+            case 6: rotateX(q, a, p[0]); break;
+            case 7: rotateY(q, a, p[0]); break;
+            case 8: rotateZ(q, a, p[0]); break;
+            case 9: phaseShift(q, a, p[0]); break;
+            case 10: controlledNot(q, a, b); break;
+            case 11: controlledPhaseFlip(q, a, b); break;
+            case 12: controlledPhaseShift(q, a, b, p[0]); break;
+            case 13: controlledRotateX(q, a, b, p[0]); break;
+            case 14: controlledRotateY(q, a, b, p[0]); break;
+            case 15: controlledRotateZ(q, a, b, p[0]); break;
+            case 16: compactUnitary(q, a, Complex{p[0], p[1]}, Complex{p[2], p[3]}); break;
+            case 17: controlledCompactUnitary(q, a, b, Complex{p[0], p[1]}, Complex{p[2], p[3]}); break;
+            case 18:
+            case 19: {
+                ComplexMatrix2 u;
+                u.r0c0 = Complex{p[0], p[1]};
+                u.r0c1 = Complex{p[2], p[3]};
+                u.r1c0 = Complex{p[4], p[5]};
+                u.r1c1 = Complex{p[6], p[7]};
+                if (g.kind == 18)
+                    unitary(q, a, u);
+                else
+                    controlledUnitary(q, a, b, u);
+                break;
+            }
+            case 20: SqX(q, a); break;
+            case 21: SqY(q, a); break;
+            case 22: SqW(q, a); break;
+            case 23: swapGate(q, a, b); break;
+            case 24: {
+                const int o = measure(q, a);
+                if (outcomes && g_errorCount.load() == before) outcomes[m] = o;
+                m++;
+                break;
+            }
+            case 25: controlledPauliY(q, a, b); break;
+            default: {
+                char msg[64];
+                snprintf(msg, sizeof msg, "record %d has unknown kind %d", i, g.kind);
+                raise(E_INVALID_ARGUMENT, __func__, msg);
+                return -1;
+            }
+        }
+        if (g_errorCount.load() != before) return -1;
+    }
+    return count;
 }
 
 int dgq_getLastError(char *msg, int len) {

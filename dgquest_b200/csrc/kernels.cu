@@ -15,230 +15,13 @@
 
 #include <cstdint>
 
+#include "interp.cuh"
 #include "kernels.h"
 #include "tile_program.h"
 
 namespace dgq {
 
 __device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u); }
-
-// ------------------------------------------------------------------ ops
-template <int K, class F>
-__device__ __forceinline__ void forPairs(double2 (&a)[kRegs], uint32_t ctrlReg, F f) {
-#pragma unroll
-    for (int p = 0; p < kRegs / 2; p++) {
-        const int j0 = ((p >> K) << (K + 1)) | (p & ((1 << K) - 1));
-        const int j1 = j0 | (1 << K);
-        if ((j0 & ctrlReg) == ctrlReg) f(a[j0], a[j1]);
-    }
-}
-
-template <class F>
-__device__ __forceinline__ void forAll(double2 (&a)[kRegs], uint32_t ctrlReg, F f) {
-#pragma unroll
-    for (int j = 0; j < kRegs; j++) {
-        if ((j & ctrlReg) == ctrlReg) f(a[j], j);
-    }
-}
-
-#define DGQ_DISPATCH_K(kval, ...)       \
-    switch (kval) {                     \
-        case 0: {                       \
-            constexpr int K = 0;        \
-            __VA_ARGS__;                \
-        } break;                        \
-        case 1: {                       \
-            constexpr int K = 1;        \
-            __VA_ARGS__;                \
-        } break;                        \
-        case 2: {                       \
-            constexpr int K = 2;        \
-            __VA_ARGS__;                \
-        } break;                        \
-        default: {                      \
-            constexpr int K = 3;        \
-            __VA_ARGS__;                \
-        } break;                        \
-    }
-
-template <int KK>
-__device__ __forceinline__ void denseApply(double2 (&a)[kRegs], uint32_t ctrlReg, const double *m) {
-    constexpr int D = 1 << KK;
-#pragma unroll
-    for (int g = 0; g < (kRegs >> KK); g++) {
-        const int base = g << KK;
-        if ((base & ctrlReg) != ctrlReg) continue;
-        double2 v[D];
-#pragma unroll
-        for (int c = 0; c < D; c++) v[c] = a[base + c];
-#pragma unroll
-        for (int r = 0; r < D; r++) {
-            double re = 0.0, im = 0.0;
-#pragma unroll
-            for (int c = 0; c < D; c++) {
-                const double mr = m[2 * (r * D + c)], mi = m[2 * (r * D + c) + 1];
-                re = fma(mr, v[c].x, re);
-                re = fma(-mi, v[c].y, re);
-                im = fma(mr, v[c].y, im);
-                im = fma(mi, v[c].x, im);
-            }
-            a[base + r] = make_double2(re, im);
-        }
-    }
-}
-
-__device__ __forceinline__ void applyOp(const KOp &op, const double *coef, double2 (&a)[kRegs], uint32_t loc,
-                                        uint32_t cta) {
-    if ((cta & op.ctrlCta) != op.ctrlCta || (loc & op.ctrlLoc) != op.ctrlLoc) return;
-    const uint32_t cr = op.ctrlReg;
-    const double *c = coef + op.coef;
-    switch (op.kind) {
-        case KOP_M2R: {
-            const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 nx = make_double2(m0 * x.x + m1 * y.x, m0 * x.y + m1 * y.y);
-                const double2 ny = make_double2(m2 * x.x + m3 * y.x, m2 * x.y + m3 * y.y);
-                x = nx;
-                y = ny;
-            }));
-            break;
-        }
-        case KOP_M2I: {
-            // [[a, i b], [i c, d]]
-            const double m0 = c[0], m1 = c[1], m2 = c[2], m3 = c[3];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 nx = make_double2(m0 * x.x - m1 * y.y, m0 * x.y + m1 * y.x);
-                const double2 ny = make_double2(m3 * y.x - m2 * x.y, m3 * y.y + m2 * x.x);
-                x = nx;
-                y = ny;
-            }));
-            break;
-        }
-        case KOP_M2C: {
-            const double u0 = c[0], u1 = c[1], u2 = c[2], u3 = c[3], u4 = c[4], u5 = c[5], u6 = c[6], u7 = c[7];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 nx = make_double2(u0 * x.x - u1 * x.y + u2 * y.x - u3 * y.y,
-                                                u0 * x.y + u1 * x.x + u2 * y.y + u3 * y.x);
-                const double2 ny = make_double2(u4 * x.x - u5 * x.y + u6 * y.x - u7 * y.y,
-                                                u4 * x.y + u5 * x.x + u6 * y.y + u7 * y.x);
-                x = nx;
-                y = ny;
-            }));
-            break;
-        }
-        case KOP_X:
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 t = x;
-                x = y;
-                y = t;
-            }));
-            break;
-        case KOP_Y:
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 t = x;
-                x = make_double2(y.y, -y.x);
-                y = make_double2(-t.y, t.x);
-            }));
-            break;
-        case KOP_YC:
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](double2 &x, double2 &y) {
-                const double2 t = x;
-                x = make_double2(-y.y, y.x);
-                y = make_double2(t.y, -t.x);
-            }));
-            break;
-        case KOP_NEG:
-            forAll(a, cr, [&](double2 &x, int) { x = make_double2(-x.x, -x.y); });
-            break;
-        case KOP_MULI:
-            forAll(a, cr, [&](double2 &x, int) { x = make_double2(-x.y, x.x); });
-            break;
-        case KOP_MULNI:
-            forAll(a, cr, [&](double2 &x, int) { x = make_double2(x.y, -x.x); });
-            break;
-        case KOP_PH: {
-            const double cs = c[0], sn = c[1];
-            forAll(a, cr, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
-            break;
-        }
-        case KOP_Z2: {
-            const double cs = c[0], sn = c[1];
-            const bool regSel = op.code < KC_Z2T;
-            const uint32_t sr = regSel ? (1u << op.k) : 0u;
-            const bool thrBit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
-            forAll(a, cr, [&](double2 &x, int j) {
-                const bool bit = sr ? ((j & sr) != 0u) : thrBit;
-                const double s = bit ? sn : -sn;
-                x = make_double2(cs * x.x - s * x.y, cs * x.y + s * x.x);
-            });
-            break;
-        }
-        case KOP_RY1: {
-            const double t = c[0];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
-                const double2 x0 = x;
-                x = make_double2(fma(-t, y.x, x0.x), fma(-t, y.y, x0.y));
-                y = make_double2(fma(t, x0.x, y.x), fma(t, x0.y, y.y));
-            }));
-            break;
-        }
-        case KOP_RY2: {
-            const double u = c[0];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
-                const double2 x0 = x;
-                x = make_double2(fma(u, x0.x, -y.x), fma(u, x0.y, -y.y));
-                y = make_double2(fma(u, y.x, x0.x), fma(u, y.y, x0.y));
-            }));
-            break;
-        }
-        case KOP_RX1: {
-            const double t = c[0];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
-                const double2 x0 = x;
-                x = make_double2(fma(t, y.y, x0.x), fma(-t, y.x, x0.y));
-                y = make_double2(fma(t, x0.y, y.x), fma(-t, x0.x, y.y));
-            }));
-            break;
-        }
-        case KOP_RX2: {
-            const double u = c[0];
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
-                const double2 x0 = x;
-                x = make_double2(fma(u, x0.x, y.y), fma(u, x0.y, -y.x));
-                y = make_double2(fma(u, y.x, x0.y), fma(u, y.y, -x0.x));
-            }));
-            break;
-        }
-        case KOP_H1:
-            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](double2 &x, double2 &y) {
-                const double2 x0 = x;
-                x = make_double2(x0.x + y.x, x0.y + y.y);
-                y = make_double2(x0.x - y.x, x0.y - y.y);
-            }));
-            break;
-        case KOP_PH1: {
-            const double cs = c[0], sn = c[1];
-            if (op.code == KC_PH1T) {
-                const bool bit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
-                if (bit) forAll(a, 0u, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
-            } else {
-                const uint32_t sr = 1u << op.k;
-                forAll(a, sr, [&](double2 &x, int) { x = make_double2(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
-            }
-            break;
-        }
-        case KOP_DENSE:
-            switch (op.k) {
-                case 1: denseApply<1>(a, cr, c); break;
-                case 2: denseApply<2>(a, cr, c); break;
-                case 3: denseApply<3>(a, cr, c); break;
-                default: denseApply<4>(a, cr, c); break;
-            }
-            break;
-        default:
-            break;
-    }
-}
 
 // ------------------------------------------------------------ tile kernel
 // 128 registers per thread: 16 warps per SM at every tile width.

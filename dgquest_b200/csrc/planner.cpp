@@ -520,6 +520,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             kp.regOff[j] = (uint16_t) tileSwizzle(loc);
         }
         for (double c : coef) prog->coef[numCoef++] = c;
+        prog->numCoef = (uint16_t) numCoef;
         if (stats) stats->phases++;
     }
     if (stats) stats->gates += (int) block.gates.size();

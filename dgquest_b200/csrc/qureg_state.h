@@ -1,0 +1,68 @@
+// qureg_state.h -- the engine state behind a Qureg handle (shared by the
+// register API in api.cpp and the batched form in batch_host.cpp).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "QuEST.h"
+#include "dgq.h"
+#include "ir.h"
+#include "planner.h"
+#include "tile_program.h"
+
+struct QuregState {
+    int numQubits = 0;  // user-visible qubits
+    int numBits = 0;    // address bits of the buffer (>= numQubits, >= kMinTileBits)
+    bool single = false;  // complex64 amplitudes (float2) instead of complex128
+    void *dState = nullptr;
+    cudaStream_t stream = nullptr;
+
+    // recorded, not yet executed
+    std::vector<dgq::Gate> pending;
+    dgq::MatrixPool pool;
+    bool initPending = false;
+    int32_t initKind = dgq::INIT_NONE;
+    uint64_t initIndex = 0;
+    double initAmp = 0.0;
+
+    // lazy measurement collapse applied to the state in HBM
+    bool restrictActive = false;
+    uint64_t rMask = 0, rValue = 0;
+    double rScale = 1.0;
+
+    // logical qubit -> address bit (swapGate relabels instead of moving data)
+    int l2v[64];
+    int v2l[64];
+
+    // P(bit = 0) per address bit, of the (collapsed, normalised) state
+    bool probsValid = false;
+    std::vector<double> p0;
+    double totalProb = 1.0;
+    double *dPartial = nullptr;
+    size_t partialCap = 0;
+    double *dProbOut = nullptr;
+    double *dNorm = nullptr;  // complex64 renormalisation: two running sums of |a|^2
+
+    int tileBitsSetting = 0;  // 0 = cost model
+    std::vector<dgq::TileProgram> planned;
+    std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)
+    int plannedTileBits = 0;
+    dgq_plan_stats stats{};
+};
+
+namespace dgq {
+
+// Plans the register's pending gates (and pending initialisation or
+// collapse) into sweep programs of tile width W. Returns 0, or the QuEST
+// error code with err set. The register is not changed.
+int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err);
+// Drops the pending work that buildPrograms planned (after it has been
+// launched or kept for launching).
+void consumePending(QuregState &s);
+
+}  // namespace dgq

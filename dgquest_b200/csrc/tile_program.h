@@ -135,7 +135,8 @@ struct TileProgram {
     double restrictScale;
     uint8_t highPos[kMaxTileBits - kCoalescedBits];  // address bit of tile-local bit 5 + i
     uint8_t ctaPos[kMaxStateBits];                   // address bit of blockIdx bit i
-    uint8_t pad0[4];
+    uint16_t numCoef;  // coefficients used (coef[0 .. numCoef))
+    uint8_t pad0[2];
     KPhase phases[kMaxPhases];
     KOp ops[kMaxOps];
     double coef[kMaxCoef];

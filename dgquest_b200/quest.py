@@ -66,6 +66,32 @@ class PlanStats(Structure):
     ]
 
 
+class BatchConfig(Structure):
+    _fields_ = [("tileBits", ctypes.c_int32), ("groupFactor", ctypes.c_int32), ("ctasPerSm", ctypes.c_int32),
+                ("tune", ctypes.c_int32)]
+
+
+class BatchStats(Structure):
+    _fields_ = [
+        ("registers", ctypes.c_int32),
+        ("wholeRegisters", ctypes.c_int32),
+        ("sweeps", ctypes.c_int32),
+        ("tileBits", ctypes.c_int32),
+        ("groupFactor", ctypes.c_int32),
+        ("grid", ctypes.c_int32),
+        ("ctasPerSm", ctypes.c_int32),
+        ("tuned", ctypes.c_int32),
+        ("items", ctypes.c_int64),
+        ("gates", ctypes.c_int64),
+        ("programBytes", ctypes.c_int64),
+        ("stateBytes", ctypes.c_int64),
+        ("sweepBytes", ctypes.c_int64),
+        ("planMillis", c_double),
+        ("tuneMillis", c_double),
+        ("flopsPerLaunch", c_double),
+    ]
+
+
 class QuESTError(RuntimeError):
     def __init__(self, code, message):
         super().__init__(f"[{code}] {message}")
@@ -161,6 +187,14 @@ _SIGS = {
     "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),
+    "dgq_applyCircuit": (I, [Q, c_void_p, I, P(I)]),
+    "dgq_batchCreate": (c_void_p, [P(Qureg), I, P(BatchConfig)]),
+    "dgq_batchLaunch": (I, [c_void_p]),
+    "dgq_batchWait": (I, [c_void_p]),
+    "dgq_batchExpectationZ": (I, [c_void_p, P(D)]),
+    "dgq_batchGetStats": (I, [c_void_p, P(BatchStats)]),
+    "dgq_batchGetStream": (c_void_p, [c_void_p]),
+    "dgq_batchDestroy": (None, [c_void_p]),
 }
 
 _lib = None
@@ -253,8 +287,63 @@ def seed(keys):
     seedQuEST(arr, len(keys))
 
 
+def apply_circuit(q, ops):
+    """Records an op list (circuits.OP_DTYPE records, the dgq_gate_record
+    layout) through dgq_applyCircuit in one call; returns measurement outcomes."""
+    ops = np.ascontiguousarray(ops)
+    assert ops.dtype.itemsize == 80
+    n_meas = int((ops["kind"] == 24).sum()) if len(ops) else 0
+    out = (c_int * max(1, n_meas))()
+    dgq_applyCircuit(q, ops.ctypes.data if len(ops) else None, len(ops), out)
+    return [int(out[i]) for i in range(n_meas)]
+
+
 def init_from_amps(q, amps):
     amps = np.ascontiguousarray(amps, dtype=np.complex128)
     re = np.ascontiguousarray(amps.real)
     im = np.ascontiguousarray(amps.imag)
     initStateFromAmps(q, re.ctypes.data_as(POINTER(c_double)), im.ctypes.data_as(POINTER(c_double)))
+
+
+class Batch:
+    """A dgq_batch over registers whose gates are already recorded.
+
+    config: None (autotuned) or a dict with tileBits / groupFactor / ctasPerSm / tune."""
+
+    def __init__(self, quregs, config=None):
+        self.quregs = list(quregs)
+        self.handle = None
+        arr = (Qureg * len(self.quregs))(*self.quregs)
+        cfg = None
+        if config is not None:
+            cfg = BatchConfig(int(config.get("tileBits", 0)), int(config.get("groupFactor", 0)),
+                              int(config.get("ctasPerSm", 0)), int(config.get("tune", 0)))
+        self.handle = dgq_batchCreate(arr, len(self.quregs), ctypes.byref(cfg) if cfg is not None else None)
+        if not self.handle:
+            raise QuESTError(-1, "dgq_batchCreate returned NULL")
+        self.num_values = sum(int(q.numQubitsRepresented) for q in self.quregs)
+
+    def launch(self):
+        dgq_batchLaunch(self.handle)
+
+    def wait(self):
+        dgq_batchWait(self.handle)
+
+    def expectation_z(self):
+        out = np.empty(self.num_values, dtype=np.float64)
+        dgq_batchExpectationZ(self.handle, out.ctypes.data_as(POINTER(c_double)))
+        return out
+
+    def stats(self):
+        st = BatchStats()
+        dgq_batchGetStats(self.handle, ctypes.byref(st))
+        return st
+
+    def stream(self):
+        return dgq_batchGetStream(self.handle)
+
+    def close(self):
+        if self.handle:
+            dgq_batchDestroy(self.handle)
+            self.handle = None
+

@@ -134,6 +134,75 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
                     int len);
 int dgq_compileSweepSource(const char *source, char *log, int len);
 
+/* Circuit records: one 80-byte record per API call, applied in order
+ * through the entry points of QuEST.h (same validation, same lazy
+ * recording). kind: 0 hadamard, 1 pauliX, 2 pauliY, 3 pauliZ, 4 sGate,
+ * 5 tGate, 6 rotateX, 7 rotateY, 8 rotateZ, 9 phaseShift (angle p[0]),
+ * 10 controlledNot, 11 controlledPhaseFlip, 12 controlledPhaseShift,
+ * 13 controlledRotateX, 14 controlledRotateY, 15 controlledRotateZ
+ * (control q0, target q1, angle p[0]), 16 compactUnitary (alpha p[0..1],
+ * beta p[2..3]), 17 controlledCompactUnitary (control q0, target q1),
+ * 18 unitary (ComplexMatrix2 as r0c0 r0c1 r1c0 r1c1 re/im pairs in p),
+ * 19 controlledUnitary, 20 SqX, 21 SqY, 22 SqW, 23 swapGate (q0, q1),
+ * 24 measure (outcome appended to outcomes), 25 controlledPauliY.
+ * No counterpart in dgQuEST (its callers make one API call per gate).
+ * Returns the number of records applied, or -1 at the first record the
+ * API rejected (error mode "record") or with an unknown kind. */
+typedef struct dgq_gate_record {
+    int32_t kind;
+    int32_t q0, q1, q2;
+    double p[8];
+} dgq_gate_record;
+int dgq_applyCircuit(Qureg qureg, const dgq_gate_record *records, int count, int *outcomes);
+
+/* ---------------------------------------------------------------- batches
+ * Batched form (no counterpart in dgQuEST, which runs one register at a
+ * time). The pending gates of many registers -- recorded through the usual
+ * API calls, one precision per batch -- are planned together and run by ONE
+ * persistent kernel launch, captured in a CUDA graph with the resets it
+ * needs. CTAs take (register, sweep, tile) work items in order and wait, on
+ * device counters, for the previous sweep of the same register.
+ * Each launch recomputes every register from its recorded initialisation,
+ * so a batch can be launched repeatedly when every register starts with
+ * initZeroState / initPlusState / initClassicalState; the states hold the
+ * final amplitudes after each launch (getAmp etc. work as usual). */
+typedef struct dgq_batch_s *dgq_batch;
+typedef struct dgq_batch_config {
+    int32_t tileBits;     /* widest tile, 9..12 (registers narrower than it use their width); 0 = choose */
+    int32_t groupFactor;  /* registers interleaved sweep by sweep: about groupFactor x grid tiles; 0 = choose */
+    int32_t ctasPerSm;    /* persistent CTAs per SM; 0 = as many as fit */
+    int32_t tune;         /* 1: time candidate tile widths and group factors on a sample of the batch */
+} dgq_batch_config;
+typedef struct dgq_batch_stats {
+    int32_t registers;
+    int32_t wholeRegisters;  /* registers that fit one tile: one item runs all their sweeps */
+    int32_t sweeps;          /* sweep programs over all registers */
+    int32_t tileBits;
+    int32_t groupFactor;
+    int32_t grid;            /* persistent CTAs */
+    int32_t ctasPerSm;
+    int32_t tuned;           /* 1 when the autotuner ran for this batch */
+    int64_t items;           /* work items per launch */
+    int64_t gates;           /* recorded gates (before merging) */
+    int64_t programBytes;    /* device bytes of programs and work list (uploaded once) */
+    int64_t stateBytes;      /* amplitude bytes of all registers */
+    int64_t sweepBytes;      /* algorithmic HBM bytes of one launch: sum over sweeps of 2 x state bytes */
+    double planMillis;       /* host planning and packing */
+    double tuneMillis;       /* autotuning (0 when a cached choice was used) */
+    double flopsPerLaunch;   /* algorithmic flops of one launch */
+} dgq_batch_stats;
+/* cfg NULL: autotuned (the choice is cached per precision and register-size
+ * histogram; DGQ_BATCH_TUNE=0 disables tuning). Returns NULL on error. */
+dgq_batch dgq_batchCreate(const Qureg *quregs, int count, const dgq_batch_config *cfg);
+int dgq_batchLaunch(dgq_batch batch);   /* replays the graph; does not wait */
+int dgq_batchWait(dgq_batch batch);     /* waits and checks the kernel's wait-timeout flag */
+/* Waits, then writes <Z_q> = P(q=0) - P(q=1) of every register's qubits,
+ * register by register (sum of numQubits values). */
+int dgq_batchExpectationZ(dgq_batch batch, double *out);
+int dgq_batchGetStats(dgq_batch batch, dgq_batch_stats *out);
+void *dgq_batchGetStream(dgq_batch batch);
+void dgq_batchDestroy(dgq_batch batch);
+
 #ifdef __cplusplus
 }
 #endif
