@@ -238,11 +238,12 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
     }
 }
 
+// The kernel's dynamic shared-memory limit is set once, to the widest tile,
+// by ctasPerSmV (called before any launch is recorded), so that launches
+// recorded in graphs stay valid whatever tile width later batches use.
 template <class V>
 cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, cudaStream_t s) {
     const size_t smem = sizeof(V) << maxTileBits;
-    cudaError_t e = cudaFuncSetAttribute(batchKernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    if (e != cudaSuccess) return e;
     batchKernel<V><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
     return cudaGetLastError();
 }
@@ -250,7 +251,8 @@ cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, cudaStre
 template <class V>
 int ctasPerSmV(int maxTileBits) {
     const size_t smem = sizeof(V) << maxTileBits;
-    if (cudaFuncSetAttribute(batchKernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(batchKernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) (sizeof(V) << kBatchMaxTileBits)) != cudaSuccess)
         return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<V>, 1 << (maxTileBits - kRegBits), smem) !=

@@ -277,7 +277,7 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
     a.coef = d.coef;
     a.items = d.items;
     a.numItems = (uint32_t) d.numItems;
-    a.spinLimit = 1u << 24;  // polls of >= 256 ns each: several seconds
+    a.spinLimit = 1u << 22;  // polls of >= 256 ns each: a second or more
     a.ticket = d.counters;
     a.done = d.counters;
     a.zsum = d.zsum;
@@ -391,6 +391,9 @@ dgq_batch dgq_batchCreate(const Qureg *quregs, int count, const dgq_batch_config
         if (!s->initPending) allInit = false;
         maxBits = std::max(maxBits, s->numBits);
     }
+    // work items carry the register in 20 bits, the sweep in 16 and the tile in 28
+    if (count > (1 << 20)) return abandon(E_INVALID_ARGUMENT, "more than 2^20 registers");
+    if (maxBits - dgq::kMinTileBits > 28) return abandon(E_UNSUPPORTED, "a register wider than 37 qubits");
     {
         std::vector<QuregState *> sorted = b->regs;
         std::sort(sorted.begin(), sorted.end());
@@ -465,6 +468,10 @@ dgq_batch dgq_batchCreate(const Qureg *quregs, int count, const dgq_batch_config
     double flops = 0.0;
     int64_t gates = 0;
     for (int i = 0; i < count; i++) {
+        if (!plans[i].err && plans[i].sweeps.size() >= dgq::kBatchWhole) {
+            plans[i].err = E_UNSUPPORTED;
+            plans[i].errMsg = "a register needs 65535 or more sweeps";
+        }
         if (plans[i].err) {
             const std::string msg = plans[i].errMsg;
             return abandon(plans[i].err, msg.c_str());

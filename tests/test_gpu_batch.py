@@ -95,7 +95,9 @@ def test_batch_relaunch_is_idempotent(quest, env):
     for _ in range(3):
         b.launch()
     z2 = b.expectation_z()
-    assert np.array_equal(z1, z2)
+    # amplitudes repeat bit for bit; <Z> sums are accumulated by atomics in
+    # whatever order the CTAs finish, so they repeat to rounding
+    assert np.abs(z1 - z2).max() <= 1e-14
     for q, a in zip(regs, amps1):
         assert np.array_equal(Q.state_vector(q), a)
     b.close()
