@@ -317,10 +317,31 @@ def run_gpu(args, world, rank, local):
 
 
 def run_ncu_case(args):
-    """One plan of the random circuit on a small register, run twice (ncu: -s skips the first)."""
+    """One plan of the random circuit on a small register, run twice (ncu: -s skips the first);
+    with --batch-case K, the first K circuits of the batched workload as one batch, launched twice."""
     from dgquest_b200 import circuits as C
     from dgquest_b200 import quest as Q
     env = Q.createQuESTEnv()
+    if args.batch_case:
+        single = args.precision == 1
+        regs = []
+        for n, d, ops in C.batch_workload(args.batch_case):
+            q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+            Q.initZeroState(q)
+            Q.apply_circuit(q, ops)
+            regs.append(q)
+        b = Q.Batch(regs, {"tileBits": args.tile_bits or 12, "groupFactor": 2})
+        for _ in range(2):
+            b.launch()
+        z = b.expectation_z()
+        st = b.stats()
+        print(json.dumps({"case": "batch", "circuits": len(regs), "items": int(st.items), "sweeps": st.sweeps,
+                          "sweep_bytes": int(st.sweepBytes), "z_abs_max": float(np.abs(z).max())}))
+        b.close()
+        for q in regs:
+            Q.destroyQureg(q, env)
+        Q.destroyQuESTEnv(env)
+        return
     q = Q.dgq_createQuregF32(args.qubits, env) if args.precision == 1 else Q.createQureg(args.qubits, env)
     if args.tile_bits:
         Q.dgq_setTileBits(q, args.tile_bits)
@@ -405,6 +426,30 @@ def run_batch_form(args, world):
     return out
 
 
+def run_serving_form(args, world):
+    """Serving loop: Poisson arrivals at 200 requests/s, n uniform in [16, 33]
+    (complex64) or [16, 32] (complex128), 40/30/30 random / GHZ+QFT / BV,
+    1024 samples and <Z> on 4 qubits per request; the first --serve-requests
+    requests of the stream, admitted by state bytes against free HBM."""
+    from dgquest_b200 import quest as Q
+    from dgquest_b200 import serving as S
+    env = Q.createQuESTEnv()
+    out = {"workload": "Poisson arrivals 200/s; random(depth 8-24)/GHZ+QFT/BV 40/30/30; 1024 samples + <Z> on 4 qubits",
+           "requests_per_precision": args.serve_requests}
+    for name, single in (("complex64", True), ("complex128", False)):
+        reqs = S.make_requests(args.serve_requests, rate=200.0, single=single)
+        srv = S.Server(env, workers=args.serve_workers)
+        res = srv.serve(reqs, realtime=True)
+        st = S.summarize(res)
+        st.update({"peak_in_flight": srv.peak_in_flight, "peak_state_gb": srv.peak_in_use / 1e9,
+                   "budget_gb": srv.budget / 1e9, "offered_rate": 200.0,
+                   "offered_state_gb_per_s": sum(S.state_bytes(r) for r in reqs) / reqs[-1].arrival / 1e9,
+                   "n_range": [min(r.n for r in reqs), max(r.n for r in reqs)]})
+        out[name] = st
+    Q.destroyQuESTEnv(env)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,6 +466,10 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-circuits", type=int, default=4096)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--batch-case", type=int, default=0, help="--ncu-case: a batch of this many workload circuits")
+    ap.add_argument("--serve-requests", type=int, default=120)
+    ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--precision", type=int, default=2, choices=[1, 2], help="--ncu-case register precision")
     ap.add_argument("--ncu-case", action="store_true",
                     help="run one small case once (for ncu captures): --qubits/--depth/--tile-bits, specialised kernels")
@@ -442,6 +491,8 @@ def main():
         batch = run_batch_form(args, world)
         if rank == 0:
             line["batched_form"] = batch
+    if not args.no_serve and rank == 0:
+        line["serving"] = run_serving_form(args, world)
     if rank == 0 and world == 1 and not args.no_cpu:
         from dgquest_b200 import circuits as C
         ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))

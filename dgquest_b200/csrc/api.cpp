@@ -373,6 +373,56 @@ bool launchPlanned(QuregState &s, const char *func) {
     return true;
 }
 
+// Register memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// register's stream, from the device's default pool with no release
+// threshold): creating or destroying one register neither waits for nor
+// serialises kernels that other registers run on their own streams, and
+// freed states are reused by later registers without returning to the driver.
+cudaMemPool_t registerPool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPool_t p = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&p, dev) != cudaSuccess) return nullptr;
+        uint64_t keep = ~0ULL;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
+// Bytes the pool holds but no register uses.
+size_t poolSpare() {
+    cudaMemPool_t p = registerPool();
+    if (!p) return 0;
+    uint64_t reserved = 0, used = 0;
+    cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &used);
+    return reserved > used ? (size_t) (reserved - used) : 0;
+}
+
+cudaError_t allocOn(void **ptr, size_t bytes, cudaStream_t st) {
+    *ptr = nullptr;
+    cudaError_t e = cudaMallocAsync(ptr, bytes, st);
+    if (e == cudaErrorMemoryAllocation) {
+        // pool blocks of other sizes may hold the memory: hand them back, retry
+        cudaGetLastError();
+        if (cudaMemPool_t p = registerPool()) {
+            cudaStreamSynchronize(st);
+            cudaMemPoolTrimTo(p, 0);
+        }
+        e = cudaMallocAsync(ptr, bytes, st);
+    }
+    return e;
+}
+
+void freeOn(void *ptr, cudaStream_t st) {
+    if (ptr) cudaFreeAsync(ptr, st);
+}
+
 bool flush(QuregState &s, const char *func) {
     if (s.pending.empty() && !s.initPending) return true;
     if (!planPending(s, func)) return false;
@@ -394,9 +444,9 @@ bool ensureProbs(QuregState &s, const char *func) {
     a.rValue = s.restrictActive ? s.rValue : 0;
     const size_t need = (size_t) dgq::probNumCtas(a) * 17;
     if (need > s.partialCap) {
-        if (s.dPartial) cudaFree(s.dPartial);
+        freeOn(s.dPartial, s.stream);
         s.dPartial = nullptr;
-        if (!cudaOk(cudaMalloc(&s.dPartial, need * sizeof(double)), func)) return false;
+        if (!cudaOk(allocOn((void **) &s.dPartial, need * sizeof(double), s.stream), func)) return false;
         s.partialCap = need;
     }
     if (!cudaOk(dgq::launchProb(s.dState, s.single, a, s.dPartial, s.dProbOut, s.stream), func)) return false;
@@ -575,6 +625,54 @@ int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes
     return count;
 }
 
+int dgq_sampleOutcomes(Qureg q, int numSamples, uint32_t seed, uint64_t *outcomes) {
+    if (!vQureg(q, __func__)) return -1;
+    if (numSamples < 0 || (numSamples > 0 && !outcomes))
+        return raise(E_INVALID_ARGUMENT, __func__, "numSamples < 0 or null output") ? 0 : -1;
+    QuregState &s = *stateOf(q);
+    if (!flush(s, __func__)) return -1;
+    if (numSamples == 0) return 0;
+    dgq::Mt19937 rng;
+    rng.seed(seed);
+    std::vector<double> u((size_t) numSamples);
+    for (double &x : u) x = rng.res53();
+    dgq::SampleArgs a;
+    a.numAmps = 1ULL << s.numBits;
+    a.restrictMask = s.restrictActive ? s.rMask : 0;
+    a.restrictValue = s.restrictActive ? s.rValue : 0;
+    a.restrictScale2 = s.restrictActive ? s.rScale * s.rScale : 1.0;
+    const size_t runs = (size_t) dgq::sampleScratchCount(a.numAmps);
+    void *scratch = nullptr;
+    const size_t bytes = runs * sizeof(double) + (size_t) numSamples * (sizeof(double) + sizeof(uint64_t));
+    if (!cudaOk(allocOn(&scratch, bytes, s.stream), __func__)) return -1;
+    double *dSums = (double *) scratch;
+    double *dU = dSums + runs;
+    uint64_t *dOut = (uint64_t *) (dU + numSamples);
+    std::vector<uint64_t> v((size_t) numSamples);
+    bool ok = cudaOk(cudaMemcpyAsync(dU, u.data(), u.size() * sizeof(double), cudaMemcpyHostToDevice, s.stream),
+                     __func__) &&
+              cudaOk(dgq::launchSample(s.dState, s.single, a, dSums, dU, numSamples, dOut, s.stream), __func__) &&
+              cudaOk(cudaMemcpyAsync(v.data(), dOut, v.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost, s.stream),
+                     __func__);
+    freeOn(scratch, s.stream);
+    ok = ok && cudaOk(cudaStreamSynchronize(s.stream), __func__);
+    if (!ok) return -1;
+    g_launches += 3;
+    for (int k = 0; k < numSamples; k++) {
+        uint64_t logical = 0;
+        for (int b = 0; b < s.numQubits; b++)
+            if ((v[(size_t) k] >> s.l2v[b]) & 1ULL) logical |= 1ULL << b;
+        outcomes[k] = logical;
+    }
+    return 0;
+}
+
+int64_t dgq_getAvailableMemory(void) {
+    size_t freeB = 0, totalB = 0;
+    if (!cudaOk(cudaMemGetInfo(&freeB, &totalB), __func__)) return -1;
+    return (int64_t) (freeB + poolSpare());
+}
+
 int dgq_getLastError(char *msg, int len) {
     std::lock_guard<std::mutex> lk(g_errMutex);
     const int code = g_lastError;
@@ -647,16 +745,23 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
         delete s;
         return q;
     }
-    if (bytes + (64u << 20) > freeB) {
+    if (bytes + (64u << 20) > freeB + poolSpare()) {
         delete s;
         raise(E_SYS_TOO_BIG_FOR_DEVICE, func);
         return q;
     }
-    if (!cudaOk(cudaMalloc(&s->dState, bytes), func) ||
-        !cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func) ||
-        !cudaOk(cudaMalloc(&s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1)), func) ||
-        !cudaOk(cudaMalloc(&s->dNorm, sizeof(double) * 2), func)) {
-        if (s->dState) cudaFree(s->dState);
+    if (!cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func)) {
+        delete s;
+        return q;
+    }
+    if (!registerPool() || !cudaOk(allocOn(&s->dState, bytes, s->stream), func) ||
+        !cudaOk(allocOn((void **) &s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1), s->stream), func) ||
+        !cudaOk(allocOn((void **) &s->dNorm, sizeof(double) * 2, s->stream), func) ||
+        !cudaOk(cudaStreamSynchronize(s->stream), func)) {
+        freeOn(s->dState, s->stream);
+        freeOn(s->dProbOut, s->stream);
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
         delete s;
         return q;
     }
@@ -694,12 +799,15 @@ void destroyQureg(Qureg qureg, QuESTEnv env) {
     (void) env;
     QuregState *s = qureg.state;
     if (!s) return;
-    if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->dState) cudaFree(s->dState);
-    if (s->dPartial) cudaFree(s->dPartial);
-    if (s->dProbOut) cudaFree(s->dProbOut);
-    if (s->dNorm) cudaFree(s->dNorm);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->stream) {
+        cudaStreamSynchronize(s->stream);
+        freeOn(s->dState, s->stream);
+        freeOn(s->dPartial, s->stream);
+        freeOn(s->dProbOut, s->stream);
+        freeOn(s->dNorm, s->stream);
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
     delete s;
 }
 

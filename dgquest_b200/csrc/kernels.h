@@ -42,6 +42,18 @@ struct InnerArgs {
     uint8_t l2vKet[kMaxStateBits];
 };
 
+struct SampleArgs {
+    uint64_t numAmps;
+    uint64_t restrictMask, restrictValue;  // lazy collapse (mask 0: none)
+    double restrictScale2;                 // its scale squared
+};
+
+// Samples: `count` addresses drawn from |amp|^2 by the uniforms in [0, 1);
+// sums holds sampleScratchCount(numAmps) doubles of scratch.
+cudaError_t launchSample(const void *st, bool single, const SampleArgs &a, double *sums, const double *uniforms,
+                         int count, uint64_t *out, cudaStream_t s);
+uint64_t sampleScratchCount(uint64_t numAmps);
+
 cudaError_t launchInner(const void *bra, bool braSingle, const void *ket, bool ketSingle, const InnerArgs &args,
                         double2 *partial, double2 *out, cudaStream_t s);
 int innerNumCtas();

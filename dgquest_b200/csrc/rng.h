@@ -52,6 +52,11 @@ public:
 
     // uniform on [0, 1], the 32-bit draw over 2^32 - 1
     double real1() { return (double) next() * (1.0 / 4294967295.0); }
+    // uniform on [0, 1) with 53 bits: (a >> 5) * 2^26 + (b >> 6), over 2^53
+    double res53() {
+        const uint32_t a = next() >> 5, b = next() >> 6;
+        return ((double) a * 67108864.0 + (double) b) * (1.0 / 9007199254740992.0);
+    }
 
 private:
     static constexpr int N = 624, M = 397;

@@ -188,6 +188,8 @@ _SIGS = {
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),
     "dgq_applyCircuit": (I, [Q, c_void_p, I, P(I)]),
+    "dgq_sampleOutcomes": (I, [Q, I, ctypes.c_uint32, P(ctypes.c_uint64)]),
+    "dgq_getAvailableMemory": (c_int64, []),
     "dgq_batchCreate": (c_void_p, [P(Qureg), I, P(BatchConfig)]),
     "dgq_batchLaunch": (I, [c_void_p]),
     "dgq_batchWait": (I, [c_void_p]),
@@ -296,6 +298,13 @@ def apply_circuit(q, ops):
     out = (c_int * max(1, n_meas))()
     dgq_applyCircuit(q, ops.ctypes.data if len(ops) else None, len(ops), out)
     return [int(out[i]) for i in range(n_meas)]
+
+
+def sample(q, count, seed):
+    """dgq_sampleOutcomes: `count` logical basis-state indices drawn from |amp|^2."""
+    out = np.empty(max(1, count), dtype=np.uint64)
+    dgq_sampleOutcomes(q, count, seed & 0xFFFFFFFF, out.ctypes.data_as(POINTER(ctypes.c_uint64)))
+    return out[:count]
 
 
 def init_from_amps(q, amps):

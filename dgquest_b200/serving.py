@@ -1,0 +1,214 @@
+"""Serving loop: circuits arriving as a Poisson stream, admitted by state bytes
+against free HBM, run concurrently (continuous batching).
+
+Every admitted request gets its own register, and so its own CUDA stream and
+its own stream-ordered allocation: requests that arrive while others are on
+the GPU start as soon as a worker slot and enough memory are free, and their
+kernels overlap on the device with the ones already running. A request's
+result depends only on the request (its circuit, its sample seed), never on
+what else is in flight, which is what the mix-invariance test checks.
+
+Request i of a stream (seeded MT19937, published algorithm):
+  arrival gap -ln(1 - u) / rate; n uniform in [16, 33] (complex64) or
+  [16, 32] (complex128); kind 40 % random layers (depth uniform in [8, 24]),
+  30 % GHZ+QFT, 30 % Bernstein-Vazirani; 4 distinct qubits for <Z>.
+Each request returns 1024 sampled bitstrings and <Z_q> on its 4 qubits.
+
+No counterpart in dgQuEST, which runs one circuit per process."""
+import collections
+import math
+import threading
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import circuits as C
+from . import quest as Q
+
+SAMPLES = 1024
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str       # "random" | "ghzqft" | "bv"
+    n: int
+    depth: int      # random-layer depth (0 for the other kinds)
+    seed: int       # circuit seed
+    arrival: float  # seconds after the stream starts
+    zq: tuple       # qubits whose <Z> is returned
+    sample_seed: int
+    single: bool    # complex64 register
+
+
+@dataclass
+class Result:
+    rid: int
+    samples: np.ndarray
+    expz: np.ndarray
+    arrival: float
+    admitted: float
+    done: float
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def make_requests(count, rate=200.0, single=False, seed=None, n_range=None):
+    rng = C.Mt19937(C.config_seed(5) if seed is None else seed)
+    lo, hi = n_range or ((16, 33) if single else (16, 32))
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += -math.log(1.0 - rng.uniform()) / rate
+        n = lo + rng.below(hi - lo + 1)
+        u = rng.uniform()
+        kind = "random" if u < 0.4 else ("ghzqft" if u < 0.7 else "bv")
+        depth = 8 + rng.below(17) if kind == "random" else 0
+        zq = []
+        while len(zq) < min(4, n):
+            q = rng.below(n)
+            if q not in zq:
+                zq.append(q)
+        out.append(Request(i, kind, n, depth, C.config_seed(5, i), t, tuple(zq), C.config_seed(5, 100000 + i),
+                           single))
+    return out
+
+
+def request_ops(r):
+    if r.kind == "random":
+        return C.random_layers(r.n, r.depth, r.seed)
+    if r.kind == "ghzqft":
+        return C.ghz_qft(r.n)
+    return C.bernstein_vazirani(r.n, r.seed, measure=False)
+
+
+def state_bytes(r):
+    return (8 if r.single else 16) << max(r.n, 9)
+
+
+def run_request(r, env, ops=None):
+    """One request on its own register: samples and <Z> (2 P(q=0) - 1)."""
+    q = Q.dgq_createQuregF32(r.n, env) if r.single else Q.createQureg(r.n, env)
+    try:
+        Q.apply_circuit(q, request_ops(r) if ops is None else ops)
+        samples = Q.sample(q, SAMPLES, r.sample_seed)
+        expz = np.array([2.0 * Q.calcProbOfOutcome(q, k, 0) - 1.0 for k in r.zq])
+    finally:
+        Q.destroyQureg(q, env)
+    return samples, expz
+
+
+class Server:
+    """Admission by state bytes, `workers` requests in flight at most.
+
+    A waiting request is admitted when its state fits in the budget next to
+    the states in flight; requests behind one that does not fit may go first
+    (first fit in arrival order) until it has been passed over `max_bypass`
+    times, after which nothing else is admitted before it."""
+
+    def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None):
+        self.env = env
+        self.runner = runner or (lambda r: run_request(r, env))
+        self.peak_in_use = 0
+        self.peak_in_flight = 0
+        if hbm_budget is None:
+            # free HBM (with the register pool's spare memory), less a margin
+            # for the per-request scratch and the specialised kernels
+            hbm_budget = int(Q.dgq_getAvailableMemory() * 0.9)
+        self.budget = int(hbm_budget)
+        self.workers = int(workers)
+        self.max_bypass = int(max_bypass)
+
+    def serve(self, requests, realtime=True):
+        """Runs the stream; returns results in request order. With realtime,
+        request i becomes visible at its arrival time, else all at once."""
+        requests = sorted(requests, key=lambda r: r.arrival)
+        for r in requests:
+            if state_bytes(r) > self.budget:
+                raise ValueError(f"request {r.rid}: {state_bytes(r)} state bytes exceed the budget {self.budget}")
+        cond = threading.Condition()
+        waiting = collections.deque()
+        bypassed = collections.Counter()
+        state = {"in_use": 0, "in_flight": 0, "arrived": 0, "finished": 0, "error": None}
+        results = {}
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0  # noqa: E731
+
+        def arrivals():
+            for r in requests:
+                if realtime:
+                    dt = r.arrival - now()
+                    if dt > 0:
+                        time.sleep(dt)
+                with cond:
+                    waiting.append(r)
+                    state["arrived"] += 1
+                    cond.notify_all()
+
+        def pick():
+            # called with the lock held: first fit, head reserved once bypassed enough
+            for i, r in enumerate(waiting):
+                if state["in_use"] + state_bytes(r) <= self.budget:
+                    for j in range(i):
+                        bypassed[waiting[j].rid] += 1
+                    del waiting[i]
+                    return r
+                if bypassed[r.rid] >= self.max_bypass:
+                    return None
+            return None
+
+        def worker():
+            while True:
+                with cond:
+                    while True:
+                        if state["error"] is not None:
+                            return
+                        r = pick()
+                        if r is not None:
+                            break
+                        if state["arrived"] == len(requests) and not waiting:
+                            return
+                        cond.wait(0.05)
+                    state["in_use"] += state_bytes(r)
+                    state["in_flight"] += 1
+                    self.peak_in_use = max(self.peak_in_use, state["in_use"])
+                    self.peak_in_flight = max(self.peak_in_flight, state["in_flight"])
+                    admitted = now()
+                try:
+                    samples, expz = self.runner(r)
+                except Exception as exc:  # noqa: BLE001
+                    with cond:
+                        state["error"] = exc
+                        cond.notify_all()
+                    return
+                with cond:
+                    state["in_use"] -= state_bytes(r)
+                    state["in_flight"] -= 1
+                    state["finished"] += 1
+                    results[r.rid] = Result(r.rid, samples, expz, r.arrival, admitted, now())
+                    cond.notify_all()
+
+        feeder = threading.Thread(target=arrivals, daemon=True)
+        pool = [threading.Thread(target=worker, daemon=True) for _ in range(self.workers)]
+        feeder.start()
+        for t in pool:
+            t.start()
+        feeder.join()
+        for t in pool:
+            t.join()
+        if state["error"] is not None:
+            raise state["error"]
+        return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
+
+
+def summarize(results):
+    lat = np.array([r.latency for r in results]) * 1e3
+    first = min(r.arrival for r in results)
+    last = max(r.done for r in results)
+    return {"requests": len(results), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "circuits_per_s": len(results) / (last - first) if last > first else float("nan"),
+            "wall_s": last - first}

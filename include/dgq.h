@@ -155,6 +155,23 @@ typedef struct dgq_gate_record {
 } dgq_gate_record;
 int dgq_applyCircuit(Qureg qureg, const dgq_gate_record *records, int count, int *outcomes);
 
+/* Draws numSamples basis states from |amp|^2 of the register (after its
+ * pending gates run) and writes them as logical indices (bit q = qubit q).
+ * Sample k uses the k-th 53-bit uniform u of MT19937 seeded with
+ * init_genrand(seed) ((a >> 5) * 2^26 + (b >> 6) over 2^53) and is the
+ * smallest address of the state buffer whose cumulative probability
+ * exceeds u x total; registers without swapGate calls keep addresses in
+ * logical order. The state is not changed. Deterministic for a given state
+ * and seed. No counterpart in dgQuEST (its measure is single-shot and
+ * unimplemented). */
+int dgq_sampleOutcomes(Qureg qureg, int numSamples, uint32_t seed, uint64_t *outcomes);
+
+/* Device bytes new registers can use on the current device: free memory
+ * plus what the registers' stream-ordered pool holds unused (register
+ * memory is allocated and freed in stream order, so destroyed registers'
+ * states are kept for reuse instead of being returned). */
+int64_t dgq_getAvailableMemory(void);
+
 /* ---------------------------------------------------------------- batches
  * Batched form (no counterpart in dgQuEST, which runs one register at a
  * time). The pending gates of many registers -- recorded through the usual

@@ -1,0 +1,71 @@
+"""Serving loop host logic on the CPU: the request stream and the admission
+controller (with a stand-in for the GPU work)."""
+import threading
+import time
+
+import numpy as np
+
+from dgquest_b200 import serving as S
+
+
+def test_request_stream_shape():
+    reqs = S.make_requests(2000, rate=200.0, single=True)
+    arr = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arr) > 0)
+    # mean gap 1/rate within a few percent over 2000 draws
+    assert abs(arr[-1] / len(reqs) - 1 / 200.0) < 0.1 / 200.0
+    ns = np.array([r.n for r in reqs])
+    assert ns.min() == 16 and ns.max() == 33
+    kinds = [r.kind for r in reqs]
+    frac = {k: kinds.count(k) / len(kinds) for k in ("random", "ghzqft", "bv")}
+    assert abs(frac["random"] - 0.4) < 0.05 and abs(frac["ghzqft"] - 0.3) < 0.05
+    for r in reqs[:200]:
+        assert len(set(r.zq)) == 4 and all(0 <= q < r.n for q in r.zq)
+        if r.kind == "random":
+            assert 8 <= r.depth <= 24
+    f64 = S.make_requests(500, single=False)
+    assert max(r.n for r in f64) == 32
+    # the stream is a pure function of its seed
+    again = S.make_requests(2000, rate=200.0, single=True)
+    assert [(r.n, r.kind, r.zq, r.arrival) for r in again] == [(r.n, r.kind, r.zq, r.arrival) for r in reqs]
+
+
+def test_admission_respects_budget_and_finishes_everything():
+    reqs = S.make_requests(60, rate=5000.0, single=False, n_range=(16, 20))
+    budget = 3 * (16 << 20)  # room for three 20-qubit states at most
+    lock = threading.Lock()
+    live = {"bytes": 0, "peak": 0}
+
+    def fake(r):
+        with lock:
+            live["bytes"] += S.state_bytes(r)
+            live["peak"] = max(live["peak"], live["bytes"])
+        time.sleep(0.002 * (1 + (r.n - 16)))
+        with lock:
+            live["bytes"] -= S.state_bytes(r)
+        return np.zeros(4, dtype=np.uint64), np.zeros(4)
+
+    srv = S.Server(env=None, hbm_budget=budget, workers=8, runner=fake)
+    out = srv.serve(reqs, realtime=True)
+    assert [r.rid for r in out] == list(range(60))
+    assert live["peak"] <= budget and srv.peak_in_use <= budget
+    assert srv.peak_in_flight > 1  # requests overlapped
+    st = S.summarize(out)
+    assert st["requests"] == 60 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_head_of_line_request_is_not_starved():
+    # one big request followed by a stream of small ones: the big one must run
+    big = S.Request(0, "bv", 20, 0, 1, 0.0, (0, 1, 2, 3), 1, False)
+    small = [S.Request(i, "bv", 16, 0, 1, 0.0001 * i, (0, 1, 2, 3), 1, False) for i in range(1, 40)]
+    budget = S.state_bytes(big) + S.state_bytes(small[0])
+
+    def fake(r):
+        time.sleep(0.003)
+        return np.zeros(1, dtype=np.uint64), np.zeros(1)
+
+    srv = S.Server(env=None, hbm_budget=budget, workers=4, max_bypass=3, runner=fake)
+    out = srv.serve([big] + small, realtime=False)
+    assert len(out) == 40
+    admitted_order = sorted(out, key=lambda r: r.admitted)
+    assert [r.rid for r in admitted_order].index(0) <= 3 + 1
