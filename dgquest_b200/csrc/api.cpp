@@ -246,6 +246,23 @@ int chooseTileBits(QuregState &s) {
 // microseconds and the generic tile kernel beats a compile.
 std::atomic<int> g_jitMinBits{-1};
 
+// The complex64 paired form (DGQ_F32_PAIRED=0 turns it off).
+bool pairedEnabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("DGQ_F32_PAIRED");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// Tile bits of the paired form, the in-slot bit included: 2^12 slots of two
+// amplitudes (64 KiB of shared memory, 256 threads), or a set width 10..13.
+int pairedTileBits(const QuregState &s) {
+    int W = (s.tileBitsSetting >= 10 && s.tileBitsSetting <= dgq::kMaxTileBits) ? s.tileBitsSetting : dgq::kMaxTileBits;
+    return std::min(W, s.numBits);
+}
+
 int jitMinBits() {
     int v = g_jitMinBits.load();
     if (v < 0) {
@@ -260,7 +277,8 @@ int jitMinBits() {
 
 namespace dgq {
 
-int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err) {
+int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err,
+                  bool paired) {
     out.clear();
     SweepHeader h;
     if (s.initPending) {
@@ -274,7 +292,7 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         h.restrictScale = s.rScale;
     }
     bool complete = true;
-    std::vector<BlockPlan> blocks = planBlocks(s.pending, s.numBits, W, &complete);
+    std::vector<BlockPlan> blocks = planBlocks(s.pending, s.numBits, W, &complete, paired ? kCoalescedBits + 1 : kCoalescedBits);
     if (!complete) {
         err = "a multi-qubit gate is wider than the register tile (max 4 targets)";
         return E_UNSUPPORTED;
@@ -282,12 +300,12 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
     bool first = true;
     for (const auto &b : blocks) {
         SweepHeader hb = first ? h : SweepHeader();
-        if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err)) return E_UNSUPPORTED;
+        if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err, paired)) return E_UNSUPPORTED;
         first = false;
     }
     if (blocks.empty()) {
         out.emplace_back();
-        encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back());
+        encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
         st.sweeps = 1;
     }
     return 0;
@@ -311,11 +329,23 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.planned.clear();
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
-    const int W = chooseTileBits(s);
+    // complex64 registers of >= 2^10 amplitudes run the paired form (two
+    // amplitudes per slot, packed FP32 arithmetic) unless a sweep cannot
+    // be encoded that way (a multi-qubit unitary on address bit 0)
+    bool paired = s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
+    int W = paired ? pairedTileBits(s) : chooseTileBits(s);
     dgq::PlanStats st;
     std::string err;
-    const int code = dgq::buildPrograms(s, W, s.planned, st, err);
+    int code = dgq::buildPrograms(s, W, s.planned, st, err, paired);
+    if (code && paired) {
+        paired = false;
+        W = chooseTileBits(s);
+        st = dgq::PlanStats();
+        err.clear();
+        code = dgq::buildPrograms(s, W, s.planned, st, err, false);
+    }
     if (code) return raise(code, func, err.c_str());
+    s.plannedPaired = paired;
     s.plannedTileBits = W;
     for (size_t i = 0; i < s.planned.size(); i++) {
         dgq::TileProgram &p = s.planned[i];
@@ -1479,7 +1509,8 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
     QuregState s;
     s.numQubits = numQubits;
     s.numBits = std::max(numQubits, dgq::kMinTileBits);
-    s.single = precision == 1;
+    s.single = precision == 1 || precision == 3;
+    s.allowPaired = precision == 1;
     resetMapping(s);
     s.tileBitsSetting = tileBits;
     for (int i = 0; i < count; i++) {

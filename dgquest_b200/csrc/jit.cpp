@@ -245,10 +245,233 @@ static std::string generatePersistent(const TileProgram &prog, int W) {
 // The persistent form has no renormalisation step, so complex64 programs
 // (which renormalise every sweep) always use the plain form.
 static bool usePersistent(const TileProgram &prog) {
-    return jitPersistent() && prog.numPhases > 0 && !prog.renormIn && !prog.renormOut;
+    return jitPersistent() && prog.numPhases > 0 && !prog.renormIn && !prog.renormOut && !prog.paired;
+}
+
+// ------------------------------------------------------------ paired form
+namespace {
+
+std::string cf(int off) { return "(float) prog.coef[" + std::to_string(off) + "]"; }
+
+// In-slot 2x2 (target address bit 0) as 8 float expressions (row-major re, im).
+bool inSlotMatrix(const KOp &op, std::string m[8]) {
+    const int off = op.coef;
+    const char *z = "0.0f", *one = "1.0f", *mone = "-1.0f";
+    auto set = [&](std::initializer_list<std::string> v) {
+        int i = 0;
+        for (const auto &x : v) m[i++] = x;
+    };
+    switch (op.kind) {
+        case KOP_M2R: set({cf(off), z, cf(off + 1), z, cf(off + 2), z, cf(off + 3), z}); return true;
+        case KOP_M2I: set({cf(off), z, z, cf(off + 1), z, cf(off + 2), cf(off + 3), z}); return true;
+        case KOP_M2C:
+            set({cf(off), cf(off + 1), cf(off + 2), cf(off + 3), cf(off + 4), cf(off + 5), cf(off + 6), cf(off + 7)});
+            return true;
+        case KOP_X: set({z, z, one, z, one, z, z, z}); return true;
+        case KOP_Y: set({z, z, z, mone, z, one, z, z}); return true;
+        case KOP_YC: set({z, z, z, one, z, mone, z, z}); return true;
+        case KOP_RY1: set({one, z, "-" + cf(off), z, cf(off), z, one, z}); return true;
+        case KOP_RY2: set({cf(off), z, mone, z, one, z, cf(off), z}); return true;
+        case KOP_RX1: set({one, z, z, "-" + cf(off), z, "-" + cf(off), one, z}); return true;
+        case KOP_RX2: set({cf(off), z, z, mone, z, mone, cf(off), z}); return true;
+        case KOP_H1: set({one, z, one, z, one, z, mone, z}); return true;
+        default: return false;
+    }
+}
+
+std::string selExpr(const KOp &op) {
+    std::ostringstream sel;
+    bool any = false;
+    const unsigned sl = op.selLoc & ~1u;
+    if (sl) {
+        sel << "((loc & " << sl << "u) != 0u)";
+        any = true;
+    }
+    if (op.selCta >= 0) {
+        sel << (any ? " || " : "") << "(((cta >> " << (int) op.selCta << ") & 1u) != 0u)";
+        any = true;
+    }
+    return any ? sel.str() : std::string("false");
+}
+
+void emitOpPaired(std::ostringstream &o, const KOp &op) {
+    const unsigned cr = op.ctrlReg;
+    const bool ctrl = cr != 0;
+    const bool hi = (op.ctrlLoc & 1u) != 0;  // controlled on address bit 0
+    const int off = op.coef;
+    const int k = op.k;
+    const std::string tpl3 = std::string(ctrl ? "true" : "false") + ", " + std::to_string(cr) + "u, " + (hi ? "true" : "false");
+    std::ostringstream body;
+    const bool pairKind = op.kind == KOP_M2R || op.kind == KOP_M2I || op.kind == KOP_M2C || op.kind == KOP_X ||
+                          op.kind == KOP_Y || op.kind == KOP_YC || op.kind == KOP_RY1 || op.kind == KOP_RY2 ||
+                          op.kind == KOP_RX1 || op.kind == KOP_RX2 || op.kind == KOP_H1;
+    if (pairKind && k == 4) {
+        std::string m[8];
+        inSlotMatrix(op, m);
+        body << "dgq::pInSlot<" << (ctrl ? "true" : "false") << ", " << cr << "u>(R, I";
+        for (int i = 0; i < 8; i++) body << ", " << m[i];
+        body << ");";
+    } else {
+        switch (op.kind) {
+            case KOP_M2R: body << "dgq::pM2R<" << k << ", " << tpl3 << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_M2I: body << "dgq::pM2I<" << k << ", " << tpl3 << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_M2C: body << "dgq::pM2C<" << k << ", " << tpl3 << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_X: body << "dgq::pX<" << k << ", " << tpl3 << ">(R, I);"; break;
+            case KOP_Y: body << "dgq::pY<" << k << ", " << tpl3 << ">(R, I);"; break;
+            case KOP_YC: body << "dgq::pYC<" << k << ", " << tpl3 << ">(R, I);"; break;
+            case KOP_RY1: body << "dgq::pRY1<" << k << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_RY2: body << "dgq::pRY2<" << k << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_RX1: body << "dgq::pRX1<" << k << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_RX2: body << "dgq::pRX2<" << k << ">(R, I, prog.coef + " << off << ");"; break;
+            case KOP_H1: body << "dgq::pH1<" << k << ">(R, I);"; break;
+            case KOP_NEG: body << "dgq::pNEG<" << tpl3 << ">(R, I);"; break;
+            case KOP_MULI: body << "dgq::pMULI<" << tpl3 << ">(R, I);"; break;
+            case KOP_MULNI: body << "dgq::pMULNI<" << tpl3 << ">(R, I);"; break;
+            case KOP_PH:
+                body << "dgq::pPH<" << tpl3 << ">(R, I, dgq::b2(" << cf(off) << "), dgq::b2(" << cf(off + 1) << "));";
+                break;
+            case KOP_Z2:
+                if (op.code < KC_Z2T) {
+                    body << "dgq::pZ2R<" << k << ", " << tpl3 << ">(R, I, prog.coef + " << off << ");";
+                } else if (op.selLoc == 1u) {
+                    body << "dgq::pPH<" << tpl3 << ">(R, I, dgq::b2(" << cf(off) << "), make_float2(-" << cf(off + 1)
+                         << ", " << cf(off + 1) << "));";
+                } else {
+                    body << "{ const bool b_ = " << selExpr(op) << "; dgq::pPH<" << tpl3 << ">(R, I, dgq::b2(" << cf(off)
+                         << "), dgq::b2(b_ ? " << cf(off + 1) << " : -" << cf(off + 1) << ")); }";
+                }
+                break;
+            case KOP_PH1:
+                if (op.code < KC_PH1T) {
+                    body << "dgq::pPH1R<" << k << ">(R, I, prog.coef + " << off << ");";
+                } else if (op.selLoc == 1u) {
+                    body << "dgq::pPH<false, 0u, false>(R, I, make_float2(1.0f, " << cf(off) << "), make_float2(0.0f, "
+                         << cf(off + 1) << "));";
+                } else {
+                    body << "if (" << selExpr(op) << ") dgq::pPH<false, 0u, false>(R, I, dgq::b2(" << cf(off)
+                         << "), dgq::b2(" << cf(off + 1) << "));";
+                }
+                break;
+            case KOP_DENSE: body << "dgq::pDense<" << k << ", " << cr << "u>(R, I, prog.coef + " << off << ");"; break;
+            default: break;
+        }
+    }
+    const unsigned cl = op.ctrlLoc & ~1u;
+    if (cl || op.ctrlCta) {
+        std::ostringstream cond;
+        bool any = false;
+        if (cl) {
+            cond << "((loc & " << cl << "u) == " << cl << "u)";
+            any = true;
+        }
+        if (op.ctrlCta) cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+        o << "    if (" << cond.str() << ") { " << body.str() << " }\n";
+    } else {
+        o << "    " << body.str() << "\n";
+    }
+}
+
+// Address bit of tile-local bit l of a paired tile (bits 0..5 are address bits 0..5).
+std::string pairedAddr(int l) {
+    if (l < kCoalescedBits) return std::to_string(l);
+    return "prog.highPos[" + std::to_string(l - kCoalescedBits) + "]";
+}
+
+// slot loop helpers: address of this thread's slot j in a layout (gt | rb bits)
+void emitPairedLayoutAddressing(std::ostringstream &o, const KPhase &ph, int W, const char *gt, const char *rb) {
+    o << "    const uint64_t " << gt << " = cb";
+    for (int i = 0; i < W - kRegBits - 1; i++)
+        o << " | ((uint64_t) ((tid >> " << i << ") & 1u) << " << pairedAddr(ph.thrPos[i]) << ")";
+    o << ";\n    const uint64_t " << rb << "[4] = {";
+    for (int b = 0; b < kRegBits; b++) o << (b ? ", " : "") << "1ULL << " << pairedAddr(ph.regPos[b]);
+    o << "};\n";
+}
+
+}  // namespace
+
+std::string generatePairedSource(const TileProgram &prog, int W) {
+    const int T = 1 << (W - kRegBits - 1);
+    const int minBlocks = ctasPerSm(T, false);
+    std::ostringstream o;
+    o << "#include \"jit_prelude.cuh\"\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << minBlocks
+      << ") dgq_sweep(float2 *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
+    o << "    constexpr int W = " << W << ";\n";
+    o << "    constexpr uint32_t T = " << T << "u;\n";
+    o << "    extern __shared__ float4 sm[];\n";
+    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x;\n";
+    o << "    (void) cta;\n    (void) T;\n";
+    o << "    float2 R[dgq::kRegs], I[dgq::kRegs];\n";
+    o << "    const uint64_t cb = dgq::jCtaBase(prog, cta, W);\n";
+    const int np = prog.numPhases;
+    const bool firstDirect = np > 0 && prog.phases[0].direct;
+    const bool lastDirect = np > 0 && prog.phases[np - 1].direct;
+    const std::string fix = "dgq::pFixSlot<" + std::to_string(prog.initKind) + ", " +
+                            (prog.hasRestrict ? "true" : "false") + ">(prog, g_, R[j], I[j]);";
+    const bool needFix = prog.initKind != INIT_NONE || prog.hasRestrict;
+    const std::string load = prog.initKind == INIT_NONE ? "dgq::pLoadSlot(st, g_, R[j], I[j]); " : "";
+    if (firstDirect) {
+        emitPairedLayoutAddressing(o, prog.phases[0], W, "gIn", "rbIn");
+        o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) { const uint64_t g_ = dgq::jIdx(gIn, rbIn, j); "
+          << load << (needFix ? fix : "") << " }\n";
+    } else {
+        // canonical layout: slot tid + T * j (lanes on address bits 1..5)
+        o << "    const uint64_t gC = cb | ((uint64_t) (tid & 31u) << 1)";
+        for (int i = 0; i < W - 10; i++) o << " | ((uint64_t) ((tid >> " << 5 + i << ") & 1u) << prog.highPos[" << 1 + i << "])";
+        o << ";\n    const uint64_t rbC[4] = {";
+        for (int b = 0; b < kRegBits; b++) o << (b ? ", " : "") << "1ULL << prog.highPos[" << W - 9 + b << "]";
+        o << "};\n";
+        o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) { const uint64_t g_ = dgq::jIdx(gC, rbC, j); "
+          << load << (needFix ? fix : "") << " }\n";
+        if (np > 0)
+            o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) sm[dgq::swz(tid + T * (uint32_t) j)] = "
+                 "make_float4(R[j].x, R[j].y, I[j].x, I[j].y);\n    __syncthreads();\n";
+    }
+    for (int p = 0; p < np; p++) {
+        const KPhase &ph = prog.phases[p];
+        const bool readSmem = !(p == 0 && firstDirect);
+        const bool writeSmem = !(p == np - 1 && lastDirect);
+        o << "  {\n    const uint32_t loc = 0u";
+        for (int i = 0; i < W - kRegBits - 1; i++) o << " | (((tid >> " << i << ") & 1u) << " << (int) ph.thrPos[i] << ")";
+        o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc >> 1);\n    (void) sb;\n";
+        if (readSmem)
+            for (int j = 0; j < kRegs; j++)
+                o << "    { const float4 q_ = sm[sb ^ " << ph.regOff[j] << "u]; R[" << j << "] = make_float2(q_.x, q_.y); I["
+                  << j << "] = make_float2(q_.z, q_.w); }\n";
+        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOpPaired(o, prog.ops[k]);
+        if (writeSmem) {
+            for (int j = 0; j < kRegs; j++)
+                o << "    sm[sb ^ " << ph.regOff[j] << "u] = make_float4(R[" << j << "].x, R[" << j << "].y, I[" << j
+                  << "].x, I[" << j << "].y);\n";
+            o << "    __syncthreads();\n";
+        }
+        o << "  }\n";
+    }
+    if (np > 0 && !lastDirect)
+        o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) { const float4 q_ = sm[dgq::swz(tid + T * "
+             "(uint32_t) j)]; R[j] = make_float2(q_.x, q_.y); I[j] = make_float2(q_.z, q_.w); }\n";
+    if (prog.renormIn) {
+        o << "    { const double sc_ = rsqrt(*prog.normIn); dgq::pGlobal(R, I, prog.globalRe * sc_, prog.globalIm * sc_); }\n";
+    } else if (prog.hasGlobal) {
+        o << "    dgq::pGlobal(R, I, prog.globalRe, prog.globalIm);\n";
+    }
+    if (prog.renormOut) o << "    dgq::pNormAccumulate(R, I, prog.normOut);\n";
+    if (lastDirect) {
+        emitPairedLayoutAddressing(o, prog.phases[np - 1], W, "gOut", "rbOut");
+        o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) dgq::pStoreSlot(st, dgq::jIdx(gOut, rbOut, j), R[j], I[j]);\n}\n";
+    } else {
+        o << "    const uint64_t gS = cb | ((uint64_t) (tid & 31u) << 1)";
+        for (int i = 0; i < W - 10; i++)
+            o << " | ((uint64_t) ((tid >> " << 5 + i << ") & 1u) << prog.highPos[" << 1 + i << "])";
+        o << ";\n    const uint64_t rbS[4] = {";
+        for (int b = 0; b < kRegBits; b++) o << (b ? ", " : "") << "1ULL << prog.highPos[" << W - 9 + b << "]";
+        o << "};\n#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) dgq::pStoreSlot(st, dgq::jIdx(gS, rbS, j), R[j], I[j]);\n}\n";
+    }
+    return o.str();
 }
 
 std::string generateSweepSource(const TileProgram &prog, int W) {
+    if (prog.paired) return generatePairedSource(prog, W);
     if (usePersistent(prog)) return generatePersistent(prog, W);
     const int T = 1 << (W - kRegBits);
     const int minBlocks = ctasPerSm(T, prog.isSingle != 0);
@@ -481,7 +704,8 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
 }
 
 cudaError_t launchJitSweep(CUfunction fn, void *st, int W, const TileProgram &prog, cudaStream_t s) {
-    const int T = 1 << (W - kRegBits);
+    // paired complex64 form: 16 slots of 2 amplitudes per thread
+    const int T = 1 << (W - kRegBits - (prog.paired ? 1 : 0));
     const bool persistent = usePersistent(prog);
     const unsigned smem = (unsigned) (((prog.isSingle ? sizeof(float2) : sizeof(double2)) << W) * (persistent ? 2 : 1));
     // one attribute call per function: cheap and idempotent

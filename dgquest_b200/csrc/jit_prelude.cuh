@@ -442,4 +442,323 @@ __device__ __forceinline__ void jFromSmem(const V *sm, uint32_t tid, V (&a)[kReg
     for (int j = 0; j < kRegs; j++) a[j] = sm[swz(tid + T * (uint32_t) j)];
 }
 
+// ============================================================ paired form
+// complex64 state, address bit 0 kept inside the thread: slot j of a thread
+// holds two amplitudes (address bit 0 = 0 "lo" and 1 "hi") as packed pairs
+// R[j] = (re_lo, re_hi), I[j] = (im_lo, im_hi). Every op below applies the
+// same arithmetic to both halves with one packed FP32 instruction
+// (__ffma2_rn / __fmul2_rn / __fadd2_rn), so a thread updates 32
+// amplitudes with the instruction count the complex128 kernel spends on 16.
+// HI: the op is controlled on address bit 0 (only the hi halves change).
+__device__ __forceinline__ float2 b2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
+template <bool HI>
+__device__ __forceinline__ float2 keepLo(float2 old, float2 nw) {
+    return HI ? make_float2(old.x, nw.y) : nw;
+}
+
+#define DGQP_PAIR_LOOP(K, CTRL, cr, ...)                                        \
+    _Pragma("unroll") for (int p_ = 0; p_ < kRegs / 2; p_++) {                  \
+        const int j0 = ((p_ >> (K)) << ((K) + 1)) | (p_ & ((1 << (K)) - 1));    \
+        const int j1 = j0 | (1 << (K));                                         \
+        if ((CTRL) && (j0 & (cr)) != (cr)) continue;                            \
+        const float2 rx = R[j0], ix = I[j0], ry = R[j1], iy = I[j1];            \
+        float2 nrx, nix, nry, niy;                                              \
+        __VA_ARGS__                                                             \
+        R[j0] = keepLo<HI>(rx, nrx);                                            \
+        I[j0] = keepLo<HI>(ix, nix);                                            \
+        R[j1] = keepLo<HI>(ry, nry);                                            \
+        I[j1] = keepLo<HI>(iy, niy);                                            \
+    }
+
+#define DGQP_SLOT_LOOP(CTRL, cr, ...)                                           \
+    _Pragma("unroll") for (int j = 0; j < kRegs; j++) {                         \
+        if ((CTRL) && (j & (cr)) != (cr)) continue;                             \
+        const float2 r = R[j], i = I[j];                                        \
+        float2 nr, ni;                                                          \
+        __VA_ARGS__                                                             \
+        R[j] = keepLo<HI>(r, nr);                                               \
+        I[j] = keepLo<HI>(i, ni);                                               \
+    }
+
+typedef float2 PRegs[kRegs];
+
+// [[m0, m1], [m2, m3]] real
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pM2R(PRegs &R, PRegs &I, const double *c) {
+    const float2 m0 = b2((float) c[0]), m1 = b2((float) c[1]), m2 = b2((float) c[2]), m3 = b2((float) c[3]);
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = fma2(m0, rx, mul2(m1, ry));
+        nix = fma2(m0, ix, mul2(m1, iy));
+        nry = fma2(m3, ry, mul2(m2, rx));
+        niy = fma2(m3, iy, mul2(m2, ix));
+    })
+}
+// [[m0, i m1], [i m2, m3]]
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pM2I(PRegs &R, PRegs &I, const double *c) {
+    const float2 m0 = b2((float) c[0]), m1 = b2((float) c[1]), m2 = b2((float) c[2]), m3 = b2((float) c[3]);
+    const float2 n1 = b2(-(float) c[1]), n2 = b2(-(float) c[2]);
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = fma2(m0, rx, mul2(n1, iy));
+        nix = fma2(m0, ix, mul2(m1, ry));
+        nry = fma2(m3, ry, mul2(n2, ix));
+        niy = fma2(m3, iy, mul2(m2, rx));
+    })
+}
+// general complex 2x2, row-major (re, im)
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pM2C(PRegs &R, PRegs &I, const double *c) {
+    const float2 u0 = b2((float) c[0]), u1 = b2((float) c[1]), u2 = b2((float) c[2]), u3 = b2((float) c[3]);
+    const float2 u4 = b2((float) c[4]), u5 = b2((float) c[5]), u6 = b2((float) c[6]), u7 = b2((float) c[7]);
+    const float2 v1 = b2(-(float) c[1]), v3 = b2(-(float) c[3]), v5 = b2(-(float) c[5]), v7 = b2(-(float) c[7]);
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = fma2(v3, iy, fma2(u2, ry, fma2(v1, ix, mul2(u0, rx))));
+        nix = fma2(u3, ry, fma2(u2, iy, fma2(u1, rx, mul2(u0, ix))));
+        nry = fma2(v7, iy, fma2(u6, ry, fma2(v5, ix, mul2(u4, rx))));
+        niy = fma2(u7, ry, fma2(u6, iy, fma2(u5, rx, mul2(u4, ix))));
+    })
+}
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pX(PRegs &R, PRegs &I) {
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = ry;
+        nix = iy;
+        nry = rx;
+        niy = ix;
+    })
+}
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pY(PRegs &R, PRegs &I) {
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = iy;
+        nix = neg2(ry);
+        nry = neg2(ix);
+        niy = rx;
+    })
+}
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pYC(PRegs &R, PRegs &I) {
+    DGQP_PAIR_LOOP(K, CTRL, CR, {
+        nrx = neg2(iy);
+        nix = ry;
+        nry = ix;
+        niy = neg2(rx);
+    })
+}
+// slot-wise phase (c + i s), c / s / -s given as packed pairs
+__device__ __forceinline__ void pMulPhase(float2 &r, float2 &i, float2 c, float2 s, float2 ns) {
+    const float2 r0 = r;
+    r = fma2(c, r0, mul2(ns, i));
+    i = fma2(c, i, mul2(s, r0));
+}
+// diag(c - i s, c + i s) selected by slot register bit K
+template <int K, bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pZ2R(PRegs &R, PRegs &I, const double *cf) {
+    const float2 c = b2((float) cf[0]), s = b2((float) cf[1]), ns = b2(-(float) cf[1]);
+    DGQP_SLOT_LOOP(CTRL, CR, {
+        nr = r;
+        ni = i;
+        if ((j >> K) & 1)
+            pMulPhase(nr, ni, c, s, ns);
+        else
+            pMulPhase(nr, ni, c, ns, s);
+    })
+}
+// phase (c + i s) on every (controlled) slot; c, s packed per half
+template <bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pPH(PRegs &R, PRegs &I, float2 c, float2 s) {
+    const float2 ns = mul2(s, make_float2(-1.0f, -1.0f));
+    DGQP_SLOT_LOOP(CTRL, CR, {
+        nr = r;
+        ni = i;
+        pMulPhase(nr, ni, c, s, ns);
+    })
+}
+template <bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pNEG(PRegs &R, PRegs &I) {
+    DGQP_SLOT_LOOP(CTRL, CR, {
+        nr = neg2(r);
+        ni = neg2(i);
+    })
+}
+template <bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pMULI(PRegs &R, PRegs &I) {
+    DGQP_SLOT_LOOP(CTRL, CR, {
+        nr = neg2(i);
+        ni = r;
+    })
+}
+template <bool CTRL, uint32_t CR, bool HI>
+__device__ __forceinline__ void pMULNI(PRegs &R, PRegs &I) {
+    DGQP_SLOT_LOOP(CTRL, CR, {
+        nr = i;
+        ni = neg2(r);
+    })
+}
+// factored uncontrolled rotations on a slot register bit
+template <int K>
+__device__ __forceinline__ void pRY1(PRegs &R, PRegs &I, const double *c) {
+    constexpr bool HI = false;
+    const float2 t = b2((float) c[0]), nt = b2(-(float) c[0]);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = fma2(nt, ry, rx);
+        nix = fma2(nt, iy, ix);
+        nry = fma2(t, rx, ry);
+        niy = fma2(t, ix, iy);
+    })
+}
+template <int K>
+__device__ __forceinline__ void pRY2(PRegs &R, PRegs &I, const double *c) {
+    constexpr bool HI = false;
+    const float2 u = b2((float) c[0]);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = fma2(u, rx, neg2(ry));
+        nix = fma2(u, ix, neg2(iy));
+        nry = fma2(u, ry, rx);
+        niy = fma2(u, iy, ix);
+    })
+}
+template <int K>
+__device__ __forceinline__ void pRX1(PRegs &R, PRegs &I, const double *c) {
+    constexpr bool HI = false;
+    const float2 t = b2((float) c[0]), nt = b2(-(float) c[0]);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = fma2(t, iy, rx);
+        nix = fma2(nt, ry, ix);
+        nry = fma2(t, ix, ry);
+        niy = fma2(nt, rx, iy);
+    })
+}
+template <int K>
+__device__ __forceinline__ void pRX2(PRegs &R, PRegs &I, const double *c) {
+    constexpr bool HI = false;
+    const float2 u = b2((float) c[0]);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = fma2(u, rx, iy);
+        nix = fma2(u, ix, neg2(ry));
+        nry = fma2(u, ry, ix);
+        niy = fma2(u, iy, neg2(rx));
+    })
+}
+template <int K>
+__device__ __forceinline__ void pH1(PRegs &R, PRegs &I) {
+    constexpr bool HI = false;
+    const float2 m1 = make_float2(-1.0f, -1.0f);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = add2(rx, ry);
+        nix = add2(ix, iy);
+        nry = fma2(m1, ry, rx);
+        niy = fma2(m1, iy, ix);
+    })
+}
+// phase (c + i s) on the slots whose register bit K is 1
+template <int K>
+__device__ __forceinline__ void pPH1R(PRegs &R, PRegs &I, const double *cf) {
+    const float2 c = b2((float) cf[0]), s = b2((float) cf[1]), ns = b2(-(float) cf[1]);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++)
+        if ((j >> K) & 1) pMulPhase(R[j], I[j], c, s, ns);
+}
+// general complex 2x2 acting inside each (controlled) slot: (lo, hi) -> M (lo, hi)
+template <bool CTRL, uint32_t CR>
+__device__ __forceinline__ void pInSlot(PRegs &R, PRegs &I, float m0r, float m0i, float m1r, float m1i, float m2r,
+                                        float m2i, float m3r, float m3i) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        if (CTRL && (j & CR) != CR) continue;
+        const float2 r = R[j], i = I[j];
+        R[j] = make_float2(m0r * r.x - m0i * i.x + m1r * r.y - m1i * i.y, m2r * r.x - m2i * i.x + m3r * r.y - m3i * i.y);
+        I[j] = make_float2(m0r * i.x + m0i * r.x + m1r * i.y + m1i * r.y, m2r * i.x + m2i * r.x + m3r * i.y + m3i * r.y);
+    }
+}
+template <int KK, uint32_t CR>
+__device__ __forceinline__ void pDense(PRegs &R, PRegs &I, const double *m) {
+    constexpr int D = 1 << KK;
+#pragma unroll
+    for (int g = 0; g < (kRegs >> KK); g++) {
+        const int base = g << KK;
+        if ((base & CR) != CR) continue;
+        float2 vr[D], vi[D];
+#pragma unroll
+        for (int c = 0; c < D; c++) {
+            vr[c] = R[base + c];
+            vi[c] = I[base + c];
+        }
+#pragma unroll
+        for (int r = 0; r < D; r++) {
+            float2 ar = b2(0.0f), ai = b2(0.0f);
+#pragma unroll
+            for (int c = 0; c < D; c++) {
+                const float mr = (float) m[2 * (r * D + c)], mi = (float) m[2 * (r * D + c) + 1];
+                ar = fma2(b2(mr), vr[c], ar);
+                ar = fma2(b2(-mi), vi[c], ar);
+                ai = fma2(b2(mr), vi[c], ai);
+                ai = fma2(b2(mi), vr[c], ai);
+            }
+            R[base + r] = ar;
+            I[base + r] = ai;
+        }
+    }
+}
+__device__ __forceinline__ void pGlobal(PRegs &R, PRegs &I, double grd, double gid) {
+    const float2 c = b2((float) grd), s = b2((float) gid), ns = b2(-(float) gid);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) pMulPhase(R[j], I[j], c, s, ns);
+}
+// Adds the CTA's sum of |a|^2 to *out (FP32 per thread, FP64 across threads).
+__device__ __forceinline__ void pNormAccumulate(const PRegs &R, const PRegs &I, double *out) {
+    __shared__ double red[32];
+    float2 acc = b2(0.0f);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        acc = fma2(R[j], R[j], acc);
+        acc = fma2(I[j], I[j], acc);
+    }
+    double t = (double) acc.x + (double) acc.y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double u = 0.0;
+        for (int w = 0; w < (int) (blockDim.x >> 5); w++) u += red[w];
+        atomicAdd(out, u);
+    }
+}
+// global I/O of one slot: amplitudes g (bit 0 clear) and g | 1 are adjacent
+__device__ __forceinline__ void pLoadSlot(const float2 *__restrict__ st, uint64_t g, float2 &r, float2 &i) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(st + g));
+    r = make_float2(v.x, v.z);
+    i = make_float2(v.y, v.w);
+}
+__device__ __forceinline__ void pStoreSlot(float2 *__restrict__ st, uint64_t g, float2 r, float2 i) {
+    *reinterpret_cast<float4 *>(st + g) = make_float4(r.x, i.x, r.y, i.y);
+}
+// initial state / lazy collapse of a slot at address g (bit 0 clear)
+template <int INIT, bool RESTRICT>
+__device__ __forceinline__ void pFixSlot(const TileProgram &prog, uint64_t g, float2 &r, float2 &i) {
+    if (INIT == INIT_CLASSICAL) {
+        r = make_float2(g == prog.initIndex ? 1.0f : 0.0f, (g | 1ULL) == prog.initIndex ? 1.0f : 0.0f);
+        i = b2(0.0f);
+    } else if (INIT == INIT_PLUS) {
+        const float a = (float) prog.initAmp;
+        r = make_float2((g >> prog.numReal) == 0ULL ? a : 0.0f, ((g | 1ULL) >> prog.numReal) == 0ULL ? a : 0.0f);
+        i = b2(0.0f);
+    } else if (INIT == INIT_BLANK) {
+        r = b2(0.0f);
+        i = b2(0.0f);
+    }
+    if (RESTRICT) {
+        const float sc = (float) prog.restrictScale;
+        const float2 k = make_float2((g & prog.restrictMask) == prog.restrictValue ? sc : 0.0f,
+                                     ((g | 1ULL) & prog.restrictMask) == prog.restrictValue ? sc : 0.0f);
+        r = mul2(r, k);
+        i = mul2(i, k);
+    }
+}
+
 }  // namespace dgq

@@ -49,19 +49,20 @@ static void growMask(const GateDag &dag, u64 &mask, int budget, bool preferHigh)
     }
 }
 
-std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete) {
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete,
+                                  int seedBits) {
     std::vector<BlockPlan> blocks;
     if (complete) *complete = true;
     GateDag dag(numBits, true);
     for (const Gate &g : gates) dag.add(g);
-    const u64 seed = (1ULL << kCoalescedBits) - 1;
+    const u64 seed = (1ULL << seedBits) - 1;
     const u64 all = numBits >= 64 ? ~0ULL : ((1ULL << numBits) - 1);
     while (!dag.empty()) {
         BlockPlan b;
         u64 mask = seed & all;
         growMask(dag, mask, tileBits, false);
-        // pad to tileBits with the lowest unused bits from bit 5 upward
-        for (int bit = kCoalescedBits; popcount64(mask) < tileBits && bit < numBits; bit++) mask |= 1ULL << bit;
+        // pad to tileBits with the lowest unused bits above the seed
+        for (int bit = seedBits; popcount64(mask) < tileBits && bit < numBits; bit++) mask |= 1ULL << bit;
         b.tileMask = mask & all;
         b.gates = dag.takeAllowed(b.tileMask);
         if (b.gates.empty()) {
@@ -129,10 +130,13 @@ struct PhaseLayout {
 // targets, then padding from the top tile bit down. Thread bits: three bits
 // of distinct (position mod 3) first, so that each quarter-warp touches 8
 // distinct swizzled bank groups, then the rest in increasing order.
-PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int tileBits) {
+PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int tileBits, bool paired = false) {
     PhaseLayout L;
     int nr = 0;
-    uint32_t used = 0;
+    // paired form: tile-local bit 0 is the pair inside a slot, never a
+    // register or thread bit
+    uint32_t used = paired ? 1u : 0u;
+    if (paired) targetsLocal &= ~1u;
     for (int p : front) {
         L.regPos[nr++] = p;
         used |= 1u << p;
@@ -149,11 +153,14 @@ PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int
             used |= 1u << p;
         }
     }
+    if (paired) used &= ~1u;
     L.regLocalMask = used;
     std::vector<int> thr;
-    for (int p = 0; p < tileBits; p++)
+    for (int p = paired ? 1 : 0; p < tileBits; p++)
         if (!((used >> p) & 1u)) thr.push_back(p);
-    L.direct = (used & ((1u << kCoalescedBits) - 1)) == 0;
+    // slots (16 B) are indexed by tile-local bits 1.. in the paired form
+    const int sh = paired ? 1 : 0;
+    L.direct = ((used >> sh) & ((1u << kCoalescedBits) - 1)) == 0;
     if (L.direct) {
         // lanes on tile bits 0..4 (address bits 0..4): the phase can read and
         // write HBM directly in 512-byte runs; bits 0..2 have distinct
@@ -165,9 +172,10 @@ PhaseLayout makeLayout(const std::vector<int> &front, uint32_t targetsLocal, int
     std::vector<int> lanes, rest;
     int classes = 0;
     for (int p : thr) {
-        if ((int) lanes.size() < 3 && !((classes >> (p % 3)) & 1)) {
+        const int q = p - sh;
+        if ((int) lanes.size() < 3 && !((classes >> (q % 3)) & 1)) {
             lanes.push_back(p);
-            classes |= 1 << (p % 3);
+            classes |= 1 << (q % 3);
         } else {
             rest.push_back(p);
         }
@@ -210,8 +218,10 @@ double opFlopsPerAmp(const KOp &op) {
     return f / (double) (1u << c);
 }
 
-void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out) {
+void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out,
+                      bool paired) {
     std::memset(&out, 0, sizeof(out));
+    out.paired = paired ? 1 : 0;
     out.globalRe = 1.0;
     out.numBits = numBits;
     out.numReal = numReal;
@@ -228,7 +238,8 @@ void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader 
 }
 
 bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits, const MatrixPool &pool,
-                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err) {
+                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err,
+                 bool paired) {
     const TileMap tm = makeTileMap(block.tileMask, numBits);
 
     // ---- phases: greedy DAG selection with the register budget
@@ -242,8 +253,9 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         GateDag dag(numBits, false);
         for (const Gate &g : block.gates) dag.add(g);
         while (!dag.empty()) {
-            u64 mask = 0;
-            growMask(dag, mask, kRegBits, true);
+            // paired form: address bit 0 is always inside the thread
+            u64 mask = paired ? 1ULL : 0ULL;
+            growMask(dag, mask, kRegBits + (paired ? 1 : 0), true);
             std::vector<Gate> gs = dag.takeAllowed(mask);
             if (gs.empty()) {
                 // a multi-target gate wider than the register bits
@@ -262,6 +274,10 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             };
             for (const Gate &g : gs) {
                 if (g.type == OP_MULTI_UNITARY) {
+                    if (paired && (g.targetMask & 1ULL)) {
+                        if (err) *err = "paired form: a multi-qubit unitary targets address bit 0";
+                        return false;
+                    }
                     flush();
                     Phase d;
                     d.gates.push_back(g);
@@ -287,6 +303,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         p.globalRe = 1.0;
         p.globalIm = 0.0;
         p.hasGlobal = 0;
+        p.paired = paired ? 1 : 0;
         if (isFirst) {
             p.initKind = first.initKind;
             p.initIndex = first.initIndex;
@@ -308,7 +325,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
     int numCoef = 0;
 
     for (const Phase &ph : phases) {
-        const PhaseLayout L = makeLayout(ph.front, ph.targetsLocal, tileBits);
+        const PhaseLayout L = makeLayout(ph.front, ph.targetsLocal, tileBits, paired);
         // encode the phase's ops into a scratch list first; uncontrolled
         // rotations leave their scalar factor in (phRe, phIm)
         std::vector<KOp> ops;
@@ -330,6 +347,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             op.coef = (uint16_t) coef.size();  // phase-relative, rebased when copied
             auto targetReg = [&](u64 tmask) -> int {
                 const Split t = splitMask(tmask, tm);
+                if (paired && t.tileLocal == 1u) return 4;  // the pair inside a slot
                 for (int b = 0; b < kRegBits; b++)
                     if (t.tileLocal == (1u << L.regPos[b])) return b;
                 return -1;
@@ -457,6 +475,8 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             }
             if (emit) {
                 const int rc = op.ctrlReg ? 1 : 0;
+                const uint8_t kSaved = op.k;
+                if (op.k == 4 && op.kind != KOP_DENSE) op.k = 0;  // codes index k < 4; paired ops keep k = 4
                 op.thrCtl = (op.ctrlLoc || op.ctrlCta) ? 1 : 0;
                 switch (op.kind) {
                     case KOP_M2R: op.code = (uint8_t) (KC_M2R + op.k + 4 * rc); break;
@@ -479,6 +499,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     case KOP_PH1: op.code = (uint8_t) (selIsReg ? KC_PH1R + op.k : KC_PH1T); break;
                     default: break;
                 }
+                op.k = kSaved;
                 ops.push_back(op);
             }
         }
@@ -500,7 +521,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         }
         KPhase &kp = prog->phases[prog->numPhases++];
         std::memset(&kp, 0, sizeof(kp));
-        for (int i = 0; i < tileBits - kRegBits; i++) kp.thrPos[i] = (uint8_t) L.thrPos[i];
+        for (int i = 0; i < tileBits - kRegBits - (paired ? 1 : 0); i++) kp.thrPos[i] = (uint8_t) L.thrPos[i];
         for (int b = 0; b < kRegBits; b++) kp.regPos[b] = (uint8_t) L.regPos[b];
         kp.direct = L.direct ? 1 : 0;
         kp.opBegin = (uint16_t) prog->numOps;
@@ -517,7 +538,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
             uint32_t loc = 0;
             for (int b = 0; b < kRegBits; b++)
                 if ((j >> b) & 1) loc |= 1u << L.regPos[b];
-            kp.regOff[j] = (uint16_t) tileSwizzle(loc);
+            kp.regOff[j] = (uint16_t) tileSwizzle(paired ? loc >> 1 : loc);
         }
         for (double c : coef) prog->coef[numCoef++] = c;
         prog->numCoef = (uint16_t) numCoef;

@@ -39,7 +39,11 @@ struct MatrixPool {
 
 // `complete` (if given) is set to false when gates are left that no tile
 // can hold (a gate with more non-diagonal targets than the tile width).
-std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete = nullptr);
+// seedBits: the lowest address bits every tile holds (5: the coalesced bits
+// of complex128 tiles; 6 for the complex64 paired form, whose tile-local
+// bit 0 is the pair inside a slot and bits 1..5 the coalesced slot bits).
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete = nullptr,
+                                  int seedBits = kCoalescedBits);
 
 // Encodes one block. The gate list may not fit one TileProgram; then the
 // block is emitted as several programs over the same tile (each one more
@@ -53,11 +57,15 @@ struct SweepHeader {
     double restrictScale = 1.0;
 };
 
+// paired: encode for the complex64 paired form (TileProgram::paired); fails
+// (with *err set) on a multi-qubit unitary that targets address bit 0.
 bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits, const MatrixPool &pool,
-                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err);
+                 const SweepHeader &first, std::vector<TileProgram> &out, PlanStats *stats, std::string *err,
+                 bool paired = false);
 
 // A program that only applies the header (init and/or lazy collapse).
-void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out);
+void encodeHeaderOnly(int numBits, int numReal, int tileBits, const SweepHeader &hdr, TileProgram &out,
+                      bool paired = false);
 
 // Algorithmic FP64 flops per amplitude of one kernel op (formulas of
 // QuEST_gpu_kernel.cu:17-170 counted as multiplies + adds per amplitude,

@@ -49,6 +49,8 @@ struct QuregState {
     double *dNorm = nullptr;  // complex64 renormalisation: two running sums of |a|^2
 
     int tileBitsSetting = 0;  // 0 = cost model
+    bool allowPaired = true;  // complex64: the paired form where it applies
+    bool plannedPaired = false;
     std::vector<dgq::TileProgram> planned;
     std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)
     int plannedTileBits = 0;
@@ -60,7 +62,10 @@ namespace dgq {
 // Plans the register's pending gates (and pending initialisation or
 // collapse) into sweep programs of tile width W. Returns 0, or the QuEST
 // error code with err set. The register is not changed.
-int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err);
+// paired: the complex64 paired form (TileProgram::paired; W counts the
+// in-slot bit, so W - 1 tile bits index 16-byte slots).
+int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err,
+                  bool paired = false);
 // Drops the pending work that buildPrograms planned (after it has been
 // launched or kept for launching).
 void consumePending(QuregState &s);

@@ -136,7 +136,13 @@ struct TileProgram {
     uint8_t highPos[kMaxTileBits - kCoalescedBits];  // address bit of tile-local bit 5 + i
     uint8_t ctaPos[kMaxStateBits];                   // address bit of blockIdx bit i
     uint16_t numCoef;  // coefficients used (coef[0 .. numCoef))
-    uint8_t pad0[2];
+    // 1: complex64 paired form. Address bit 0 stays inside each thread: a
+    // thread holds 16 slots of two amplitudes (address bit 0 = 0 and 1), as
+    // packed (re_lo, re_hi) and (im_lo, im_hi) pairs; phases place 4 slot
+    // bits in registers, the other W - 5 tile bits on threads, and ops with
+    // op.k == 4 act on the pair inside a slot (target address bit 0).
+    uint8_t paired;
+    uint8_t pad0[1];
     KPhase phases[kMaxPhases];
     KOp ops[kMaxOps];
     double coef[kMaxCoef];

@@ -125,7 +125,8 @@ int dgq_setSpecialisationMinBits(int minBits);
 
 /* Host-only view of the runtime specialisation: the CUDA source generated
  * for sweep `sweep` of the plan of the given gates (same encoding as
- * dgq_planGates; precision 1 = complex64, 2 = complex128; returns the number
+ * dgq_planGates; precision 1 = complex64 (the paired form where it applies),
+ * 2 = complex128, 3 = complex64 in the unpaired form; returns the number
  * of sweeps, -2 if buf is too small), and
  * an NVRTC compile of such a source for sm_100a (returns the cubin size, or
  * -1 with the compiler log in `log`). Neither needs a GPU. */

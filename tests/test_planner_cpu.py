@@ -51,7 +51,7 @@ def _sources(ops, n, w, precision=2):
     return out
 
 
-@pytest.mark.parametrize("w,precision", [(9, 2), (12, 2), (13, 1)])
+@pytest.mark.parametrize("w,precision", [(9, 2), (12, 2), (13, 1), (11, 1), (12, 3)])
 def test_generated_sweeps_compile(w, precision):
     ops = np.concatenate([C.mixed_ops(14, 150, 3, kinds=[k for k in range(26) if k != C.MEASURE]),
                           C.random_layers(14, 2, 5)])
@@ -61,3 +61,5 @@ def test_generated_sweeps_compile(w, precision):
     for s in srcs[:3]:
         size = Q.dgq_compileSweepSource(s, log, len(log))
         assert size > 0, log.value.decode()
+    # precision 1 selects the paired complex64 form (float4 slots)
+    assert all((b"float4 sm[]" in s) == (precision == 1) for s in srcs)
