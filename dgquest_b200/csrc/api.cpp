@@ -219,8 +219,8 @@ int chooseTileBits(QuregState &s) {
     // complex64 tiles could reach 2^13 amplitudes in 64 KiB, but at 16
     // amplitudes a thread that is one 512-thread CTA per SM, which hides no
     // latency; 2^12 keeps three CTAs per SM (override: dgq_setTileBits(13))
-    const int hi = std::min(s.single && s.tileBitsSetting == dgq::kMaxTileBits ? dgq::kMaxTileBits
-                                                                                 : dgq::kMaxTileBitsF64,
+    const int hi = std::min(s.single && s.tileBitsSetting >= dgq::kMaxTileBitsC64 ? dgq::kMaxTileBitsC64
+                                                                                    : dgq::kMaxTileBitsF64,
                             s.numBits);
     const int lo = dgq::kMinTileBits;
     if (s.tileBitsSetting > 0) return std::max(lo, std::min(hi, s.tileBitsSetting));
@@ -257,9 +257,9 @@ bool pairedEnabled() {
 }
 
 // Tile bits of the paired form, the in-slot bit included: 2^12 slots of two
-// amplitudes (64 KiB of shared memory, 256 threads), or a set width 10..13.
+// amplitudes (64 KiB of shared memory, 256 threads), or a set width 10..14.
 int pairedTileBits(const QuregState &s) {
-    int W = (s.tileBitsSetting >= 10 && s.tileBitsSetting <= dgq::kMaxTileBits) ? s.tileBitsSetting : dgq::kMaxTileBits;
+    int W = (s.tileBitsSetting >= 10 && s.tileBitsSetting <= dgq::kMaxTileBits) ? s.tileBitsSetting : 13;
     return std::min(W, s.numBits);
 }
 
@@ -347,15 +347,25 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     if (code) return raise(code, func, err.c_str());
     s.plannedPaired = paired;
     s.plannedTileBits = W;
-    for (size_t i = 0; i < s.planned.size(); i++) {
-        dgq::TileProgram &p = s.planned[i];
+    // complex64: every 4th sweep (counting back from the last) adds up the
+    // norm of its output and the next sweep divides by its square root, so
+    // FP32 rounding drift never accumulates over more than 4 sweeps and the
+    // final sweep starts from a renormalised state (the per-sweep global
+    // factor already restores the scale of the factored rotations exactly)
+    const int last = (int) s.planned.size() - 1;
+    int event = 0;
+    for (int i = 0; i <= last; i++) {
+        dgq::TileProgram &p = s.planned[(size_t) i];
         p.isSingle = s.single ? 1 : 0;
-        if (s.single && p.numPhases > 0) {
-            // renormalise every sweep: sweep i divides by the norm sweep i-1 measured
+        if (!s.single) continue;
+        const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
+        if (prev && prev->renormOut) {
+            p.renormIn = 1;
+            p.normIn = prev->normOut;
+        }
+        if (i < last && (last - 1 - i) % 4 == 0) {
             p.renormOut = 1;
-            p.normOut = s.dNorm + (i & 1);
-            p.renormIn = (i > 0 && s.planned[i - 1].renormOut) ? 1 : 0;
-            p.normIn = s.dNorm + ((i + 1) & 1);
+            p.normOut = s.dNorm + (event++ & 1);
         }
     }
     s.plannedFns.assign(s.planned.size(), nullptr);
@@ -1337,7 +1347,7 @@ int dgq_setTileBits(Qureg q, int tileBits) {
     QuregState &s = *stateOf(q);
     const int prev = s.tileBitsSetting;
     if (tileBits != 0 && (tileBits < dgq::kMinTileBits || tileBits > dgq::kMaxTileBits)) {
-        raise(E_INVALID_ARGUMENT, __func__, "tile bits must be 0 or in [9, 12]");
+        raise(E_INVALID_ARGUMENT, __func__, "tile bits must be 0 or in [9, 14] (14: paired complex64 only)");
         return prev;
     }
     s.tileBitsSetting = tileBits;

@@ -455,6 +455,12 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 neg2(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
+// sign flip on the integer pipe (standalone negations: CZ, S, Y), leaving
+// the FMA pipe to the arithmetic
+__device__ __forceinline__ float2 flip2(float2 a) {
+    return make_float2(__int_as_float(__float_as_int(a.x) ^ (int) 0x80000000),
+                       __int_as_float(__float_as_int(a.y) ^ (int) 0x80000000));
+}
 template <bool HI>
 __device__ __forceinline__ float2 keepLo(float2 old, float2 nw) {
     return HI ? make_float2(old.x, nw.y) : nw;
@@ -535,18 +541,18 @@ template <int K, bool CTRL, uint32_t CR, bool HI>
 __device__ __forceinline__ void pY(PRegs &R, PRegs &I) {
     DGQP_PAIR_LOOP(K, CTRL, CR, {
         nrx = iy;
-        nix = neg2(ry);
-        nry = neg2(ix);
+        nix = flip2(ry);
+        nry = flip2(ix);
         niy = rx;
     })
 }
 template <int K, bool CTRL, uint32_t CR, bool HI>
 __device__ __forceinline__ void pYC(PRegs &R, PRegs &I) {
     DGQP_PAIR_LOOP(K, CTRL, CR, {
-        nrx = neg2(iy);
+        nrx = flip2(iy);
         nix = ry;
         nry = ix;
-        niy = neg2(rx);
+        niy = flip2(rx);
     })
 }
 // slot-wise phase (c + i s), c / s / -s given as packed pairs
@@ -581,14 +587,14 @@ __device__ __forceinline__ void pPH(PRegs &R, PRegs &I, float2 c, float2 s) {
 template <bool CTRL, uint32_t CR, bool HI>
 __device__ __forceinline__ void pNEG(PRegs &R, PRegs &I) {
     DGQP_SLOT_LOOP(CTRL, CR, {
-        nr = neg2(r);
-        ni = neg2(i);
+        nr = flip2(r);
+        ni = flip2(i);
     })
 }
 template <bool CTRL, uint32_t CR, bool HI>
 __device__ __forceinline__ void pMULI(PRegs &R, PRegs &I) {
     DGQP_SLOT_LOOP(CTRL, CR, {
-        nr = neg2(i);
+        nr = flip2(i);
         ni = r;
     })
 }
@@ -596,7 +602,7 @@ template <bool CTRL, uint32_t CR, bool HI>
 __device__ __forceinline__ void pMULNI(PRegs &R, PRegs &I) {
     DGQP_SLOT_LOOP(CTRL, CR, {
         nr = i;
-        ni = neg2(r);
+        ni = flip2(r);
     })
 }
 // factored uncontrolled rotations on a slot register bit

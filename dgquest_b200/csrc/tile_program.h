@@ -24,9 +24,10 @@ constexpr int kRegBits = 4;
 constexpr int kRegs = 1 << kRegBits;
 constexpr int kCoalescedBits = 5;
 constexpr int kMinTileBits = 9;   // >= 32 threads (one full warp)
-constexpr int kMaxTileBits = 13;  // complex64: 2^13 x 8 B; complex128 tiles stop at 12 (64 KiB)
-constexpr int kMaxTileBitsF64 = 12;
-constexpr int kMaxThreadBits = kMaxTileBits - kRegBits;
+constexpr int kMaxTileBits = 14;      // paired complex64 form: 2^13 slots of 16 B (128 KiB)
+constexpr int kMaxTileBitsF64 = 12;   // complex128: 2^12 x 16 B (64 KiB)
+constexpr int kMaxTileBitsC64 = 13;   // unpaired complex64: 2^13 x 8 B (64 KiB)
+constexpr int kMaxThreadBits = kMaxTileBits - kRegBits - 1;  // 512 threads
 constexpr int kMaxStateBits = 40;
 constexpr int kMaxPhases = 56;
 constexpr int kMaxOps = 640;
