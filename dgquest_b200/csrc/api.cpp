@@ -325,67 +325,91 @@ void consumePending(QuregState &s) {
 
 namespace {
 
+// 0: compile specialised kernels when a plan needs them; 1: specialise only
+// plans whose kernels are compiled already, interpret the others while
+// their kernels compile on background host threads (serving: a one-off
+// circuit structure should not wait for NVRTC).
+std::atomic<int> g_specPolicy{0};
+
+// dgq_sweepSource (specialise = false) plans as for specialisation but
+// compiles nothing.
 bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.planned.clear();
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
-    // complex64 registers of >= 2^10 amplitudes run the paired form (two
-    // amplitudes per slot, packed FP32 arithmetic) unless a sweep cannot
-    // be encoded that way (a multi-qubit unitary on address bit 0)
-    bool paired = s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
-    int W = paired ? pairedTileBits(s) : chooseTileBits(s);
+    const bool jitOn = dgq::jitEnabled();
+    const bool wantJit = jitOn && (!specialise || s.numBits >= jitMinBits());
     dgq::PlanStats st;
     std::string err;
-    int code = dgq::buildPrograms(s, W, s.planned, st, err, paired);
-    if (code && paired) {
-        paired = false;
-        W = chooseTileBits(s);
+    int W = 0;
+    bool paired = false;
+    // interpret: the programs are for the interpreting kernel (W <= 12, unpaired)
+    auto build = [&](bool pairedForm, bool interpret) -> int {
+        paired = pairedForm;
+        W = paired ? pairedTileBits(s) : chooseTileBits(s);
+        if (interpret) W = std::min(W, dgq::kMaxTileBitsF64);
         st = dgq::PlanStats();
         err.clear();
-        code = dgq::buildPrograms(s, W, s.planned, st, err, false);
-    }
+        int code = dgq::buildPrograms(s, W, s.planned, st, err, paired);
+        if (code) return code;
+        // complex64: every 4th sweep (counting back from the last) adds up the
+        // norm of its output and the next sweep divides by its square root, so
+        // FP32 rounding drift never accumulates over more than 4 sweeps and the
+        // final sweep starts from a renormalised state (the per-sweep global
+        // factor already restores the scale of the factored rotations exactly)
+        const int last = (int) s.planned.size() - 1;
+        int event = 0;
+        for (int i = 0; i <= last; i++) {
+            dgq::TileProgram &p = s.planned[(size_t) i];
+            p.isSingle = s.single ? 1 : 0;
+            if (!s.single) continue;
+            const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
+            if (prev && prev->renormOut) {
+                p.renormIn = 1;
+                p.normIn = prev->normOut;
+            }
+            if (i < last && (last - 1 - i) % 4 == 0) {
+                p.renormOut = 1;
+                p.normOut = s.dNorm + (event++ & 1);
+            }
+        }
+        return 0;
+    };
+    // complex64 registers of >= 2^10 amplitudes run the paired form (two
+    // amplitudes per slot, packed FP32 arithmetic) when specialised, unless a
+    // sweep cannot be encoded that way (a multi-qubit unitary on address bit 0)
+    const bool pairedOk = wantJit && s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
+    int code = build(pairedOk, !wantJit);
+    if (code && pairedOk) code = build(false, !wantJit);
     if (code) return raise(code, func, err.c_str());
-    s.plannedPaired = paired;
-    s.plannedTileBits = W;
-    // complex64: every 4th sweep (counting back from the last) adds up the
-    // norm of its output and the next sweep divides by its square root, so
-    // FP32 rounding drift never accumulates over more than 4 sweeps and the
-    // final sweep starts from a renormalised state (the per-sweep global
-    // factor already restores the scale of the factored rotations exactly)
-    const int last = (int) s.planned.size() - 1;
-    int event = 0;
-    for (int i = 0; i <= last; i++) {
-        dgq::TileProgram &p = s.planned[(size_t) i];
-        p.isSingle = s.single ? 1 : 0;
-        if (!s.single) continue;
-        const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
-        if (prev && prev->renormOut) {
-            p.renormIn = 1;
-            p.normIn = prev->normOut;
-        }
-        if (i < last && (last - 1 - i) % 4 == 0) {
-            p.renormOut = 1;
-            p.normOut = s.dNorm + (event++ & 1);
-        }
-    }
     s.plannedFns.assign(s.planned.size(), nullptr);
-    if (s.single && specialise && !dgq::jitEnabled())
-        return raise(E_UNSUPPORTED, func, "complex64 registers need runtime-specialised kernels (DGQ_JIT=0 is set)");
     s.stats.jitCompiled = 0;
     s.stats.jitReused = 0;
     s.stats.jitMillis = 0.0;
-    if (specialise && dgq::jitEnabled() && (s.single || s.numBits >= jitMinBits())) {
+    if (specialise && wantJit) {
         std::vector<std::string> sources;
         sources.reserve(s.planned.size());
         for (const auto &p : s.planned) sources.push_back(dgq::generateSweepSource(p, W));
-        dgq::JitStats js;
-        std::string jerr;
-        if (!dgq::jitGetKernels(sources, s.plannedFns, &js, &jerr))
-            return raise(E_UNSUPPORTED, func, jerr.c_str());
-        s.stats.jitCompiled = js.compiled;
-        s.stats.jitReused = js.reused;
-        s.stats.jitMillis = js.compileMillis;
+        if (g_specPolicy.load() == 1 && !dgq::jitAllReady(sources)) {
+            dgq::jitCompileInBackground(sources);
+            if (paired || W > dgq::kMaxTileBitsF64) {
+                // the interpreting kernel runs unpaired programs of W <= 12
+                code = build(false, true);
+                if (code) return raise(code, func, err.c_str());
+                s.plannedFns.assign(s.planned.size(), nullptr);
+            }
+        } else {
+            dgq::JitStats js;
+            std::string jerr;
+            if (!dgq::jitGetKernels(sources, s.plannedFns, &js, &jerr))
+                return raise(E_UNSUPPORTED, func, jerr.c_str());
+            s.stats.jitCompiled = js.compiled;
+            s.stats.jitReused = js.reused;
+            s.stats.jitMillis = js.compileMillis;
+        }
     }
+    s.plannedPaired = paired;
+    s.plannedTileBits = W;
     s.stats.sweeps = st.sweeps;
     s.stats.phases = st.phases;
     s.stats.ops = st.ops;
@@ -406,7 +430,7 @@ bool launchPlanned(QuregState &s, const char *func) {
             !cudaOk(cudaMemsetAsync(s.planned[i].normOut, 0, sizeof(double), s.stream), func))
             return false;
         const cudaError_t e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, s.planned[i], s.stream)
-                                 : dgq::launchTile((double2 *) s.dState, s.plannedTileBits, s.planned[i], s.stream);
+                                 : dgq::launchTile(s.dState, s.single, s.plannedTileBits, s.planned[i], s.stream);
         if (!cudaOk(e, func)) return false;
         g_launches++;
     }
@@ -705,6 +729,14 @@ int dgq_sampleOutcomes(Qureg q, int numSamples, uint32_t seed, uint64_t *outcome
         outcomes[k] = logical;
     }
     return 0;
+}
+
+int dgq_setSpecialisationPolicy(int policy) {
+    if (policy != 0 && policy != 1) {
+        raise(E_INVALID_ARGUMENT, __func__, "policy must be 0 or 1");
+        return -1;
+    }
+    return g_specPolicy.exchange(policy);
 }
 
 int64_t dgq_getAvailableMemory(void) {

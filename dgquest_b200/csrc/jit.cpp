@@ -4,6 +4,7 @@
 #include <nvrtc.h>
 
 #include <atomic>
+#include <condition_variable>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -620,6 +621,105 @@ bool compileOne(const std::string &src, std::vector<char> &cubin, std::string &l
 
 }  // namespace
 
+namespace {
+
+// Compiled but not yet loaded kernels (from background compiles), and the
+// background compile queue. Heap-allocated and never destroyed, so a
+// compile still running at process exit touches no destroyed object.
+struct CubinCache {
+    std::mutex mu;
+    std::condition_variable idle;
+    std::unordered_map<size_t, std::vector<std::pair<std::string, std::vector<char>>>> cubins;
+    std::vector<std::string> queue;
+    std::unordered_map<size_t, int> queued;  // source hash -> pending count
+    int workers = 0;
+    bool stopping = false;
+};
+CubinCache &cubinCache() {
+    static CubinCache *c = new CubinCache();
+    return *c;
+}
+
+bool cubinFind(const std::string &src, std::vector<char> *out) {
+    CubinCache &c = cubinCache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    auto it = c.cubins.find(std::hash<std::string>()(src));
+    if (it == c.cubins.end()) return false;
+    for (const auto &e : it->second)
+        if (e.first == src) {
+            if (out) *out = e.second;
+            return true;
+        }
+    return false;
+}
+
+void backgroundWorker() {
+    CubinCache &c = cubinCache();
+    for (;;) {
+        std::string src;
+        {
+            std::lock_guard<std::mutex> lk(c.mu);
+            if (c.queue.empty() || c.stopping) {
+                c.workers--;
+                c.idle.notify_all();
+                return;
+            }
+            src = std::move(c.queue.back());
+            c.queue.pop_back();
+        }
+        std::vector<char> cubin;
+        std::string log;
+        const bool ok = compileOne(src, cubin, log);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t h = std::hash<std::string>()(src);
+        if (ok) c.cubins[h].emplace_back(src, std::move(cubin));
+        if (--c.queued[h] <= 0) c.queued.erase(h);
+    }
+}
+
+}  // namespace
+
+bool jitAllReady(const std::vector<std::string> &sources) {
+    for (const auto &src : sources)
+        if (!cacheFind(src) && !cubinFind(src, nullptr)) return false;
+    return true;
+}
+
+// At process exit: drop the queue and wait for compiles in progress, so no
+// background thread is inside NVRTC while the process tears down.
+static void stopBackgroundCompiles() {
+    CubinCache &c = cubinCache();
+    std::unique_lock<std::mutex> lk(c.mu);
+    c.stopping = true;
+    c.queue.clear();
+    c.idle.wait_for(lk, std::chrono::seconds(60), [&]() { return c.workers == 0; });
+}
+
+void jitCompileInBackground(const std::vector<std::string> &sources) {
+    static std::once_flag registered;
+    std::call_once(registered, []() { std::atexit(stopBackgroundCompiles); });
+    CubinCache &c = cubinCache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.stopping) return;
+    for (const auto &src : sources) {
+        if (cacheFind(src)) continue;
+        const size_t h = std::hash<std::string>()(src);
+        bool have = false;
+        auto it = c.cubins.find(h);
+        if (it != c.cubins.end())
+            for (const auto &e : it->second) have = have || e.first == src;
+        if (have || c.queued.count(h)) continue;
+        c.queued[h]++;
+        c.queue.push_back(src);
+    }
+    unsigned hw = std::thread::hardware_concurrency();
+    const int maxWorkers = (int) std::max(1u, std::min(8u, hw / 2));
+    while (c.workers < maxWorkers && (int) c.queue.size() > c.workers) {
+        c.workers++;
+        std::thread(backgroundWorker).detach();
+    }
+}
+
 bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log) {
     return compileOne(src, cubin, log);
 }
@@ -650,6 +750,7 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
     std::vector<std::vector<char>> cubins(sources.size());
     std::vector<std::string> logs(sources.size());
     std::vector<char> ok(sources.size(), 0);
+    std::atomic<int> fromBackground{0};
     if (!todo.empty()) {
         unsigned hw = std::thread::hardware_concurrency();
         if (hw == 0) hw = 4;
@@ -658,6 +759,11 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
         auto worker = [&]() {
             for (size_t t; (t = next.fetch_add(1)) < todo.size();) {
                 const size_t i = todo[t];
+                if (cubinFind(sources[i], &cubins[i])) {
+                    ok[i] = 1;
+                    fromBackground++;
+                    continue;
+                }
                 ok[i] = compileOne(sources[i], cubins[i], logs[i]) ? 1 : 0;
             }
         };
@@ -696,8 +802,9 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
     for (size_t i = 0; i < sources.size(); i++)
         if (dupOf[i] != (size_t) -1) out[i] = out[dupOf[i]];
     if (stats) {
-        stats->compiled = (int) todo.size();
-        stats->reused = reused;
+        // kernels compiled in the background and only loaded here count as reused
+        stats->compiled = (int) todo.size() - fromBackground.load();
+        stats->reused = reused + fromBackground.load();
         stats->compileMillis = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return allOk;

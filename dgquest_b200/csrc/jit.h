@@ -32,6 +32,14 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
 
 cudaError_t launchJitSweep(CUfunction fn, void *st, int tileBits, const TileProgram &prog, cudaStream_t s);
 
+// Whether every source is compiled already (loaded, or compiled in the
+// background and waiting to be loaded).
+bool jitAllReady(const std::vector<std::string> &sources);
+// Queues the sources that are neither loaded nor compiled for NVRTC
+// compilation on background host threads (no GPU work); later
+// jitGetKernels calls load the results instead of compiling.
+void jitCompileInBackground(const std::vector<std::string> &sources);
+
 // NVRTC compile only (no GPU needed).
 bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log);
 

@@ -1,6 +1,6 @@
 // kernels.cu -- the sm_100a kernels of the FP64 state-vector path.
 //
-//   tileKernel<W>    one sweep of the state applying a fused block
+//   tileKernel<W,V>  one sweep of the state applying a fused block
 //                    (dgQuEST statevec_fusedKernel, QuEST_gpu_kernel.cu:175-359)
 //   probKernel       P(bit = 0) for every address bit in one read pass
 //   probFinalize     (statevec_findProbabilityOfZeroKernel + reducePingpong,
@@ -24,12 +24,17 @@ namespace dgq {
 __device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u); }
 
 // ------------------------------------------------------------ tile kernel
-// 128 registers per thread: 16 warps per SM at every tile width.
-template <int W>
+// 128 registers per thread: 16 warps per SM at every tile width. V is
+// double2 (complex128) or float2 (complex64, with the per-sweep
+// renormalisation of the complex64 form: scale by 1/sqrt(*normIn) with the
+// global factor, add the output's sum of |a|^2 to *normOut).
+template <int W, class V>
 __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kRegBits)))
-    tileKernel(double2 *__restrict__ st, const __grid_constant__ TileProgram prog) {
+    tileKernel(V *__restrict__ st, const __grid_constant__ TileProgram prog) {
+    typedef typename Real<V>::T R;
     constexpr int T = 1 << (W - kRegBits);
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char smRaw[];
+    V *sm = reinterpret_cast<V *>(smRaw);
     const uint32_t tid = threadIdx.x;
     const uint32_t cta = blockIdx.x;
 
@@ -47,7 +52,7 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
         return tpart | ((j & 1) ? jb0 : 0ULL) | ((j & 2) ? jb1 : 0ULL) | ((j & 4) ? jb2 : 0ULL) | ((j & 8) ? jb3 : 0ULL);
     };
 
-    double2 a[kRegs];
+    V a[kRegs];
     if (prog.initKind == INIT_NONE) {
 #pragma unroll
         for (int j = 0; j < kRegs; j++) a[j] = st[gidx(j)];
@@ -64,16 +69,16 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
                 re = (g == ci) ? 1.0 : 0.0;
             else if (kind == INIT_PLUS)
                 re = ((g >> nr) == 0ULL) ? pa : 0.0;
-            a[j] = make_double2(re, 0.0);
+            a[j] = mk<V>((R) re, (R) 0);
         }
     }
     if (prog.hasRestrict) {
         const uint64_t rm = prog.restrictMask, rv = prog.restrictValue;
-        const double sc = prog.restrictScale;
+        const R sc = (R) prog.restrictScale;
 #pragma unroll
         for (int j = 0; j < kRegs; j++) {
             const bool keep = (gidx(j) & rm) == rv;
-            a[j] = keep ? make_double2(a[j].x * sc, a[j].y * sc) : make_double2(0.0, 0.0);
+            a[j] = keep ? mk<V>(a[j].x * sc, a[j].y * sc) : mk<V>((R) 0, (R) 0);
         }
     }
 
@@ -99,30 +104,52 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
 #pragma unroll
         for (int j = 0; j < kRegs; j++) a[j] = sm[swz(tid + (uint32_t) (T * j))];
     }
-    if (prog.hasGlobal) {
-        const double gr = prog.globalRe, gi = prog.globalIm;
+    if (prog.hasGlobal || prog.renormIn) {
+        double grd = prog.globalRe, gid = prog.globalIm;
+        if (prog.renormIn) {
+            const double sc = rsqrt(*prog.normIn);
+            grd *= sc;
+            gid *= sc;
+        }
+        const R gr = (R) grd, gi = (R) gid;
 #pragma unroll
-        for (int j = 0; j < kRegs; j++) a[j] = make_double2(gr * a[j].x - gi * a[j].y, gr * a[j].y + gi * a[j].x);
+        for (int j = 0; j < kRegs; j++) a[j] = mk<V>(gr * a[j].x - gi * a[j].y, gr * a[j].y + gi * a[j].x);
+    }
+    if (prog.renormOut) {
+        __shared__ double red[32];
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < kRegs; j++) acc += (double) a[j].x * (double) a[j].x + (double) a[j].y * (double) a[j].y;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((tid & 31u) == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < T / 32; w++) t += red[w];
+            atomicAdd(prog.normOut, t);
+        }
     }
 #pragma unroll
     for (int j = 0; j < kRegs; j++) st[gidx(j)] = a[j];
 }
 
-template <int W>
-static cudaError_t launchTileW(double2 *st, const TileProgram &prog, cudaStream_t s) {
+template <int W, class V>
+static cudaError_t launchTileW(V *st, const TileProgram &prog, cudaStream_t s) {
     static bool attrSet = false;
-    const size_t smem = sizeof(double2) << W;
+    const size_t smem = sizeof(V) << W;
     if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(tileKernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaError_t e = cudaFuncSetAttribute(tileKernel<W, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
         if (e != cudaSuccess) return e;
         attrSet = true;
     }
     const unsigned grid = 1u << (prog.numBits - W);
-    tileKernel<W><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
+    tileKernel<W, V><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
     return cudaGetLastError();
 }
 
-cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s) {
+template <class V>
+static cudaError_t launchTileV(V *st, int tileBits, const TileProgram &prog, cudaStream_t s) {
     switch (tileBits) {
         case 9: return launchTileW<9>(st, prog, s);
         case 10: return launchTileW<10>(st, prog, s);
@@ -130,6 +157,11 @@ cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaS
         case 12: return launchTileW<12>(st, prog, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launchTile(void *st, bool single, int tileBits, const TileProgram &prog, cudaStream_t s) {
+    if (prog.paired) return cudaErrorInvalidValue;  // the paired form is runtime-specialised only
+    return single ? launchTileV((float2 *) st, tileBits, prog, s) : launchTileV((double2 *) st, tileBits, prog, s);
 }
 
 // ------------------------------------------------------- probabilities

@@ -58,7 +58,8 @@ cudaError_t launchInner(const void *bra, bool braSingle, const void *ket, bool k
                         double2 *partial, double2 *out, cudaStream_t s);
 int innerNumCtas();
 
-cudaError_t launchTile(double2 *st, int tileBits, const TileProgram &prog, cudaStream_t s);
+// The interpreting sweep kernel (complex128 or unpaired complex64 programs, W 9..12).
+cudaError_t launchTile(void *st, bool single, int tileBits, const TileProgram &prog, cudaStream_t s);
 cudaError_t launchProb(const void *st, bool single, const ProbArgs &args, double *partial, double *out,
                        cudaStream_t s);
 int probNumCtas(const ProbArgs &args);

@@ -109,8 +109,11 @@ class Server:
     (first fit in arrival order) until it has been passed over `max_bypass`
     times, after which nothing else is admitted before it."""
 
-    def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None):
+    def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None, cached_kernels_only=True):
         self.env = env
+        # one-off circuit structures run the interpreting kernel instead of
+        # waiting for a kernel compile; their kernels compile in the background
+        self.cached_kernels_only = cached_kernels_only and runner is None
         self.runner = runner or (lambda r: run_request(r, env))
         self.peak_in_use = 0
         self.peak_in_flight = 0
@@ -191,6 +194,7 @@ class Server:
                     results[r.rid] = Result(r.rid, samples, expz, r.arrival, admitted, now())
                     cond.notify_all()
 
+        prev_policy = Q.dgq_setSpecialisationPolicy(1) if self.cached_kernels_only else None
         feeder = threading.Thread(target=arrivals, daemon=True)
         pool = [threading.Thread(target=worker, daemon=True) for _ in range(self.workers)]
         feeder.start()
@@ -199,6 +203,8 @@ class Server:
         feeder.join()
         for t in pool:
             t.join()
+        if prev_policy is not None:
+            Q.dgq_setSpecialisationPolicy(prev_policy)
         if state["error"] is not None:
             raise state["error"]
         return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]

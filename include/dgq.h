@@ -122,6 +122,12 @@ int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, 
  * sweep kernels (default 22, or DGQ_JIT_MIN_BITS; DGQ_JIT=0 disables
  * specialisation). Negative restores the default. Returns the previous value. */
 int dgq_setSpecialisationMinBits(int minBits);
+/* 0 (default): plans that need specialised kernels compile them before
+ * running. 1: a plan runs specialised only if its kernels are compiled
+ * already; otherwise it runs the interpreting kernel while its kernels
+ * compile on background host threads for later plans of the same structure
+ * (for serving one-off circuits). Returns the previous policy. */
+int dgq_setSpecialisationPolicy(int policy);
 
 /* Host-only view of the runtime specialisation: the CUDA source generated
  * for sweep `sweep` of the plan of the given gates (same encoding as

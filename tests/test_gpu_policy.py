@@ -1,0 +1,54 @@
+"""Specialisation policy 1 (serving): a plan whose kernels are not compiled
+runs the interpreting kernel at once and compiles in the background; a later
+plan of the same structure runs specialised. Both give the oracle's result
+(1e-12 complex128; complex64 fidelity >= 1 - 1e-6)."""
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from dgquest_b200 import circuits as C
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_cached_only_policy(quest, env, single):
+    Q = quest
+    prev_bits = Q.dgq_setSpecialisationMinBits(1)
+    prev = Q.dgq_setSpecialisationPolicy(1)
+    try:
+        n = 15
+        # a circuit structure no other test plans
+        ops = C.random_layers(n, 5, C.config_seed(2, 4242 + int(single)))
+        ref, _, _ = oracle.run(n, ops)
+
+        def run():
+            q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+            C.replay(q, ops)
+            Q.dgq_planPending(q)
+            st = Q.plan_stats(q)
+            Q.dgq_launchPlanned(q)
+            amps = Q.state_vector(q)
+            Q.destroyQureg(q, env)
+            return st, amps
+
+        st1, a1 = run()
+        assert st1.jitCompiled == 0 and st1.jitReused == 0  # interpreted, nothing compiled in the call
+        deadline = time.time() + 120
+        while True:
+            st2, a2 = run()
+            if st2.jitReused + st2.jitCompiled == st2.sweeps or time.time() > deadline:
+                break
+            time.sleep(0.5)
+        assert st2.jitReused + st2.jitCompiled == st2.sweeps
+        assert st2.jitCompiled == 0  # loaded from the background compiles
+        for a in (a1, a2):
+            if single:
+                assert abs(np.vdot(ref, a)) ** 2 >= 1 - 1e-6
+            else:
+                assert np.abs(a - ref).max() <= 1e-12
+    finally:
+        Q.dgq_setSpecialisationPolicy(prev)
+        Q.dgq_setSpecialisationMinBits(-1 if prev_bits == 22 else prev_bits)

@@ -76,3 +76,39 @@ def test_inner_product_and_fidelity_across_precisions(quest, env):
     assert quest.calcFidelity(q64, q64) == pytest.approx(1.0, abs=1e-12)
     quest.destroyQureg(q64, env)
     quest.destroyQureg(q32, env)
+
+
+@pytest.fixture
+def specialise_all(quest):
+    """Runtime-specialised kernels for every register size (the complex64
+    paired form needs them); restores the default afterwards."""
+    prev = quest.dgq_setSpecialisationMinBits(1)
+    yield
+    quest.dgq_setSpecialisationMinBits(-1 if prev == 22 else prev)
+
+
+@pytest.mark.parametrize("n,tile_bits", [(16, 13), (14, 10), (15, 12), (13, 13), (12, 0)])
+def test_f32_paired_form(quest, env, specialise_all, n, tile_bits):
+    """The paired form (two amplitudes per slot, packed FP32) on every kind of
+    call: random layers, the API call mix (multi-qubit unitaries on address
+    bit 0 fall back to the unpaired form), BV measurement."""
+    Q = quest
+    ops = np.concatenate([C.random_layers(n, 6, C.config_seed(2, 900 + n)), C.mixed_ops(n, 250, 60 + n)])
+    amps, p0, norm, _ = run_f32(Q, env, n, ops, tile_bits)
+    ref, ref_p0, _ = oracle.run(n, ops)
+    assert fidelity(ref, amps) >= 1 - 1e-6
+    assert np.abs(amps - ref).max() <= 2e-6
+    assert abs(norm - 1) <= 1e-5
+    assert np.abs(p0 - ref_p0).max() <= 1e-5
+
+
+def test_f32_paired_is_selected(quest, env, specialise_all):
+    Q = quest
+    n = 16
+    q = Q.dgq_createQuregF32(n, env)
+    C.replay(q, C.random_layers(n, 4, 3))
+    Q.dgq_planPending(q)
+    st = Q.plan_stats(q)
+    # the paired form uses 2^13-amplitude tiles by default and is specialised
+    assert st.tileBits == 13 and st.jitCompiled + st.jitReused == st.sweeps
+    Q.destroyQureg(q, env)
