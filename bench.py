@@ -357,6 +357,62 @@ def run_ncu_case(args):
     Q.destroyQuESTEnv(env)
 
 
+def run_precision_form(args, world):
+    """Precision form on its own workload: the 4x8 grid circuit of depth 16
+    (sqrt X / sqrt Y / sqrt W, never the same gate twice in a row on a qubit,
+    CZ on the 4 alternating edge patterns) on 32 qubits, complex64 (32 GiB)
+    against complex128 (64 GiB) of the same seed."""
+    import torch
+
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    n, depth = 32, 16
+    ops = C.grid_sqrt(4, 8, depth, C.config_seed(3))
+    env = Q.createQuESTEnv()
+    out = {"workload": "4x8 grid, depth 16, sqrt-X/Y/W + CZ patterns, 32 qubits", "qubits": n, "depth": depth}
+    regs = {}
+    for name, single in (("complex128", False), ("complex64", True)):
+        q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+        Q.initZeroState(q)
+        Q.apply_circuit(q, ops)
+        Q.dgq_planPending(q)
+        st = Q.plan_stats(q)
+        stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+        for _ in range(args.warmup):
+            Q.dgq_launchPlanned(q)
+        torch.cuda.synchronize()
+        steps = max(1, min(args.steps, 3))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            Q.dgq_launchPlanned(q)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
+        amp = 8 if single else 16
+        out[name] = {"ms_per_circuit": ms, "sweeps": st.sweeps, "tile_bits": st.tileBits,
+                     "hbm_gbs": 2.0 * (1 << n) * amp * st.sweeps / (ms / 1e3) / 1e9,
+                     "gate_layers_per_s": depth / (ms / 1e3)}
+        regs[name] = q
+    q64, q32 = regs["complex128"], regs["complex64"]
+    out["fidelity"] = Q.calcFidelity(q64, q32)
+    idx = np.random.RandomState(3).randint(0, 1 << n, size=2048)
+    err = 0.0
+    for i in idx:
+        a = Q.getAmp(q64, int(i))
+        b = Q.getAmp(q32, int(i))
+        err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
+    out["max_abs_err_sampled"] = err
+    out["amplitudes_sampled"] = len(idx)
+    out["speedup_complex64"] = out["complex128"]["ms_per_circuit"] / out["complex64"]["ms_per_circuit"]
+    out["arithmetic"] = "complex64 paired form (packed FP32 SIMT); the tensor-core dense-block GEMM is not built"
+    for q in (q64, q32):
+        Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+    return out
+
+
 def run_batch_form(args, world):
     """Batched form: 4096 ansatz circuits (n in [10, 22], depth in [4, 32]) in
     one persistent launch per step, complex128 and complex64; tile width and
@@ -465,6 +521,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-grid32", action="store_true")
     ap.add_argument("--batch-circuits", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--batch-case", type=int, default=0, help="--ncu-case: a batch of this many workload circuits")
@@ -487,6 +544,10 @@ def main():
             dist.destroy_process_group()
         return
     line = run_gpu(args, world, rank, local)
+    if not args.no_grid32:
+        grid = run_precision_form(args, world)
+        if rank == 0:
+            line["precision_form_grid32"] = grid
     if not args.no_batch:
         batch = run_batch_form(args, world)
         if rank == 0:

@@ -241,6 +241,15 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }
             break;
         }
+        case KOP_RN1: {
+            const R pr = (R) c[0], pi = (R) c[1];
+            DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](V &x, V &y) {
+                const V x0 = x;
+                x = mk<V>(fma(pr, y.x, fma(-pi, y.y, x0.x)), fma(pr, y.y, fma(pi, y.x, x0.y)));
+                y = mk<V>(fma(-pr, x0.x, fma(-pi, x0.y, y.x)), fma(-pr, x0.y, fma(pi, x0.x, y.y)));
+            }));
+            break;
+        }
         case KOP_DENSE:
             switch (op.k) {
                 case 1: denseApply<1>(a, cr, c); break;

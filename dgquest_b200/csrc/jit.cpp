@@ -76,6 +76,8 @@ void emitOp(std::ostringstream &o, const KOp &op) {
         static const char *names[4] = {"jRY1", "jRY2", "jRX1", "jRX2"};
         body << "dgq::" << names[(op.code - KC_RY1) / 4] << "<" << (op.code - KC_RY1) % 4 << ">(a, prog.coef + " << off
              << ");";
+    } else if (op.code >= KC_RN1 && op.code < KC_RN1 + 4) {
+        body << "dgq::jRN1<" << op.code - KC_RN1 << ">(a, prog.coef + " << off << ");";
     } else if (op.code >= KC_H1 && op.code < KC_H1 + 4) {
         body << "dgq::jH1<" << op.code - KC_H1 << ">(a);";
     } else if (op.code >= KC_PH1R && op.code < KC_PH1R + 4) {
@@ -276,6 +278,7 @@ bool inSlotMatrix(const KOp &op, std::string m[8]) {
         case KOP_RX1: set({one, z, z, "-" + cf(off), z, "-" + cf(off), one, z}); return true;
         case KOP_RX2: set({cf(off), z, z, mone, z, mone, cf(off), z}); return true;
         case KOP_H1: set({one, z, one, z, one, z, mone, z}); return true;
+        case KOP_RN1: set({one, z, cf(off), cf(off + 1), "-" + cf(off), cf(off + 1), one, z}); return true;
         default: return false;
     }
 }
@@ -305,7 +308,7 @@ void emitOpPaired(std::ostringstream &o, const KOp &op) {
     std::ostringstream body;
     const bool pairKind = op.kind == KOP_M2R || op.kind == KOP_M2I || op.kind == KOP_M2C || op.kind == KOP_X ||
                           op.kind == KOP_Y || op.kind == KOP_YC || op.kind == KOP_RY1 || op.kind == KOP_RY2 ||
-                          op.kind == KOP_RX1 || op.kind == KOP_RX2 || op.kind == KOP_H1;
+                          op.kind == KOP_RX1 || op.kind == KOP_RX2 || op.kind == KOP_H1 || op.kind == KOP_RN1;
     if (pairKind && k == 4) {
         std::string m[8];
         inSlotMatrix(op, m);
@@ -325,6 +328,7 @@ void emitOpPaired(std::ostringstream &o, const KOp &op) {
             case KOP_RX1: body << "dgq::pRX1<" << k << ">(R, I, prog.coef + " << off << ");"; break;
             case KOP_RX2: body << "dgq::pRX2<" << k << ">(R, I, prog.coef + " << off << ");"; break;
             case KOP_H1: body << "dgq::pH1<" << k << ">(R, I);"; break;
+            case KOP_RN1: body << "dgq::pRN1<" << k << ">(R, I, prog.coef + " << off << ");"; break;
             case KOP_NEG: body << "dgq::pNEG<" << tpl3 << ">(R, I);"; break;
             case KOP_MULI: body << "dgq::pMULI<" << tpl3 << ">(R, I);"; break;
             case KOP_MULNI: body << "dgq::pMULNI<" << tpl3 << ">(R, I);"; break;

@@ -34,6 +34,13 @@ struct VecOf<float2> {
 #define DGQJ_R typename VecOf<V>::R
 #define DGQJ_MK(x, y) VecOf<V>::make((x), (y))
 
+// Sign flips on the integer pipe (standalone negations of CZ, S, Y and
+// their conjugates), keeping the FP pipes for the gate arithmetic.
+__device__ __forceinline__ double jFlip(double x) {
+    return __longlong_as_double(__double_as_longlong(x) ^ (long long) 0x8000000000000000ULL);
+}
+__device__ __forceinline__ float jFlip(float x) { return __int_as_float(__float_as_int(x) ^ (int) 0x80000000); }
+
 __device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x >> 6) ^ (x >> 9) ^ (x >> 12)) & 7u); }
 
 // ---------------------------------------------------------------- operations
@@ -120,8 +127,8 @@ template <int K, bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jY(V (&a)[kRegs]) {
     DGQJ_PAIR_LOOP(K, CTRL, CR, {
         const V t = x;
-        x = DGQJ_MK(y.y, -y.x);
-        y = DGQJ_MK(-t.y, t.x);
+        x = DGQJ_MK(y.y, jFlip(y.x));
+        y = DGQJ_MK(jFlip(t.y), t.x);
     })
 }
 
@@ -129,8 +136,8 @@ template <int K, bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jYC(V (&a)[kRegs]) {
     DGQJ_PAIR_LOOP(K, CTRL, CR, {
         const V t = x;
-        x = DGQJ_MK(-y.y, y.x);
-        y = DGQJ_MK(t.y, -t.x);
+        x = DGQJ_MK(jFlip(y.y), y.x);
+        y = DGQJ_MK(t.y, jFlip(t.x));
     })
 }
 
@@ -156,17 +163,17 @@ __device__ __forceinline__ void jPH(V (&a)[kRegs], double cs, double sn) {
 
 template <bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jNEG(V (&a)[kRegs]) {
-    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(-x.x, -x.y); })
+    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(jFlip(x.x), jFlip(x.y)); })
 }
 
 template <bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jMULI(V (&a)[kRegs]) {
-    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(-x.y, x.x); })
+    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(jFlip(x.y), x.x); })
 }
 
 template <bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jMULNI(V (&a)[kRegs]) {
-    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(x.y, -x.x); })
+    DGQJ_AMP_LOOP(CTRL, CR, { x = DGQJ_MK(x.y, jFlip(x.x)); })
 }
 
 // Factored uncontrolled gates (the scalar factor is applied once per sweep)
@@ -204,6 +211,16 @@ __device__ __forceinline__ void jRX2(V (&a)[kRegs], const double *c) {
         const V x0 = x;
         x = DGQJ_MK(fma(u, x0.x, y.y), fma(u, x0.y, -y.x));
         y = DGQJ_MK(fma(u, y.x, x0.y), fma(u, y.y, -x0.x));
+    })
+}
+// [[1, p], [-conj(p), 1]]
+template <int K, class V>
+__device__ __forceinline__ void jRN1(V (&a)[kRegs], const double *c) {
+    const DGQJ_R pr = (DGQJ_R) c[0], pi = (DGQJ_R) c[1];
+    DGQJ_PAIR_LOOP(K, false, 0u, {
+        const V x0 = x;
+        x = DGQJ_MK(fma(pr, y.x, fma(-pi, y.y, x0.x)), fma(pr, y.y, fma(pi, y.x, x0.y)));
+        y = DGQJ_MK(fma(-pr, x0.x, fma(-pi, x0.y, y.x)), fma(-pr, x0.y, fma(pi, x0.x, y.y)));
     })
 }
 template <int K, class V>
@@ -648,6 +665,17 @@ __device__ __forceinline__ void pRX2(PRegs &R, PRegs &I, const double *c) {
         nix = fma2(u, ix, neg2(ry));
         nry = fma2(u, ry, ix);
         niy = fma2(u, iy, neg2(rx));
+    })
+}
+template <int K>
+__device__ __forceinline__ void pRN1(PRegs &R, PRegs &I, const double *c) {
+    constexpr bool HI = false;
+    const float2 pr = b2((float) c[0]), pi = b2((float) c[1]), npr = b2(-(float) c[0]), npi = b2(-(float) c[1]);
+    DGQP_PAIR_LOOP(K, false, 0u, {
+        nrx = fma2(pr, ry, fma2(npi, iy, rx));
+        nix = fma2(pr, iy, fma2(pi, ry, ix));
+        nry = fma2(npr, rx, fma2(npi, ix, ry));
+        niy = fma2(npr, ix, fma2(pi, rx, iy));
     })
 }
 template <int K>

@@ -212,6 +212,7 @@ double opFlopsPerAmp(const KOp &op) {
         case KOP_RX2: f = 4.0; break;   // one FMA per output component
         case KOP_H1: f = 2.0; break;    // one add per output component
         case KOP_PH1: f = 3.0; break;   // a complex multiply on half of the amplitudes
+        case KOP_RN1: f = 8.0; break;   // x + p y: two complex FMAs per amplitude
         default: f = 0.0; break;
     }
     const int c = __builtin_popcount(op.ctrlReg) + __builtin_popcount(op.ctrlLoc) + __builtin_popcount(op.ctrlCta);
@@ -459,6 +460,33 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     default: {
                         double m[8];
                         gateMatrix(g, m);
+                        // uncontrolled rotation about an axis in the XY plane:
+                        // U = d [[1, p], [-conj(p), 1]] with d = U00 = U11,
+                        // |p| <= 1; d goes to the sweep's global factor
+                        const double d2 = m[0] * m[0] + m[1] * m[1];
+                        const double o2 = m[2] * m[2] + m[3] * m[3];
+                        const double tol = 1e-15 * std::sqrt(d2 + o2);
+                        if (free && d2 > 0.0 && o2 <= d2 * (1.0 + 1e-12) && std::fabs(m[6] - m[0]) <= tol &&
+                            std::fabs(m[7] - m[1]) <= tol) {
+                            // p = U01 / U00, q = U10 / U00 must equal -conj(p)
+                            const double pr = (m[2] * m[0] + m[3] * m[1]) / d2, pi = (m[3] * m[0] - m[2] * m[1]) / d2;
+                            const double qr = (m[4] * m[0] + m[5] * m[1]) / d2, qi = (m[5] * m[0] - m[4] * m[1]) / d2;
+                            if (std::fabs(qr + pr) <= 1e-14 && std::fabs(qi - pi) <= 1e-14) {
+                                scaleBy(m[0], m[1]);
+                                if (std::fabs(pi) <= 1e-16) {
+                                    op.kind = KOP_RY1;  // p = -t
+                                    coef.push_back(-pr);
+                                } else if (std::fabs(pr) <= 1e-16) {
+                                    op.kind = KOP_RX1;  // p = -i t
+                                    coef.push_back(-pi);
+                                } else {
+                                    op.kind = KOP_RN1;
+                                    coef.push_back(pr);
+                                    coef.push_back(pi);
+                                }
+                                break;
+                            }
+                        }
                         if (isZero(m[1]) && isZero(m[3]) && isZero(m[5]) && isZero(m[7])) {
                             op.kind = KOP_M2R;
                             coef.insert(coef.end(), {m[0], m[2], m[4], m[6]});
@@ -497,6 +525,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
                     case KOP_RX2: op.code = (uint8_t) (KC_RX2 + op.k); break;
                     case KOP_H1: op.code = (uint8_t) (KC_H1 + op.k); break;
                     case KOP_PH1: op.code = (uint8_t) (selIsReg ? KC_PH1R + op.k : KC_PH1T); break;
+                    case KOP_RN1: op.code = (uint8_t) (KC_RN1 + op.k); break;
                     default: break;
                 }
                 op.k = kSaved;

@@ -53,7 +53,9 @@ enum KOpKind : uint8_t {
     KOP_RX1 = 14,  // [[1, -i t], [-i t, 1]]   (Rx, t = tan)
     KOP_RX2 = 15,  // [[u, -i], [-i, u]]       (Rx, u = cot)
     KOP_H1 = 16,   // [[1, 1], [1, -1]]        (Hadamard without 1/sqrt 2)
-    KOP_PH1 = 17   // multiply by (c + i s) where the selector bit is 1 (Rz without e^{-i a})
+    KOP_PH1 = 17,  // multiply by (c + i s) where the selector bit is 1 (Rz without e^{-i a})
+    KOP_RN1 = 18   // [[1, p], [-conj(p), 1]], p complex: rotations about an axis in the XY plane
+                   // (sqrt X, sqrt Y, sqrt W, ...) divided by their equal diagonal entry
 };
 
 // Dispatch codes of the tile kernel: one straight-line case per
@@ -80,7 +82,8 @@ enum KCode : uint8_t {
     KC_H1 = 86,
     KC_PH1R = 90,  // + k: selector = register bit k
     KC_PH1T = 94,  // selector is a thread/CTA bit
-    KC_COUNT = 95
+    KC_RN1 = 95,   // + k; never controlled
+    KC_COUNT = 99
 };
 
 // 16 bytes; every field is read uniformly by all threads of the CTA.
