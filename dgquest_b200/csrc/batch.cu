@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "batch.h"
 #include "interp.cuh"
@@ -91,16 +92,17 @@ __device__ __noinline__ void addExpectationSums(double tot, const double (&rs)[4
     }
 }
 
-// One tile of one sweep, run by the first 2^(W-4) threads of the CTA.
-template <class V>
-__device__ __noinline__ void sweepTile(const BatchArgs &args, const BatchSweep &h, V *__restrict__ st, uint32_t tile,
-                                       V *sm, double *zs) {
-    const int W = h.tileBits;
-    const uint32_t T = 1u << (W - kRegBits);
+// One tile of one sweep, run by the first 2^(W-4) threads of the CTA; h is
+// the sweep header staged in shared memory.
+template <class V, int W>
+__device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSweep &h, V *__restrict__ st, uint32_t tile,
+                                          V *sm, double *zs) {
+    constexpr uint32_t T = 1u << (W - kRegBits);
     const uint32_t tid = threadIdx.x;
 
     uint64_t tpart = tid & 31u;
     for (int i = 0; i < h.numBits - W; i++) tpart |= (uint64_t) ((tile >> i) & 1u) << h.ctaPos[i];
+#pragma unroll
     for (int i = 0; i < W - 9; i++) tpart |= (uint64_t) ((tid >> (5 + i)) & 1u) << h.highPos[i];
     const uint64_t jb0 = 1ULL << h.highPos[W - 9];
     const uint64_t jb1 = 1ULL << h.highPos[W - 8];
@@ -141,8 +143,8 @@ __device__ __noinline__ void sweepTile(const BatchArgs &args, const BatchSweep &
     }
 
     const KPhase *phases = args.phases + h.phaseOff;
-    const KOp *ops = args.ops + h.opOff;
-    const double *coef = args.coef + h.coefOff;
+    const KOp *__restrict__ ops = args.ops + h.opOff;
+    const double *__restrict__ coef = args.coef + h.coefOff;
     if (h.numPhases > 0) {
 #pragma unroll
         for (int j = 0; j < kRegs; j++) sm[swzB(tid + T * (uint32_t) j)] = a[j];
@@ -150,12 +152,19 @@ __device__ __noinline__ void sweepTile(const BatchArgs &args, const BatchSweep &
         for (int p = 0; p < h.numPhases; p++) {
             const KPhase &ph = phases[p];
             uint32_t loc = 0;
+#pragma unroll
             for (int i = 0; i < W - kRegBits; i++) loc |= ((tid >> i) & 1u) << ph.thrPos[i];
             const uint32_t sb = swzB(loc);
 #pragma unroll
             for (int j = 0; j < kRegs; j++) a[j] = sm[sb ^ ph.regOff[j]];
             const int e = ph.opEnd;
-            for (int o = ph.opBegin; o < e; o++) applyOp(ops[o], coef, a, loc, tile);
+            for (int o = ph.opBegin; o < e; o++) {
+                // the 16-byte op record in one read-only load
+                const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(ops + o));
+                KOp op;
+                memcpy(&op, &raw, sizeof(op));
+                applyOp(op, coef, a, loc, tile);
+            }
 #pragma unroll
             for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];
             groupBarrier(T);
@@ -168,10 +177,22 @@ __device__ __noinline__ void sweepTile(const BatchArgs &args, const BatchSweep &
 #pragma unroll
         for (int j = 0; j < kRegs; j++) a[j] = mk<V>(gr * a[j].x - gi * a[j].y, gr * a[j].y + gi * a[j].x);
     }
+    // store addresses rebuilt here (nothing address-related stays live across the phases)
+    uint64_t tp2 = tid & 31u;
+    for (int i = 0; i < h.numBits - W; i++) tp2 |= (uint64_t) ((tile >> i) & 1u) << h.ctaPos[i];
+#pragma unroll
+    for (int i = 0; i < W - 9; i++) tp2 |= (uint64_t) ((tid >> (5 + i)) & 1u) << h.highPos[i];
+    const uint64_t kb0 = 1ULL << h.highPos[W - 9];
+    const uint64_t kb1 = 1ULL << h.highPos[W - 8];
+    const uint64_t kb2 = 1ULL << h.highPos[W - 7];
+    const uint64_t kb3 = 1ULL << h.highPos[W - 6];
+    auto sidx = [&](int j) -> uint64_t {
+        return tp2 | ((j & 1) ? kb0 : 0ULL) | ((j & 2) ? kb1 : 0ULL) | ((j & 4) ? kb2 : 0ULL) | ((j & 8) ? kb3 : 0ULL);
+    };
     double tot = 0.0, rs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < kRegs; j++) {
-        __stcg(st + gidx(j), a[j]);
+        __stcg(st + sidx(j), a[j]);
         if (zs) {
             const double p = (double) a[j].x * (double) a[j].x + (double) a[j].y * (double) a[j].y;
             tot += p;
@@ -186,6 +207,23 @@ __device__ __noinline__ void sweepTile(const BatchArgs &args, const BatchSweep &
     groupBarrier(T);
 }
 
+// Sweeps [w0, w1) of one register on tile `tile` (one sweep for a tile
+// item, all of them for a whole-register item); each header is copied to
+// shared memory first, so the phase loop holds no header registers.
+template <class V, int W>
+__device__ __forceinline__ void runSweeps(const BatchArgs &args, const BatchCircuit &C, uint32_t w0, uint32_t w1,
+                                       uint32_t tile, V *sm, BatchSweep *hs) {
+    constexpr uint32_t T = 1u << (W - kRegBits);
+    V *st = reinterpret_cast<V *>(C.state);
+    for (uint32_t w = w0; w < w1; w++) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(args.sweeps + C.firstSweep + w);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(hs);
+        for (uint32_t i = threadIdx.x; i < sizeof(BatchSweep) / 4; i += T) dst[i] = __ldg(src + i);
+        groupBarrier(T);
+        sweepTile<V, W>(args, *hs, st, tile, sm, w + 1 == C.numSweeps ? args.zsum + C.zOff : nullptr);
+    }
+}
+
 template <class V>
 __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
     batchKernel(const __grid_constant__ BatchArgs args) {
@@ -193,6 +231,7 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
     V *sm = reinterpret_cast<V *>(smRaw);
     __shared__ uint64_t sItem;
     __shared__ uint32_t sAbort;
+    __shared__ BatchSweep sHead;
     const uint32_t tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
@@ -222,14 +261,14 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
         __syncthreads();
         if (sAbort) break;
         const uint32_t T = 1u << (C.tileBits - kRegBits);
-        double *zs = args.zsum + C.zOff;
         if (tid < T) {
-            V *st = reinterpret_cast<V *>(C.state);
-            if (s == kBatchWhole) {
-                for (uint32_t w = 0; w < C.numSweeps; w++)
-                    sweepTile<V>(args, args.sweeps[C.firstSweep + w], st, 0u, sm, w + 1 == C.numSweeps ? zs : nullptr);
-            } else {
-                sweepTile<V>(args, args.sweeps[C.firstSweep + s], st, t, sm, s + 1 == C.numSweeps ? zs : nullptr);
+            const uint32_t w0 = s == kBatchWhole ? 0u : s, w1 = s == kBatchWhole ? C.numSweeps : s + 1;
+            const uint32_t tile = s == kBatchWhole ? 0u : t;
+            switch (C.tileBits) {
+                case 9: runSweeps<V, 9>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 10: runSweeps<V, 10>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 11: runSweeps<V, 11>(args, C, w0, w1, tile, sm, &sHead); break;
+                default: runSweeps<V, 12>(args, C, w0, w1, tile, sm, &sHead); break;
             }
             __threadfence();
         }
