@@ -291,19 +291,56 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         h.restrictValue = s.rValue;
         h.restrictScale = s.rScale;
     }
-    bool complete = true;
-    std::vector<BlockPlan> blocks = planBlocks(s.pending, s.numBits, W, &complete, paired ? kCoalescedBits + 1 : kCoalescedBits);
-    if (!complete) {
-        err = "a multi-qubit gate is wider than the register tile (max 4 targets)";
-        return E_UNSUPPORTED;
-    }
+    // unitaries wider than a register phase are sweeps of their own: plan
+    // the gates between them as usual
+    s.denseHost.clear();
     bool first = true;
-    for (const auto &b : blocks) {
-        SweepHeader hb = first ? h : SweepHeader();
-        if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err, paired)) return E_UNSUPPORTED;
-        first = false;
+    std::vector<Gate> seg;
+    auto planSegment = [&]() -> int {
+        if (seg.empty()) return 0;
+        bool complete = true;
+        std::vector<BlockPlan> blocks =
+            planBlocks(seg, s.numBits, W, &complete, paired ? kCoalescedBits + 1 : kCoalescedBits);
+        if (!complete) {
+            err = "a multi-qubit gate is wider than the register tile";
+            return E_UNSUPPORTED;
+        }
+        for (const auto &b : blocks) {
+            SweepHeader hb = first ? h : SweepHeader();
+            if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err, paired)) return E_UNSUPPORTED;
+            first = false;
+        }
+        seg.clear();
+        return 0;
+    };
+    for (const Gate &g : s.pending) {
+        if (g.type != OP_MULTI_UNITARY || g.numMultiTargets <= kRegBits) {
+            seg.push_back(g);
+            continue;
+        }
+        if (int code = planSegment()) return code;
+        if (first) {
+            // the initialisation / collapse runs before the dense sweep
+            out.emplace_back();
+            encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
+            st.sweeps++;
+            first = false;
+        }
+        TileProgram &p = out.emplace_back();
+        std::memset(&p, 0, sizeof(p));
+        p.numBits = s.numBits;
+        p.numReal = s.numQubits;
+        p.globalRe = 1.0;
+        p.denseK = g.numMultiTargets;
+        p.denseOff = (uint32_t) s.denseHost.size();
+        for (int i = 0; i < g.numMultiTargets; i++) p.denseTargets[i] = (uint8_t) g.multiTargets[i];
+        const auto &m = s.pool.mats[(size_t) g.multiIndex];
+        s.denseHost.insert(s.denseHost.end(), m.begin(), m.end());
+        st.sweeps++;
+        st.flopsPerAmp += 8.0 * (double) (1 << g.numMultiTargets);
     }
-    if (blocks.empty()) {
+    if (int code = planSegment()) return code;
+    if (out.empty()) {
         out.emplace_back();
         encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
         st.sweeps = 1;
@@ -324,6 +361,9 @@ void consumePending(QuregState &s) {
 }  // namespace dgq
 
 namespace {
+
+cudaError_t allocOn(void **ptr, size_t bytes, cudaStream_t st);
+void freeOn(void *ptr, cudaStream_t st);
 
 // 0: compile specialised kernels when a plan needs them; 1: specialise only
 // plans whose kernels are compiled already, interpret the others while
@@ -362,9 +402,9 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
         for (int i = 0; i <= last; i++) {
             dgq::TileProgram &p = s.planned[(size_t) i];
             p.isSingle = s.single ? 1 : 0;
-            if (!s.single) continue;
+            if (!s.single || p.denseK) continue;
             const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
-            if (prev && prev->renormOut) {
+            if (prev && prev->renormOut && !prev->denseK) {
                 p.renormIn = 1;
                 p.normIn = prev->normOut;
             }
@@ -388,8 +428,12 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.stats.jitMillis = 0.0;
     if (specialise && wantJit) {
         std::vector<std::string> sources;
-        sources.reserve(s.planned.size());
-        for (const auto &p : s.planned) sources.push_back(dgq::generateSweepSource(p, W));
+        std::vector<size_t> which;  // tile programs (dense sweeps have their own kernel)
+        for (size_t i = 0; i < s.planned.size(); i++)
+            if (!s.planned[i].denseK) {
+                sources.push_back(dgq::generateSweepSource(s.planned[i], W));
+                which.push_back(i);
+            }
         if (g_specPolicy.load() == 1 && !dgq::jitAllReady(sources)) {
             dgq::jitCompileInBackground(sources);
             if (paired || W > dgq::kMaxTileBitsF64) {
@@ -401,12 +445,24 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
         } else {
             dgq::JitStats js;
             std::string jerr;
-            if (!dgq::jitGetKernels(sources, s.plannedFns, &js, &jerr))
-                return raise(E_UNSUPPORTED, func, jerr.c_str());
+            std::vector<CUfunction> fns;
+            if (!dgq::jitGetKernels(sources, fns, &js, &jerr)) return raise(E_UNSUPPORTED, func, jerr.c_str());
+            for (size_t k = 0; k < which.size(); k++) s.plannedFns[which[k]] = fns[k];
             s.stats.jitCompiled = js.compiled;
             s.stats.jitReused = js.reused;
             s.stats.jitMillis = js.compileMillis;
         }
+    }
+    if (!s.denseHost.empty()) {
+        // a new buffer per plan, freed in stream order after earlier launches
+        freeOn(s.dDense, s.stream);
+        s.dDense = nullptr;
+        if (!cudaOk(allocOn((void **) &s.dDense, s.denseHost.size() * sizeof(double), s.stream), func) ||
+            !cudaOk(cudaMemcpyAsync(s.dDense, s.denseHost.data(), s.denseHost.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, s.stream),
+                    func) ||
+            !cudaOk(cudaStreamSynchronize(s.stream), func))
+            return false;
     }
     s.plannedPaired = paired;
     s.plannedTileBits = W;
@@ -429,8 +485,17 @@ bool launchPlanned(QuregState &s, const char *func) {
         if (s.planned[i].renormOut &&
             !cudaOk(cudaMemsetAsync(s.planned[i].normOut, 0, sizeof(double), s.stream), func))
             return false;
-        const cudaError_t e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, s.planned[i], s.stream)
-                                 : dgq::launchTile(s.dState, s.single, s.plannedTileBits, s.planned[i], s.stream);
+        const dgq::TileProgram &p = s.planned[i];
+        cudaError_t e;
+        if (p.denseK) {
+            dgq::DenseArgs da;
+            if (!dgq::denseArgs(s.numBits, p.denseK, p.denseTargets, da))
+                return raise(E_UNSUPPORTED, func, "dense unitary does not fit the register");
+            e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
+        } else {
+            e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, p, s.stream)
+                   : dgq::launchTile(s.dState, s.single, s.plannedTileBits, p, s.stream);
+        }
         if (!cudaOk(e, func)) return false;
         g_launches++;
     }
@@ -877,6 +942,7 @@ void destroyQureg(Qureg qureg, QuESTEnv env) {
         freeOn(s->dPartial, s->stream);
         freeOn(s->dProbOut, s->stream);
         freeOn(s->dNorm, s->stream);
+        freeOn(s->dDense, s->stream);
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
     }
@@ -1250,8 +1316,8 @@ void multiQubitUnitary(Qureg q, int *targs, int numTargs, ComplexMatrixN u) {
         recordMatrix(q, tm, 0, m2);
         return;
     }
-    if (numTargs > dgq::kRegBits) {
-        raise(E_UNSUPPORTED, __func__, "multiQubitUnitary supports at most 4 targets in the FP64 tile path");
+    if (numTargs > dgq::kMaxDenseTargets) {
+        raise(E_UNSUPPORTED, __func__, "multiQubitUnitary supports at most 7 targets");
         return;
     }
     QuregState &s = *stateOf(q);

@@ -122,6 +122,13 @@ void planAll(const std::vector<QuregState *> &regs, const std::vector<int> &whic
                 plans[i].errMsg = err;
                 continue;
             }
+            bool dense = false;
+            for (const auto &pg : progs) dense = dense || pg.denseK;
+            if (dense) {
+                plans[i].err = E_UNSUPPORTED;
+                plans[i].errMsg = "a batch register uses a multi-qubit unitary of more than 4 targets";
+                continue;
+            }
             compact(progs, w, plans[i]);
             plans[i].flopsPerAmp = st.flopsPerAmp;
         }

@@ -476,6 +476,7 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
 }
 
 std::string generateSweepSource(const TileProgram &prog, int W) {
+    if (prog.denseK) return std::string();  // dense sweeps run the dense kernel (dense.cu)
     if (prog.paired) return generatePairedSource(prog, W);
     if (usePersistent(prog)) return generatePersistent(prog, W);
     const int T = 1 << (W - kRegBits);

@@ -42,6 +42,25 @@ struct InnerArgs {
     uint8_t l2vKet[kMaxStateBits];
 };
 
+// Dense multi-target unitaries (csrc/dense.cu): 5..7 targets.
+constexpr int kMinDenseTargets = 5;
+constexpr int kMaxDenseTargets = 7;
+struct DenseArgs {
+    int32_t numBits = 0;
+    int32_t tileBits = 0;       // min(12, numBits): targets + lowest other bits
+    int32_t hasRestrict = 0;
+    uint64_t restrictMask = 0, restrictValue = 0;
+    double restrictScale = 1.0;
+    uint8_t tilePos[12] = {0};  // address bit of tile bit b (ascending)
+    int8_t rowBit[12] = {0};    // matrix-index bit of tile bit b, or -1
+    int8_t colBit[12] = {0};    // column-index bit of tile bit b, or -1
+    uint8_t ctaPos[kMaxStateBits] = {0};
+};
+// Fills the tile map for K targets (targets[i] = address bit of matrix bit i).
+bool denseArgs(int numBits, int K, const uint8_t *targets, DenseArgs &a);
+// U: 2^K x 2^K row-major, (re, im) interleaved FP64, in device memory.
+cudaError_t launchDense(void *st, bool single, int K, const DenseArgs &a, const double *U, cudaStream_t s);
+
 struct SampleArgs {
     uint64_t numAmps;
     uint64_t restrictMask, restrictValue;  // lazy collapse (mask 0: none)

@@ -50,6 +50,9 @@ struct QuregState {
 
     int tileBitsSetting = 0;  // 0 = cost model
     bool allowPaired = true;  // complex64: the paired form where it applies
+    // matrices of the planned dense sweeps (host copy and device buffer)
+    std::vector<double> denseHost;
+    double *dDense = nullptr;
     bool plannedPaired = false;
     std::vector<dgq::TileProgram> planned;
     std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)

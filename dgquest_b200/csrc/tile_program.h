@@ -147,6 +147,12 @@ struct TileProgram {
     // op.k == 4 act on the pair inside a slot (target address bit 0).
     uint8_t paired;
     uint8_t pad0[1];
+    // > 0: not a tile sweep but a dense 2^denseK x 2^denseK unitary on the
+    // address bits denseTargets[0..denseK) (bit 0 of the matrix index first);
+    // its matrix is at denseOff doubles into the register's matrix buffer
+    int32_t denseK;
+    uint32_t denseOff;
+    uint8_t denseTargets[8];
     KPhase phases[kMaxPhases];
     KOp ops[kMaxOps];
     double coef[kMaxCoef];

@@ -122,6 +122,11 @@ class Oracle:
     def total_prob(self):
         return lib().orc_total_prob(self.ptr)
 
+    def collapse(self, q, outcome):
+        """collapseToOutcome: keep the amplitudes with bit q == outcome, renormalised."""
+        p0 = lib().orc_prob_zero(self.ptr, q)
+        lib().orc_collapse(self.ptr, q, outcome, p0 if outcome == 0 else 1.0 - p0)
+
     def measure(self, q):
         p = c_double()
         return lib().orc_measure(self.ptr, q, ctypes.byref(p)), p.value
