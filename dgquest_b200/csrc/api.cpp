@@ -336,6 +336,13 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         for (int i = 0; i < g.numMultiTargets; i++) p.denseTargets[i] = (uint8_t) g.multiTargets[i];
         const auto &m = s.pool.mats[(size_t) g.multiIndex];
         s.denseHost.insert(s.denseHost.end(), m.begin(), m.end());
+        if (s.single && g.numMultiTargets == 6 && s.numBits >= 12) {
+            // the tensor-core operand: 2 x 128 x 128 floats in the doubles buffer
+            const size_t nf = tcDenseMatrixFloats();
+            p.denseTcOff = (uint32_t) s.denseHost.size();
+            s.denseHost.resize(s.denseHost.size() + (nf + 1) / 2, 0.0);
+            packTcDenseMatrix(m.data(), reinterpret_cast<float *>(s.denseHost.data() + p.denseTcOff));
+        }
         st.sweeps++;
         st.flopsPerAmp += 8.0 * (double) (1 << g.numMultiTargets);
     }
@@ -364,6 +371,10 @@ namespace {
 
 cudaError_t allocOn(void **ptr, size_t bytes, cudaStream_t st);
 void freeOn(void *ptr, cudaStream_t st);
+
+// Dense 6-target unitaries on complex64 registers run on the tensor cores
+// (dgq_setTensorCores(0): the SIMT dense kernel instead).
+std::atomic<int> g_tensorCores{1};
 
 // 0: compile specialised kernels when a plan needs them; 1: specialise only
 // plans whose kernels are compiled already, interpret the others while
@@ -491,7 +502,13 @@ bool launchPlanned(QuregState &s, const char *func) {
             dgq::DenseArgs da;
             if (!dgq::denseArgs(s.numBits, p.denseK, p.denseTargets, da))
                 return raise(E_UNSUPPORTED, func, "dense unitary does not fit the register");
-            e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
+            if (p.denseTcOff && g_tensorCores.load()) {
+                static uint32_t *errWord = dgq::tcDenseErrorWord();
+                e = dgq::launchTcDense((float2 *) s.dState, da,
+                                       reinterpret_cast<const float *>(s.dDense + p.denseTcOff), errWord, s.stream);
+            } else {
+                e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
+            }
         } else {
             e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, p, s.stream)
                    : dgq::launchTile(s.dState, s.single, s.plannedTileBits, p, s.stream);
@@ -802,6 +819,15 @@ int dgq_setSpecialisationPolicy(int policy) {
         return -1;
     }
     return g_specPolicy.exchange(policy);
+}
+
+int dgq_setTensorCores(int enable) { return g_tensorCores.exchange(enable ? 1 : 0); }
+
+int dgq_getDeviceErrors(void) {
+    uint32_t *w = dgq::tcDenseErrorWord();
+    uint32_t v = 0;
+    if (!w || cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return (int) v;
 }
 
 int64_t dgq_getAvailableMemory(void) {

@@ -61,6 +61,14 @@ bool denseArgs(int numBits, int K, const uint8_t *targets, DenseArgs &a);
 // U: 2^K x 2^K row-major, (re, im) interleaved FP64, in device memory.
 cudaError_t launchDense(void *st, bool single, int K, const DenseArgs &a, const double *U, cudaStream_t s);
 
+// Tensor-core form for complex64 and 6 targets (tc_dense.cu): the matrix is
+// packed on the host (packTcDenseMatrix, tcDenseMatrixFloats floats).
+void packTcDenseMatrix(const double *U, float *out);
+size_t tcDenseMatrixFloats();
+// Device word set to 1 when a tensor-core sweep gave up waiting for its MMAs.
+uint32_t *tcDenseErrorWord();
+cudaError_t launchTcDense(float2 *st, const DenseArgs &a, const float *Apacked, uint32_t *error, cudaStream_t s);
+
 struct SampleArgs {
     uint64_t numAmps;
     uint64_t restrictMask, restrictValue;  // lazy collapse (mask 0: none)

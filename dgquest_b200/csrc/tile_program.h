@@ -152,6 +152,7 @@ struct TileProgram {
     // its matrix is at denseOff doubles into the register's matrix buffer
     int32_t denseK;
     uint32_t denseOff;
+    uint32_t denseTcOff;  // complex64, 6 targets: packed tensor-core operand (0: none)
     uint8_t denseTargets[8];
     KPhase phases[kMaxPhases];
     KOp ops[kMaxOps];

@@ -185,6 +185,8 @@ _SIGS = {
     "dgq_compileSweepSource": (I, [ctypes.c_char_p, ctypes.c_char_p, I]),
     "dgq_setSpecialisationMinBits": (I, [I]),
     "dgq_setSpecialisationPolicy": (I, [I]),
+    "dgq_setTensorCores": (I, [I]),
+    "dgq_getDeviceErrors": (I, []),
     "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),

@@ -128,6 +128,14 @@ int dgq_setSpecialisationMinBits(int minBits);
  * compile on background host threads for later plans of the same structure
  * (for serving one-off circuits). Returns the previous policy. */
 int dgq_setSpecialisationPolicy(int policy);
+/* multiQubitUnitary with 6 targets on a complex64 register of >= 12 qubits
+ * runs on the tensor cores (tcgen05, 3xTF32 split, FP32 accumulation) when
+ * enabled (default 1); 0 selects the SIMT dense kernel. Returns the previous
+ * setting. */
+int dgq_setTensorCores(int enable);
+/* Nonzero when a tensor-core sweep stopped waiting for its MMAs (bounded
+ * wait); its output is then invalid. Waits for the device. */
+int dgq_getDeviceErrors(void);
 
 /* Host-only view of the runtime specialisation: the CUDA source generated
  * for sweep `sweep` of the plan of the given gates (same encoding as

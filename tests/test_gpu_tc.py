@@ -1,0 +1,49 @@
+"""Dense 6-target unitaries on complex64 registers through the tensor cores
+(tcgen05, 3xTF32): against the oracle (fidelity >= 1 - 1e-6, max amplitude
+error <= 2e-6) and against the SIMT dense kernel (<= 2e-6), with no MMA wait
+timing out."""
+import numpy as np
+import pytest
+
+import oracle
+from dgquest_b200 import circuits as C
+
+pytestmark = pytest.mark.gpu
+
+
+def run(Q, env, n, targs, u, pre, post):
+    q = Q.dgq_createQuregF32(n, env)
+    C.replay(q, pre)
+    m = Q.matrixN(u)
+    Q.multiQubitUnitary(q, Q.int_array(targs), len(targs), m)
+    Q.destroyComplexMatrixN(m)
+    C.replay(q, post)
+    amps = Q.state_vector(q)
+    Q.destroyQureg(q, env)
+    return amps
+
+
+@pytest.mark.parametrize("n,targs", [(12, [0, 1, 2, 3, 4, 5]), (12, [11, 3, 7, 0, 9, 5]), (16, [15, 2, 9, 4, 12, 0]),
+                                     (20, [6, 19, 1, 13, 8, 3])])
+def test_tensor_core_dense(quest, env, n, targs):
+    Q = quest
+    u = C.random_unitary(np.random.default_rng(n + targs[0]), 64)
+    pre = C.random_layers(n, 2, C.config_seed(3, n))
+    post = C.random_layers(n, 1, C.config_seed(3, 100 + n))
+    prev = Q.dgq_setTensorCores(1)
+    try:
+        a_tc = run(Q, env, n, targs, u, pre, post)
+        assert Q.dgq_getDeviceErrors() == 0
+        Q.dgq_setTensorCores(0)
+        a_simt = run(Q, env, n, targs, u, pre, post)
+    finally:
+        Q.dgq_setTensorCores(prev)
+    o = oracle.Oracle(n)
+    o.apply(pre)
+    o.multi_qubit_unitary(targs, u)
+    o.apply(post)
+    ref = o.amps()
+    o.close()
+    assert abs(np.vdot(ref, a_tc)) ** 2 >= 1 - 1e-6
+    assert np.abs(a_tc - ref).max() <= 2e-6
+    assert np.abs(a_tc - a_simt).max() <= 2e-6
