@@ -327,6 +327,24 @@ def run_ncu_case(args):
     from dgquest_b200 import circuits as C
     from dgquest_b200 import quest as Q
     env = Q.createQuESTEnv()
+    if args.dense_case:
+        # two dense 6-qubit unitaries on a complex64 register (tensor cores), plan launched twice
+        gen = np.random.default_rng(7)
+        q = Q.dgq_createQuregF32(args.qubits, env)
+        Q.initPlusState(q)
+        for t in ([0, 1, 2, 3, 4, 5], [args.qubits - 1, 7, 15, 3, 11, 9]):
+            m = Q.matrixN(C.random_unitary(gen, 64))
+            Q.multiQubitUnitary(q, Q.int_array(t), 6, m)
+            Q.destroyComplexMatrixN(m)
+        Q.dgq_planPending(q)
+        for _ in range(2):
+            Q.dgq_launchPlanned(q)
+        Q.dgq_sync(q)
+        print(json.dumps({"case": "dense", "qubits": args.qubits, "sweeps": Q.plan_stats(q).sweeps,
+                          "norm": Q.calcTotalProb(q), "device_errors": Q.dgq_getDeviceErrors()}))
+        Q.destroyQureg(q, env)
+        Q.destroyQuESTEnv(env)
+        return
     if args.batch_case:
         single = args.precision == 1
         regs = []
@@ -360,6 +378,68 @@ def run_ncu_case(args):
                       "sweeps": st.sweeps, "norm": Q.calcTotalProb(q)}))
     Q.destroyQureg(q, env)
     Q.destroyQuESTEnv(env)
+
+
+def run_dense_form(args, world):
+    """Dense 6-qubit blocks: multiQubitUnitary with 6 targets on a 30-qubit
+    register, complex64 on the tensor cores (tcgen05, 3xTF32) and on the SIMT
+    dense kernel, complex128 on the SIMT dense kernel. Time per dense sweep."""
+    import torch
+
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    n = args.dense_qubits
+    gen = np.random.default_rng(7)
+    blocks = [([0, 1, 2, 3, 4, 5], C.random_unitary(gen, 64)), ([29, 7, 15, 22, 3, 11], C.random_unitary(gen, 64)),
+              ([6, 12, 18, 24, 28, 1], C.random_unitary(gen, 64)), ([10, 27, 5, 20, 14, 26], C.random_unitary(gen, 64))]
+    blocks = [(t, u) for t, u in blocks if max(t) < n]
+    env = Q.createQuESTEnv()
+    out = {"workload": f"{len(blocks)} dense 6-qubit unitaries (64x64) on {n} qubits", "qubits": n}
+    runs = (("complex64_tensor_cores", True, 1), ("complex64_simt", True, 0), ("complex128_simt", False, 0))
+    states = {}
+    for name, single, tc in runs:
+        prev = Q.dgq_setTensorCores(tc)
+        q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+        Q.initPlusState(q)
+        for t, u in blocks:
+            m = Q.matrixN(u)
+            Q.multiQubitUnitary(q, Q.int_array(t), 6, m)
+            Q.destroyComplexMatrixN(m)
+        Q.dgq_planPending(q)
+        st = Q.plan_stats(q)
+        stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+        for _ in range(args.warmup):
+            Q.dgq_launchPlanned(q)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        steps = max(1, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(steps):
+            Q.dgq_launchPlanned(q)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        Q.dgq_setTensorCores(prev)
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
+        # per dense block: the plan's time over its blocks (the init pass and, on
+        # complex64 tensor cores, the final renormalisation pass included)
+        per = ms / max(1, len(blocks))
+        amp = 8 if single else 16
+        flops = 8.0 * 64 * (1 << n)  # complex MACs x 8 per dense sweep (algorithmic)
+        out[name] = {"ms_per_plan": ms, "sweeps": st.sweeps, "ms_per_block": per,
+                     "tflops_algorithmic": flops / (per / 1e3) / 1e12,
+                     "hbm_gbs": 2.0 * (1 << n) * amp / (per / 1e3) / 1e9,
+                     "device_errors": Q.dgq_getDeviceErrors()}
+        states[name] = q
+    out["fidelity_tc_vs_complex128"] = Q.calcFidelity(states["complex128_simt"], states["complex64_tensor_cores"])
+    out["fidelity_simt_complex64_vs_complex128"] = Q.calcFidelity(states["complex128_simt"],
+                                                                  states["complex64_simt"])
+    out["speedup_tc_vs_simt_complex64"] = (out["complex64_simt"]["ms_per_block"] /
+                                           out["complex64_tensor_cores"]["ms_per_block"])
+    for q in states.values():
+        Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+    return out
 
 
 def run_precision_form(args, world):
@@ -527,9 +607,12 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
+    ap.add_argument("--no-dense", action="store_true")
+    ap.add_argument("--dense-qubits", type=int, default=30)
     ap.add_argument("--batch-circuits", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--batch-case", type=int, default=0, help="--ncu-case: a batch of this many workload circuits")
+    ap.add_argument("--dense-case", action="store_true", help="--ncu-case: dense 6-qubit unitaries, complex64")
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--precision", type=int, default=2, choices=[1, 2], help="--ncu-case register precision")
@@ -549,6 +632,10 @@ def main():
             dist.destroy_process_group()
         return
     line = run_gpu(args, world, rank, local)
+    if not args.no_dense:
+        dense = run_dense_form(args, world)
+        if rank == 0:
+            line["dense_blocks"] = dense
     if not args.no_grid32:
         grid = run_precision_form(args, world)
         if rank == 0:

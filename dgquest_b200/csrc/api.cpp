@@ -347,6 +347,14 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         st.flopsPerAmp += 8.0 * (double) (1 << g.numMultiTargets);
     }
     if (int code = planSegment()) return code;
+    if (s.single && !out.empty() && out.back().denseTcOff) {
+        // a tensor-core sweep rounds its FP32 sums toward zero: end with a
+        // pass that renormalises its output (wired by the renormalisation
+        // schedule, which puts a measurement on the sweep before the last)
+        out.emplace_back();
+        encodeHeaderOnly(s.numBits, s.numQubits, W, SweepHeader(), out.back(), paired);
+        st.sweeps++;
+    }
     if (out.empty()) {
         out.emplace_back();
         encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
@@ -413,9 +421,9 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
         for (int i = 0; i <= last; i++) {
             dgq::TileProgram &p = s.planned[(size_t) i];
             p.isSingle = s.single ? 1 : 0;
-            if (!s.single || p.denseK) continue;
+            if (!s.single) continue;
             const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
-            if (prev && prev->renormOut && !prev->denseK) {
+            if (prev && prev->renormOut) {
                 p.renormIn = 1;
                 p.normIn = prev->normOut;
             }
@@ -502,6 +510,8 @@ bool launchPlanned(QuregState &s, const char *func) {
             dgq::DenseArgs da;
             if (!dgq::denseArgs(s.numBits, p.denseK, p.denseTargets, da))
                 return raise(E_UNSUPPORTED, func, "dense unitary does not fit the register");
+            if (p.renormIn) da.normIn = p.normIn;
+            if (p.renormOut) da.normOut = p.normOut;
             if (p.denseTcOff && g_tensorCores.load()) {
                 static uint32_t *errWord = dgq::tcDenseErrorWord();
                 e = dgq::launchTcDense((float2 *) s.dState, da,

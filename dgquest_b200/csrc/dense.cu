@@ -43,13 +43,18 @@ __global__ void __launch_bounds__(256, 2) denseKernel(V *__restrict__ st, const 
     uint64_t base = 0;
     for (int i = 0; i < a.numBits - TB; i++) base |= (uint64_t) ((cta >> i) & 1u) << a.ctaPos[i];
 
-    // address-ordered tile index i -> (address, row, column)
-    auto place = [&](uint32_t i, uint64_t &addr, uint32_t &row, uint32_t &col) {
-        addr = base;
+    // address-ordered tile index i = tid + T j -> (address, row, column): the
+    // bits of tid and of j are disjoint, so their parts OR together; the 16
+    // j parts sit in a table
+    __shared__ uint64_t jAddr[16];
+    __shared__ uint32_t jRow[16], jCol[16];
+    const int tb = TB - 4;  // bits of tid
+    auto part = [&](uint32_t bits, int from, int to, uint64_t &addr, uint32_t &row, uint32_t &col) {
+        addr = 0;
         row = 0;
         col = 0;
-        for (int b = 0; b < TB; b++) {
-            if (!((i >> b) & 1u)) continue;
+        for (int b = from; b < to; b++) {
+            if (!((bits >> (b - from)) & 1u)) continue;
             addr |= 1ULL << a.tilePos[b];
             const int r = a.rowBit[b];
             if (r >= 0)
@@ -58,20 +63,31 @@ __global__ void __launch_bounds__(256, 2) denseKernel(V *__restrict__ st, const 
                 col |= 1u << a.colBit[b];
         }
     };
+    if (tid < 16) {
+        uint64_t ad;
+        uint32_t r, c;
+        part(tid, tb, TB, ad, r, c);
+        jAddr[tid] = ad;
+        jRow[tid] = r;
+        jCol[tid] = c;
+    }
+    uint64_t tAddr;
+    uint32_t tRow, tCol;
+    part(tid, 0, tb, tAddr, tRow, tCol);
+    tAddr |= base;
+    __syncthreads();
 
+    R inScale = (R) 1;
+    if (a.normIn) inScale = (R) rsqrt(*a.normIn);
     if ((int) tid < T) {
         for (int j = 0; j < 16; j++) {
-            const uint32_t i = tid + (uint32_t) T * (uint32_t) j;
-            uint64_t addr;
-            uint32_t row, col;
-            place(i, addr, row, col);
+            const uint64_t addr = tAddr | jAddr[j];
             V v = st[addr];
-            if (a.hasRestrict) {
-                const bool keep = (addr & a.restrictMask) == a.restrictValue;
-                const R sc = (R) a.restrictScale;
-                v = keep ? mk<V>(v.x * sc, v.y * sc) : mk<V>((R) 0, (R) 0);
-            }
-            Xs[row * G + col] = v;
+            R sc = inScale;
+            if (a.hasRestrict && (addr & a.restrictMask) != a.restrictValue) sc = (R) 0;
+            else if (a.hasRestrict) sc *= (R) a.restrictScale;
+            v = mk<V>(v.x * sc, v.y * sc);
+            Xs[(tRow | jRow[j]) * G + (tCol | jCol[j])] = v;
         }
     }
     __syncthreads();
@@ -120,13 +136,24 @@ __global__ void __launch_bounds__(256, 2) denseKernel(V *__restrict__ st, const 
             for (int q = 0; q < 4; q++) Xs[(rb * 4 + p) * G + cb * 4 + q] = mk<V>(accR[p][q], accI[p][q]);
     }
     __syncthreads();
+    double norm = 0.0;
     if ((int) tid < T) {
         for (int j = 0; j < 16; j++) {
-            const uint32_t i = tid + (uint32_t) T * (uint32_t) j;
-            uint64_t addr;
-            uint32_t row, col;
-            place(i, addr, row, col);
-            st[addr] = Xs[row * G + col];
+            const V y = Xs[(tRow | jRow[j]) * G + (tCol | jCol[j])];
+            st[tAddr | jAddr[j]] = y;
+            norm += (double) y.x * (double) y.x + (double) y.y * (double) y.y;
+        }
+    }
+    if (a.normOut) {
+        __shared__ double red[8];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) norm += __shfl_xor_sync(0xffffffffu, norm, o);
+        if ((tid & 31u) == 0) red[tid >> 5] = norm;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < 8; w++) t += red[w];
+            atomicAdd(a.normOut, t);
         }
     }
 }

@@ -55,6 +55,10 @@ struct DenseArgs {
     int8_t rowBit[12] = {0};    // matrix-index bit of tile bit b, or -1
     int8_t colBit[12] = {0};    // column-index bit of tile bit b, or -1
     uint8_t ctaPos[kMaxStateBits] = {0};
+    // complex64 renormalisation: scale the input by 1/sqrt(*normIn), add the
+    // output's sum of |a|^2 to *normOut (null: off)
+    const double *normIn = nullptr;
+    double *normOut = nullptr;
 };
 // Fills the tile map for K targets (targets[i] = address bit of matrix bit i).
 bool denseArgs(int numBits, int K, const uint8_t *targets, DenseArgs &a);

@@ -39,7 +39,11 @@ constexpr int kTcThreads = 128;
 constexpr uint32_t kABytes = kTcM * kTcKdim * 4;   // 64 KiB per A part
 constexpr uint32_t kBBytes = kTcN * kTcKdim * 4;   // 32 KiB per B part
 constexpr uint32_t kTcSmem = 2 * kABytes + 2 * kBBytes + 1024;
-constexpr uint32_t kTmemCols = 64;
+// eight accumulators (K eighths, all 512 TMEM columns), summed in FP32 with
+// round-to-nearest in the epilogue: each sums 6 MMAs instead of 48, which
+// keeps the tensor core's FP32 accumulation from biasing the norm
+constexpr int kTcAcc = 8;
+constexpr uint32_t kTmemCols = kTcN * kTcAcc;
 
 __device__ __forceinline__ uint32_t smemAddr(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
 
@@ -133,12 +137,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t mbarAddr = smemAddr(&mbar);
     uint32_t parity = 0;
 
-    auto place = [&](uint32_t i, uint64_t tileBase, uint64_t &addr, uint32_t &row, uint32_t &col) {
-        addr = tileBase;
+    // address-ordered tile index i = tid + 128 j: the parts of tid (7 bits)
+    // and of j (5 bits) OR together; the 32 j parts sit in a table
+    __shared__ uint64_t jAddr[32];
+    __shared__ uint32_t jRow[32], jCol[32];
+    auto part = [&](uint32_t bits, int from, int to, uint64_t &addr, uint32_t &row, uint32_t &col) {
+        addr = 0;
         row = 0;
         col = 0;
-        for (int b = 0; b < TB; b++) {
-            if (!((i >> b) & 1u)) continue;
+        for (int b = from; b < to; b++) {
+            if (!((bits >> (b - from)) & 1u)) continue;
             addr |= 1ULL << a.tilePos[b];
             const int r = a.rowBit[b];
             if (r >= 0)
@@ -147,22 +155,47 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 col |= 1u << a.colBit[b];
         }
     };
+    if (tid < 32) {
+        uint64_t ad;
+        uint32_t r, c;
+        part(tid, 7, TB, ad, r, c);
+        jAddr[tid] = ad;
+        jRow[tid] = r;
+        jCol[tid] = c;
+    }
+    uint64_t tAddr;
+    uint32_t tRow, tCol;
+    part(tid, 0, 7, tAddr, tRow, tCol);
+    float inScale = 1.0f;
+    if (a.normIn) inScale = (float) rsqrt(*a.normIn);
+    double norm = 0.0;
+    __syncthreads();
 
+    constexpr int kPer = 4096 / kTcThreads;  // amplitudes per thread and tile
+    auto tileBaseOf = [&](uint32_t tile) {
+        uint64_t b = 0;
+        for (int i = 0; i < a.numBits - TB; i++) b |= (uint64_t) ((tile >> i) & 1u) << a.ctaPos[i];
+        return b;
+    };
+    // the next tile's amplitudes are loaded into registers while the current
+    // tile's MMAs and epilogue run
+    float2 next[kPer];
+    if (blockIdx.x < numTiles) {
+        const uint64_t nb = tileBaseOf(blockIdx.x);
+#pragma unroll
+        for (int j = 0; j < kPer; j++) next[j] = st[nb | tAddr | jAddr[j]];
+    }
     for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x) {
-        uint64_t tileBase = 0;
-        for (int i = 0; i < a.numBits - TB; i++) tileBase |= (uint64_t) ((tile >> i) & 1u) << a.ctaPos[i];
+        const uint64_t tileBase = tileBaseOf(tile);
         // columns -> B head / tail: B[n][k] = Re X[k][n] (k < 64), Im X[k - 64][n]
-        for (uint32_t j = 0; j < (1u << TB) / kTcThreads; j++) {
-            const uint32_t i = tid + kTcThreads * j;
-            uint64_t addr;
-            uint32_t row, col;
-            place(i, tileBase, addr, row, col);
-            float2 v = st[addr];
-            if (a.hasRestrict) {
-                const bool keep = (addr & a.restrictMask) == a.restrictValue;
-                const float sc = (float) a.restrictScale;
-                v = keep ? make_float2(v.x * sc, v.y * sc) : make_float2(0.f, 0.f);
-            }
+#pragma unroll
+        for (int j = 0; j < kPer; j++) {
+            const uint64_t addr = tileBase | tAddr | jAddr[j];
+            const uint32_t row = tRow | jRow[j], col = tCol | jCol[j];
+            float2 v = next[j];
+            float sc = inScale;
+            if (a.hasRestrict) sc = (addr & a.restrictMask) == a.restrictValue ? sc * (float) a.restrictScale : 0.0f;
+            v = make_float2(v.x * sc, v.y * sc);
             const float rh = tf32Head(v.x), ih = tf32Head(v.y);
             const uint32_t oRe = kmajorOffset(col, row, kTcN / 8), oIm = kmajorOffset(col, row + kTcD, kTcN / 8);
             *reinterpret_cast<float *>(bHi + oRe) = rh;
@@ -181,12 +214,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const uint64_t dAl = smemDesc(smemAddr(aLo) + (uint32_t) s * 2 * aLbo, aLbo, 128);
                 const uint64_t dBh = smemDesc(smemAddr(bHi) + (uint32_t) s * 2 * bLbo, bLbo, 128);
                 const uint64_t dBl = smemDesc(smemAddr(bLo) + (uint32_t) s * 2 * bLbo, bLbo, 128);
-                mmaTf32(tmem, dAh, dBh, s > 0 ? 1u : 0u);
-                mmaTf32(tmem, dAh, dBl, 1u);
-                mmaTf32(tmem, dAl, dBh, 1u);
+                // K quarter q = s / 4 accumulates in TMEM columns [64 q, 64 q + 64)
+                const uint32_t acc = tmem + (uint32_t) (s / (kTcKdim / 8 / kTcAcc)) * kTcN;
+                mmaTf32(acc, dAh, dBh, (s % (kTcKdim / 8 / kTcAcc)) != 0 ? 1u : 0u);
+                mmaTf32(acc, dAh, dBl, 1u);
+                mmaTf32(acc, dAl, dBh, 1u);
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbarAddr)
                          : "memory");
+        }
+        if (tile + gridDim.x < numTiles) {
+            const uint64_t nb = tileBaseOf(tile + gridDim.x);
+#pragma unroll
+            for (int j = 0; j < kPer; j++) next[j] = st[nb | tAddr | jAddr[j]];
         }
         if (!waitParity(mbarAddr, parity, 1u << 22)) {
             atomicOr(error, 1u);
@@ -199,32 +239,51 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // D row (lane) 32 w + t: Re Y[row] for rows < 64, Im Y[row - 64] above
         const uint32_t m = warp * 32 + lane;
         float *ysf = reinterpret_cast<float *>(ys);
-#pragma unroll
+#pragma unroll 1
         for (int chunk = 0; chunk < kTcN / 16; chunk++) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((warp * 32u) << 16) + (uint32_t) chunk * 16u;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(taddr)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const uint32_t row = m & (kTcD - 1), part = m >> kTcK;
+            float y[16];
 #pragma unroll
-            for (int q = 0; q < 16; q++) ysf[2 * (row * kTcN + (uint32_t) (chunk * 16 + q)) + part] = __uint_as_float(r[q]);
+            for (int q = 0; q < 16; q++) y[q] = 0.0f;
+#pragma unroll
+            for (int acc = 0; acc < kTcAcc; acc++) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((warp * 32u) << 16) + (uint32_t) (acc * kTcN + chunk * 16);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr)
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int q = 0; q < 16; q++) y[q] += __uint_as_float(r[q]);
+            }
+            const uint32_t row = m & (kTcD - 1), half = m >> kTcK;
+#pragma unroll
+            for (int q = 0; q < 16; q++) ysf[2 * (row * kTcN + (uint32_t) (chunk * 16 + q)) + half] = y[q];
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         for (uint32_t j = 0; j < (1u << TB) / kTcThreads; j++) {
-            const uint32_t i = tid + kTcThreads * j;
-            uint64_t addr;
-            uint32_t row, col;
-            place(i, tileBase, addr, row, col);
-            st[addr] = ys[row * kTcN + col];
+            const float2 y = ys[(tRow | jRow[j]) * kTcN + (tCol | jCol[j])];
+            st[tileBase | tAddr | jAddr[j]] = y;
+            norm += (double) y.x * (double) y.x + (double) y.y * (double) y.y;
         }
         __syncthreads();
+    }
+    if (a.normOut) {
+        __shared__ double red[kTcThreads / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) norm += __shfl_xor_sync(0xffffffffu, norm, o);
+        if (lane == 0) red[warp] = norm;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < kTcThreads / 32; w++) t += red[w];
+            atomicAdd(a.normOut, t);
+        }
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
