@@ -38,7 +38,8 @@ constexpr int kTcN = 64;              // columns per tile (tile = 4096 amplitude
 constexpr int kTcThreads = 128;
 constexpr uint32_t kABytes = kTcM * kTcKdim * 4;   // 64 KiB per A part
 constexpr uint32_t kBBytes = kTcN * kTcKdim * 4;   // 32 KiB per B part
-constexpr uint32_t kTcSmem = 2 * kABytes + 2 * kBBytes + 1024;
+constexpr uint32_t kXBytes = 4096 * 8;                // tile staging: X[column][row], later Y
+constexpr uint32_t kTcSmem = 2 * kABytes + 2 * kBBytes + kXBytes + 1024;
 // eight accumulators (K eighths, all 512 TMEM columns), summed in FP32 with
 // round-to-nearest in the epilogue: each sums 6 MMAs instead of 48, which
 // keeps the tensor core's FP32 accumulation from biasing the norm
@@ -104,7 +105,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     unsigned char *aLo = base + kABytes;
     unsigned char *bHi = base + 2 * kABytes;
     unsigned char *bLo = bHi + kBBytes;
-    float2 *ys = reinterpret_cast<float2 *>(bHi);  // Y staging reuses B (MMAs done by then)
+    // tile staging: X in as [row][column], Y out as [column][row]
+    float2 *xs = reinterpret_cast<float2 *>(bLo + kBBytes);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmemBase;
     __shared__ uint32_t abort;
@@ -195,13 +197,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             float2 v = next[j];
             float sc = inScale;
             if (a.hasRestrict) sc = (addr & a.restrictMask) == a.restrictValue ? sc * (float) a.restrictScale : 0.0f;
-            v = make_float2(v.x * sc, v.y * sc);
-            const float rh = tf32Head(v.x), ih = tf32Head(v.y);
-            const uint32_t oRe = kmajorOffset(col, row, kTcN / 8), oIm = kmajorOffset(col, row + kTcD, kTcN / 8);
-            *reinterpret_cast<float *>(bHi + oRe) = rh;
-            *reinterpret_cast<float *>(bLo + oRe) = v.x - rh;
-            *reinterpret_cast<float *>(bHi + oIm) = ih;
-            *reinterpret_cast<float *>(bLo + oIm) = v.y - ih;
+            xs[row * kTcN + col] = make_float2(v.x * sc, v.y * sc);
+        }
+        __syncthreads();
+        // B head / tail in 16-byte pieces: column n, K chunk c (4 rows of X)
+        // (consecutive threads: consecutive columns, so both the 8-byte reads
+        // and the 16-byte writes are contiguous across a warp)
+        for (uint32_t p = tid; p < kTcN * (kTcKdim / 4); p += kTcThreads) {
+            const uint32_t n = p % kTcN, c = p / kTcN;  // c < 16: real parts, c >= 16: imaginary parts
+            const uint32_t r0 = (c & 15u) * 4u;
+            const float2 x0 = xs[(r0 + 0) * kTcN + n], x1 = xs[(r0 + 1) * kTcN + n];
+            const float2 x2 = xs[(r0 + 2) * kTcN + n], x3 = xs[(r0 + 3) * kTcN + n];
+            float4 v = c < 16 ? make_float4(x0.x, x1.x, x2.x, x3.x) : make_float4(x0.y, x1.y, x2.y, x3.y);
+            const float4 h = make_float4(tf32Head(v.x), tf32Head(v.y), tf32Head(v.z), tf32Head(v.w));
+            const uint32_t off = kmajorOffset(n, c * 4u, kTcN / 8);
+            *reinterpret_cast<float4 *>(bHi + off) = h;
+            *reinterpret_cast<float4 *>(bLo + off) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -238,7 +249,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (abort) break;
         // D row (lane) 32 w + t: Re Y[row] for rows < 64, Im Y[row - 64] above
         const uint32_t m = warp * 32 + lane;
-        float *ysf = reinterpret_cast<float *>(ys);
+        float *ysf = reinterpret_cast<float *>(xs);
 #pragma unroll 1
         for (int chunk = 0; chunk < kTcN / 16; chunk++) {
             float y[16];
@@ -262,12 +273,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             const uint32_t row = m & (kTcD - 1), half = m >> kTcK;
 #pragma unroll
-            for (int q = 0; q < 16; q++) ysf[2 * (row * kTcN + (uint32_t) (chunk * 16 + q)) + half] = y[q];
+            for (int q = 0; q < 16; q++) ysf[2 * ((uint32_t) (chunk * 16 + q) * kTcD + row) + half] = y[q];
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         for (uint32_t j = 0; j < (1u << TB) / kTcThreads; j++) {
-            const float2 y = ys[(tRow | jRow[j]) * kTcN + (tCol | jCol[j])];
+            const float2 y = xs[(tCol | jCol[j]) * kTcD + (tRow | jRow[j])];
             st[tileBase | tAddr | jAddr[j]] = y;
             norm += (double) y.x * (double) y.x + (double) y.y * (double) y.y;
         }
