@@ -453,7 +453,10 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
                 sources.push_back(dgq::generateSweepSource(s.planned[i], W));
                 which.push_back(i);
             }
-        if (g_specPolicy.load() == 1 && !dgq::jitAllReady(sources)) {
+        // policy 1 still compiles for registers of >= 2^28 amplitudes: their
+        // sweeps take longer than a compile, and the interpreting kernel runs
+        // them 2-3x slower than specialised code
+        if (g_specPolicy.load() == 1 && s.numBits < 28 && !dgq::jitAllReady(sources)) {
             dgq::jitCompileInBackground(sources);
             if (paired || W > dgq::kMaxTileBitsF64) {
                 // the interpreting kernel runs unpaired programs of W <= 12
