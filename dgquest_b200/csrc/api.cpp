@@ -19,6 +19,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -186,33 +187,37 @@ uint64_t toVirtualIndex(const QuregState &s, uint64_t logical) {
 // ---------------------------------------------------------------- cost model
 // Recast of dgQuEST's time predictor (src/cpp/time_predictor.cpp:201-395):
 // dgQuEST predicts T(K) = sum over sections of the calculation time
-// (processTime + sum of per-gate times per fused gate) plus transfers, and
-// takes the argmin over K. Here the state stays in HBM, so a plan's time is
-// the sum over sweeps of max(HBM time, FP64 time + shared-memory time), and
-// the argmin is over the tile width W.
+// (processTime + sum of per-gate times per fused gate) plus transfers, with
+// per-gate times measured on its GPU, and takes the argmin over K. Here the
+// state stays in HBM and the argmin is over the tile width W; a plan's time
+// is a cost per sweep (one pass of the state through HBM) plus a cost per
+// register phase (one pass of the tile through shared memory and the FP64
+// pipes), both per amplitude. The two rates are fitted to sweep-kernel times
+// measured on B200 (complex128, 2^28 and 2^30 amplitudes; random layers of
+// depth 8 and 20, a 4-row sqrt-gate grid, GHZ+QFT and a hardware-efficient
+// ansatz, each at W = 10, 11, 12): 2.6 ms per sweep and 1.8 ms per phase
+// for 2^30 amplitudes. For circuits of equal gates the FP64 work is the same
+// at every W, so it lives in those two rates.
 struct CostModel {
-    double hbmBytesPerSec = 6.0e12;
-    double fp64FlopsPerSec = 3.0e13;
-    double smemBytesPerSec = 3.0e13;
+    double sweepSecondsPerAmp = 2.6e-3 / 1073741824.0;
+    double phaseSecondsPerAmp = 1.8e-3 / 1073741824.0;
+    double launchSeconds = 3e-6;
 };
 
-double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, const dgq::MatrixPool &pool) {
+double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, const dgq::MatrixPool &pool,
+                          int lookahead) {
     const CostModel cm;
-    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(gates, numBits, W);
+    std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(gates, numBits, W, nullptr, dgq::kCoalescedBits, lookahead);
     const double amps = std::ldexp(1.0, numBits);
-    double t = 0.0;
+    std::vector<dgq::TileProgram> progs;
+    dgq::PlanStats st;
+    dgq::SweepHeader h;
+    std::string err;
     for (const auto &b : blocks) {
-        std::vector<dgq::TileProgram> progs;
-        dgq::PlanStats st;
-        dgq::SweepHeader h;
-        std::string err;
+        progs.clear();
         if (!dgq::encodeBlock(b, numBits, numBits, W, pool, h, progs, &st, &err)) return 1e30;
-        const double mem = st.sweeps * amps * 32.0 / cm.hbmBytesPerSec;
-        const double comp = amps * st.flopsPerAmp / cm.fp64FlopsPerSec +
-                            (st.phases + st.sweeps) * amps * 32.0 / cm.smemBytesPerSec;
-        t += std::max(mem, comp);
     }
-    return t;
+    return st.sweeps * (amps * cm.sweepSecondsPerAmp + cm.launchSeconds) + st.phases * amps * cm.phaseSecondsPerAmp;
 }
 
 int chooseTileBits(QuregState &s) {
@@ -223,18 +228,41 @@ int chooseTileBits(QuregState &s) {
                                                                                     : dgq::kMaxTileBitsF64,
                             s.numBits);
     const int lo = dgq::kMinTileBits;
+    s.planLookahead = -1;
     if (s.tileBitsSetting > 0) return std::max(lo, std::min(hi, s.tileBitsSetting));
     if (const char *env = getenv("DGQ_TILE_BITS")) {
         const int w = atoi(env);
         if (w > 0) return std::max(lo, std::min(hi, w));
     }
+    // candidates: every width, with and without lookahead block selection on
+    // registers large enough for it; planned concurrently, one host thread each
+    struct Cand {
+        int W, lookahead;
+        double t;
+    };
+    std::vector<Cand> cands;
+    for (int W = lo; W <= hi; W++) {
+        if (dgq::lookaheadBySize(s.numBits)) cands.push_back({W, 1, 1e300});
+        cands.push_back({W, 0, 1e300});
+    }
+    {
+        std::vector<std::thread> th;
+        for (size_t i = 1; i < cands.size(); i++)
+            th.emplace_back([&, i]() {
+                cands[i].t = predictPlanSeconds(s.pending, s.numBits, cands[i].W, s.pool, cands[i].lookahead);
+            });
+        cands[0].t = predictPlanSeconds(s.pending, s.numBits, cands[0].W, s.pool, cands[0].lookahead);
+        for (auto &x : th) x.join();
+    }
+    // the smaller tile, then lookahead, on ties
     int best = std::min(hi, 12);
     double bestT = 1e300;
-    for (int W = lo; W <= hi; W++) {
-        const double t = predictPlanSeconds(s.pending, s.numBits, W, s.pool);
-        if (t < bestT * 0.98) {  // prefer the smaller tile on near ties
-            bestT = t;
-            best = W;
+    s.planLookahead = -1;
+    for (const Cand &c : cands) {
+        if (c.t < bestT) {
+            bestT = c.t;
+            best = c.W;
+            s.planLookahead = c.lookahead;
         }
     }
     return best;
@@ -278,7 +306,14 @@ int jitMinBits() {
 namespace dgq {
 
 int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err,
-                  bool paired) {
+                  bool paired, const std::function<bool(size_t)> &emit) {
+    // hands the programs from index `from` on to emit
+    auto emitted = [&](size_t from) -> bool {
+        if (!emit) return true;
+        for (size_t i = from; i < out.size(); i++)
+            if (!emit(i)) return false;
+        return true;
+    };
     out.clear();
     SweepHeader h;
     if (s.initPending) {
@@ -298,17 +333,28 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
     std::vector<Gate> seg;
     auto planSegment = [&]() -> int {
         if (seg.empty()) return 0;
-        bool complete = true;
-        std::vector<BlockPlan> blocks =
-            planBlocks(seg, s.numBits, W, &complete, paired ? kCoalescedBits + 1 : kCoalescedBits);
+        int code = 0;
+        const bool complete = planBlocksEach(seg, s.numBits, W, paired ? kCoalescedBits + 1 : kCoalescedBits,
+                                             [&](BlockPlan &b) {
+                                                 SweepHeader hb = first ? h : SweepHeader();
+                                                 const size_t from = out.size();
+                                                 if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st,
+                                                                  &err, paired)) {
+                                                     code = E_UNSUPPORTED;
+                                                     return false;
+                                                 }
+                                                 first = false;
+                                                 if (!emitted(from)) {
+                                                     code = -1;
+                                                     return false;
+                                                 }
+                                                 return true;
+                                             },
+                                             s.planLookahead);
+        if (code) return code;
         if (!complete) {
             err = "a multi-qubit gate is wider than the register tile";
             return E_UNSUPPORTED;
-        }
-        for (const auto &b : blocks) {
-            SweepHeader hb = first ? h : SweepHeader();
-            if (!encodeBlock(b, s.numBits, s.numQubits, W, s.pool, hb, out, &st, &err, paired)) return E_UNSUPPORTED;
-            first = false;
         }
         seg.clear();
         return 0;
@@ -325,6 +371,7 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
             encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
             st.sweeps++;
             first = false;
+            if (!emitted(out.size() - 1)) return -1;
         }
         TileProgram &p = out.emplace_back();
         std::memset(&p, 0, sizeof(p));
@@ -345,6 +392,7 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         }
         st.sweeps++;
         st.flopsPerAmp += 8.0 * (double) (1 << g.numMultiTargets);
+        if (!emitted(out.size() - 1)) return -1;
     }
     if (int code = planSegment()) return code;
     if (s.single && !out.empty() && out.back().denseTcOff) {
@@ -354,11 +402,13 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         out.emplace_back();
         encodeHeaderOnly(s.numBits, s.numQubits, W, SweepHeader(), out.back(), paired);
         st.sweeps++;
+        if (!emitted(out.size() - 1)) return -1;
     }
     if (out.empty()) {
         out.emplace_back();
         encodeHeaderOnly(s.numBits, s.numQubits, W, h, out.back(), paired);
         st.sweeps = 1;
+        if (!emitted(0)) return -1;
     }
     return 0;
 }
@@ -390,73 +440,155 @@ std::atomic<int> g_tensorCores{1};
 // circuit structure should not wait for NVRTC).
 std::atomic<int> g_specPolicy{0};
 
-// dgq_sweepSource (specialise = false) plans as for specialisation but
-// compiles nothing.
-bool planPending(QuregState &s, const char *func, bool specialise = true) {
+bool launchProgram(QuregState &s, size_t i, const char *func) {
+    const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+    const dgq::TileProgram &p = s.planned[i];
+    if (p.renormOut && !cudaOk(cudaMemsetAsync(p.normOut, 0, sizeof(double), s.stream), func)) return false;
+    cudaError_t e;
+    if (p.denseK) {
+        dgq::DenseArgs da;
+        if (!dgq::denseArgs(s.numBits, p.denseK, p.denseTargets, da))
+            return raise(E_UNSUPPORTED, func, "dense unitary does not fit the register");
+        if (p.renormIn) da.normIn = p.normIn;
+        if (p.renormOut) da.normOut = p.normOut;
+        if (p.denseTcOff && g_tensorCores.load()) {
+            static uint32_t *errWord = dgq::tcDenseErrorWord();
+            e = dgq::launchTcDense((float2 *) s.dState, da, reinterpret_cast<const float *>(s.dDense + p.denseTcOff),
+                                   errWord, s.stream);
+        } else {
+            e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
+        }
+    } else {
+        e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, p, s.stream)
+               : dgq::launchTile(s.dState, s.single, s.plannedTileBits, p, s.stream);
+    }
+    if (!cudaOk(e, func)) return false;
+    g_launches++;
+    return true;
+}
+
+// Programs from index `from` on.
+bool launchPlanned(QuregState &s, const char *func, size_t from = 0) {
+    for (size_t i = from; i < s.planned.size(); i++)
+        if (!launchProgram(s, i, func)) return false;
+    return true;
+}
+
+// complex64: sweep i < last adds up the norm of its output when i % 4 == 3
+// or it is the sweep before the last, and the next sweep divides by its
+// square root, so FP32 rounding drift never accumulates over more than 4
+// sweeps and the final sweep starts from a renormalised state (the
+// per-sweep global factor already restores the scale of the factored
+// rotations exactly). `last` is unknown (SIZE_MAX) while a sweep two or
+// more places before the last is launched as the plan is being made.
+void setRenorm(QuregState &s, size_t i, size_t last, int &event) {
+    dgq::TileProgram &p = s.planned[i];
+    p.isSingle = s.single ? 1 : 0;
+    if (!s.single) return;
+    const dgq::TileProgram *prev = i > 0 ? &s.planned[i - 1] : nullptr;
+    if (prev && prev->renormOut) {
+        p.renormIn = 1;
+        p.normIn = prev->normOut;
+    }
+    if (i < last && (i % 4 == 3 || i + 1 == last)) {
+        p.renormOut = 1;
+        p.normOut = s.dNorm + (event++ & 1);
+    }
+}
+
+// Plans the pending gates into s.planned (dgq_sweepSource: specialise =
+// false plans as for specialisation but compiles nothing). With launch, the
+// sweeps are issued too: when their kernels are compiled already, each sweep
+// is launched as soon as the two after it are planned, so planning the rest
+// of the circuit overlaps the GPU's work on the first sweeps.
+bool planPending(QuregState &s, const char *func, bool specialise = true, bool launch = false) {
     s.planned.clear();
+    s.plannedFns.clear();
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
     const bool jitOn = dgq::jitEnabled();
     const bool wantJit = jitOn && (!specialise || s.numBits >= jitMinBits());
-    dgq::PlanStats st;
-    std::string err;
-    int W = 0;
-    bool paired = false;
-    // interpret: the programs are for the interpreting kernel (W <= 12, unpaired)
-    auto build = [&](bool pairedForm, bool interpret) -> int {
-        paired = pairedForm;
-        W = paired ? pairedTileBits(s) : chooseTileBits(s);
-        if (interpret) W = std::min(W, dgq::kMaxTileBitsF64);
-        st = dgq::PlanStats();
-        err.clear();
-        int code = dgq::buildPrograms(s, W, s.planned, st, err, paired);
-        if (code) return code;
-        // complex64: every 4th sweep (counting back from the last) adds up the
-        // norm of its output and the next sweep divides by its square root, so
-        // FP32 rounding drift never accumulates over more than 4 sweeps and the
-        // final sweep starts from a renormalised state (the per-sweep global
-        // factor already restores the scale of the factored rotations exactly)
-        const int last = (int) s.planned.size() - 1;
-        int event = 0;
-        for (int i = 0; i <= last; i++) {
-            dgq::TileProgram &p = s.planned[(size_t) i];
-            p.isSingle = s.single ? 1 : 0;
-            if (!s.single) continue;
-            const dgq::TileProgram *prev = i > 0 ? &s.planned[(size_t) i - 1] : nullptr;
-            if (prev && prev->renormOut) {
-                p.renormIn = 1;
-                p.normIn = prev->normOut;
-            }
-            if (i < last && (last - 1 - i) % 4 == 0) {
-                p.renormOut = 1;
-                p.normOut = s.dNorm + (event++ & 1);
-            }
-        }
-        return 0;
-    };
     // complex64 registers of >= 2^10 amplitudes run the paired form (two
     // amplitudes per slot, packed FP32 arithmetic) when specialised, unless a
     // sweep cannot be encoded that way (a multi-qubit unitary on address bit 0)
     const bool pairedOk = wantJit && s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
+    // policy 1 still compiles for registers of >= 2^28 amplitudes: their
+    // sweeps take longer than a compile, and the interpreting kernel runs
+    // them 2-3x slower than specialised code
+    const bool cachedOnly = specialise && wantJit && g_specPolicy.load() == 1 && s.numBits < 28;
+    // launching while planning: not when the plan may be redone (policy 1
+    // falls back to the interpreting kernel when a kernel is missing; the
+    // paired form falls back on a multi-qubit unitary on bit 0) nor with dense
+    // sweeps, whose matrices are uploaded once the plan is complete
+    bool stream = launch && specialise && !cachedOnly;
+    for (const Gate &g : s.pending)
+        if (g.type == dgq::OP_MULTI_UNITARY && (g.numMultiTargets > dgq::kRegBits || (pairedOk && (g.targetMask & 1ULL))))
+            stream = false;
+    dgq::PlanStats st;
+    std::string err;
+    int W = 0;
+    bool paired = false;
+    size_t launched = 0;  // programs issued while planning
+    bool missing = false;  // a sweep's kernel is not loaded: the rest wait for the plan
+    int event = 0;
+    int reused = 0;
+    std::function<bool(size_t)> emit;
+    if (stream) {
+        emit = [&](size_t k) -> bool {
+            while (!missing && launched + 2 <= k) {
+                const size_t i = launched;
+                setRenorm(s, i, SIZE_MAX, event);
+                CUfunction fn = nullptr;
+                if (wantJit && !s.planned[i].denseK) {
+                    fn = dgq::jitFindLoaded(dgq::generateSweepSource(s.planned[i], W));
+                    if (!fn) {
+                        missing = true;
+                        break;
+                    }
+                    reused++;
+                }
+                s.plannedFns.resize(i + 1, nullptr);
+                s.plannedFns[i] = fn;
+                s.plannedTileBits = W;
+                if (!launchProgram(s, i, func)) return false;
+                launched++;
+            }
+            return true;
+        };
+    }
+    // interpret: the programs are for the interpreting kernel (W <= 12, unpaired)
+    auto build = [&](bool pairedForm, bool interpret) -> int {
+        paired = pairedForm;
+        s.planLookahead = -1;
+        W = paired ? pairedTileBits(s) : chooseTileBits(s);
+        if (interpret) W = std::min(W, dgq::kMaxTileBitsF64);
+        st = dgq::PlanStats();
+        err.clear();
+        event = 0;
+        int code = dgq::buildPrograms(s, W, s.planned, st, err, paired, emit);
+        if (code) return code;
+        const size_t last = s.planned.size() - 1;
+        for (size_t i = launched; i <= last; i++) setRenorm(s, i, last, event);
+        return 0;
+    };
     int code = build(pairedOk, !wantJit);
-    if (code && pairedOk) code = build(false, !wantJit);
+    if (code == -1) return false;
+    if (code && pairedOk && launched == 0) code = build(false, !wantJit);
+    if (code == -1) return false;
     if (code) return raise(code, func, err.c_str());
-    s.plannedFns.assign(s.planned.size(), nullptr);
+    s.plannedFns.resize(s.planned.size(), nullptr);
     s.stats.jitCompiled = 0;
-    s.stats.jitReused = 0;
+    s.stats.jitReused = reused;
     s.stats.jitMillis = 0.0;
     if (specialise && wantJit) {
         std::vector<std::string> sources;
         std::vector<size_t> which;  // tile programs (dense sweeps have their own kernel)
-        for (size_t i = 0; i < s.planned.size(); i++)
+        for (size_t i = launched; i < s.planned.size(); i++)
             if (!s.planned[i].denseK) {
                 sources.push_back(dgq::generateSweepSource(s.planned[i], W));
                 which.push_back(i);
             }
-        // policy 1 still compiles for registers of >= 2^28 amplitudes: their
-        // sweeps take longer than a compile, and the interpreting kernel runs
-        // them 2-3x slower than specialised code
-        if (g_specPolicy.load() == 1 && s.numBits < 28 && !dgq::jitAllReady(sources)) {
+        if (cachedOnly && !dgq::jitAllReady(sources)) {
             dgq::jitCompileInBackground(sources);
             if (paired || W > dgq::kMaxTileBitsF64) {
                 // the interpreting kernel runs unpaired programs of W <= 12
@@ -471,7 +603,7 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
             if (!dgq::jitGetKernels(sources, fns, &js, &jerr)) return raise(E_UNSUPPORTED, func, jerr.c_str());
             for (size_t k = 0; k < which.size(); k++) s.plannedFns[which[k]] = fns[k];
             s.stats.jitCompiled = js.compiled;
-            s.stats.jitReused = js.reused;
+            s.stats.jitReused += js.reused;
             s.stats.jitMillis = js.compileMillis;
         }
     }
@@ -497,39 +629,9 @@ bool planPending(QuregState &s, const char *func, bool specialise = true) {
     s.stats.flopsPerAmp = st.flopsPerAmp;
     s.stats.launchBytes = (int64_t) st.sweeps * (int64_t) sizeof(dgq::TileProgram);
     s.stats.planMillis = nowMillis() - t0;
+    s.stats.streamedSweeps = (int) launched;
     dgq::consumePending(s);
-    return true;
-}
-
-bool launchPlanned(QuregState &s, const char *func) {
-    for (size_t i = 0; i < s.planned.size(); i++) {
-        const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
-        if (s.planned[i].renormOut &&
-            !cudaOk(cudaMemsetAsync(s.planned[i].normOut, 0, sizeof(double), s.stream), func))
-            return false;
-        const dgq::TileProgram &p = s.planned[i];
-        cudaError_t e;
-        if (p.denseK) {
-            dgq::DenseArgs da;
-            if (!dgq::denseArgs(s.numBits, p.denseK, p.denseTargets, da))
-                return raise(E_UNSUPPORTED, func, "dense unitary does not fit the register");
-            if (p.renormIn) da.normIn = p.normIn;
-            if (p.renormOut) da.normOut = p.normOut;
-            if (p.denseTcOff && g_tensorCores.load()) {
-                static uint32_t *errWord = dgq::tcDenseErrorWord();
-                e = dgq::launchTcDense((float2 *) s.dState, da,
-                                       reinterpret_cast<const float *>(s.dDense + p.denseTcOff), errWord, s.stream);
-            } else {
-                e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
-            }
-        } else {
-            e = fn ? dgq::launchJitSweep(fn, s.dState, s.plannedTileBits, p, s.stream)
-                   : dgq::launchTile(s.dState, s.single, s.plannedTileBits, p, s.stream);
-        }
-        if (!cudaOk(e, func)) return false;
-        g_launches++;
-    }
-    return true;
+    return !launch || launchPlanned(s, func, launched);
 }
 
 // Register memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
@@ -584,8 +686,7 @@ void freeOn(void *ptr, cudaStream_t st) {
 
 bool flush(QuregState &s, const char *func) {
     if (s.pending.empty() && !s.initPending) return true;
-    if (!planPending(s, func)) return false;
-    return launchPlanned(s, func);
+    return planPending(s, func, true, true);
 }
 
 bool ensureProbs(QuregState &s, const char *func) {

@@ -120,6 +120,7 @@ bool GateDag::tryMerge(int top, const Gate &g) {
 }
 
 void GateDag::unlinkDeleted(int idx) {
+    flatValid_ = false;
     Node &d = nodes_[(size_t) idx];
     for (auto &st : qubitStack_) {
         if (!st.empty() && st.back() == idx) st.pop_back();
@@ -139,6 +140,7 @@ void GateDag::unlinkDeleted(int idx) {
 }
 
 void GateDag::add(const Gate &g) {
+    flatValid_ = false;
     const u64 barrier = g.targetMask | g.controlMask;
     const int idx = (int) nodes_.size();
     Node node;
@@ -220,6 +222,7 @@ std::vector<Gate> GateDag::takeBlock(int budget, u64 &mask, size_t maxGates) {
     }
     // rebuild the residual DAG (with merging, as a fresh DAG)
     nodes_.clear();
+    flatValid_ = false;
     front_.clear();
     alive_ = 0;
     for (auto &st : qubitStack_) st.clear();
@@ -227,72 +230,61 @@ std::vector<Gate> GateDag::takeBlock(int budget, u64 &mask, size_t maxGates) {
     return taken;
 }
 
-// Insertion order is a topological order, so one forward pass decides
-// which gates are reachable inside `allowed`.
-size_t GateDag::countAllowed(u64 allowed) const {
-    std::vector<char> ok(nodes_.size(), 0);
-    size_t count = 0;
-    for (size_t i = 0; i < nodes_.size(); i++) {
-        const Node &nd = nodes_[i];
+void GateDag::refreshFlat() const {
+    if (flatValid_) return;
+    flatTouch_.clear();
+    flatCost_.clear();
+    for (const Node &nd : nodes_) {
         if (!nd.alive) continue;
-        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
-        if (cost & ~allowed) continue;
-        bool all = true;
-        for (int p : nd.prev)
-            if (!ok[(size_t) p]) {
-                all = false;
-                break;
-            }
-        if (!all) continue;
-        ok[i] = 1;
+        flatTouch_.push_back(nd.g.targetMask | nd.g.controlMask);
+        flatCost_.push_back(isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask);
+    }
+    flatValid_ = true;
+}
+
+// Insertion order is a topological order, so one forward pass decides
+// which gates are reachable inside `allowed`: a gate held back holds back
+// every later gate on its qubits.
+size_t GateDag::countAllowed(u64 allowed) const {
+    refreshFlat();
+    const size_t n = flatTouch_.size();
+    const u64 *touch = flatTouch_.data(), *cost = flatCost_.data();
+    const u64 all = numQubits_ >= 64 ? ~0ULL : ((1ULL << numQubits_) - 1);
+    u64 blocked = 0;
+    size_t count = 0;
+    for (size_t i = 0; i < n && blocked != all; i++) {
+        if ((touch[i] & blocked) || (cost[i] & ~allowed)) {
+            blocked |= touch[i];
+            continue;
+        }
         count++;
     }
     return count;
 }
 
 u64 GateDag::frontierTargets(u64 allowed) const {
-    std::vector<char> ok(nodes_.size(), 0);
     u64 frontier = 0;
-    for (size_t i = 0; i < nodes_.size(); i++) {
-        const Node &nd = nodes_[i];
-        if (!nd.alive) continue;
-        bool all = true;
-        for (int p : nd.prev)
-            if (!ok[(size_t) p]) {
-                all = false;
-                break;
-            }
-        if (!all) continue;
-        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
-        if (cost & ~allowed) {
-            frontier |= cost & ~allowed;
-            continue;
-        }
-        ok[i] = 1;
-    }
+    for (u64 m : frontierSets(allowed)) frontier |= m;
     return frontier;
 }
 
 std::vector<u64> GateDag::frontierSets(u64 allowed) const {
-    std::vector<char> ok(nodes_.size(), 0);
+    refreshFlat();
+    const size_t n = flatTouch_.size();
+    const u64 *touch = flatTouch_.data(), *cost = flatCost_.data();
+    const u64 all = numQubits_ >= 64 ? ~0ULL : ((1ULL << numQubits_) - 1);
     std::vector<u64> sets;
-    for (size_t i = 0; i < nodes_.size(); i++) {
-        const Node &nd = nodes_[i];
-        if (!nd.alive) continue;
-        bool all = true;
-        for (int p : nd.prev)
-            if (!ok[(size_t) p]) {
-                all = false;
-                break;
-            }
-        if (!all) continue;
-        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
-        const u64 missing = cost & ~allowed;
-        if (missing) {
-            if (std::find(sets.begin(), sets.end(), missing) == sets.end()) sets.push_back(missing);
+    u64 blocked = 0;
+    for (size_t i = 0; i < n && blocked != all; i++) {
+        if (touch[i] & blocked) {
+            blocked |= touch[i];
             continue;
         }
-        ok[i] = 1;
+        const u64 missing = cost[i] & ~allowed;
+        if (missing) {
+            if (std::find(sets.begin(), sets.end(), missing) == sets.end()) sets.push_back(missing);
+            blocked |= touch[i];
+        }
     }
     return sets;
 }
@@ -315,6 +307,7 @@ std::vector<Gate> GateDag::takeAllowed(u64 allowed) {
         }
     }
     nodes_.clear();
+    flatValid_ = false;
     front_.clear();
     alive_ = 0;
     for (auto &st : qubitStack_) st.clear();

@@ -50,6 +50,15 @@ public:
     std::vector<u64> frontierSets(u64 allowed) const;
 
 private:
+    // Alive nodes in insertion order as (touched qubits, non-diagonal
+    // targets): a gate can run inside `allowed` exactly when its targets lie
+    // in `allowed` and no earlier gate on one of its qubits was held back,
+    // because its predecessors are the latest earlier gates on its qubits.
+    // The scans below run over this flat copy, rebuilt after a change.
+    void refreshFlat() const;
+    mutable bool flatValid_ = false;
+    mutable std::vector<u64> flatTouch_, flatCost_;
+
     struct Node {
         Gate g;
         std::vector<int> prev;

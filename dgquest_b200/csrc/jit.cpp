@@ -684,6 +684,8 @@ void backgroundWorker() {
 
 }  // namespace
 
+CUfunction jitFindLoaded(const std::string &source) { return cacheFind(source); }
+
 bool jitAllReady(const std::vector<std::string> &sources) {
     for (const auto &src : sources)
         if (!cacheFind(src) && !cubinFind(src, nullptr)) return false;

@@ -32,6 +32,10 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
 
 cudaError_t launchJitSweep(CUfunction fn, void *st, int tileBits, const TileProgram &prog, cudaStream_t s);
 
+// The loaded kernel of `source`, or nullptr when it is not loaded yet
+// (compiles nothing).
+CUfunction jitFindLoaded(const std::string &source);
+
 // Whether every source is compiled already (loaded, or compiled in the
 // background and waiting to be loaded).
 bool jitAllReady(const std::vector<std::string> &sources);

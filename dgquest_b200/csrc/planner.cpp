@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 
 #include "dag.h"
 
@@ -22,15 +23,37 @@ static const double kRsqrt2 = 0.7071067811865475244008443621;
 // Grows `mask` up to `budget` bits: each step adds the missing target bits
 // of one runnable-next gate, choosing the addition that lets the most gates
 // run (ties: fewer new bits; with preferHigh, bits above the 5 coalesced).
-static void growMask(const GateDag &dag, u64 &mask, int budget, bool preferHigh) {
+// Registers of at least this many address bits choose tile bits with a
+// one-step lookahead unless told otherwise (measured on the 30-qubit random
+// circuit of depth 20: 17 instead of 19 sweeps for 3x the planning time).
+static int lookaheadMinBits() {
+    static const int v = []() {
+        const char *e = getenv("DGQ_PLAN_LOOKAHEAD_BITS");
+        return e ? atoi(e) : 24;
+    }();
+    return v;
+}
+
+bool lookaheadBySize(int numBits) { return numBits >= lookaheadMinBits(); }
+
+// lookahead: score each candidate addition by the best follow-up addition too
+static void growMask(const GateDag &dag, u64 &mask, int budget, bool preferHigh, bool lookahead = false) {
     const u64 low = (1ULL << kCoalescedBits) - 1;
+    const bool look = lookahead;
     while (popcount64(mask) < budget) {
         const std::vector<u64> cands = dag.frontierSets(mask);
         size_t best = 0;
         u64 bestAdd = 0;
         for (u64 add : cands) {
             if (popcount64(mask | add) > budget) continue;
-            const size_t c = dag.countAllowed(mask | add);
+            size_t c = dag.countAllowed(mask | add);
+            if (look && popcount64(mask | add) < budget) {
+                // score a candidate by the best follow-up addition as well
+                for (u64 add2 : dag.frontierSets(mask | add)) {
+                    if (popcount64(mask | add | add2) > budget) continue;
+                    c = std::max(c, dag.countAllowed(mask | add | add2));
+                }
+            }
             bool better = c > best;
             if (!better && c == best && bestAdd) {
                 const int pa = popcount64(add), pb = popcount64(bestAdd);
@@ -49,29 +72,39 @@ static void growMask(const GateDag &dag, u64 &mask, int budget, bool preferHigh)
     }
 }
 
-std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete,
-                                  int seedBits) {
-    std::vector<BlockPlan> blocks;
-    if (complete) *complete = true;
+bool planBlocksEach(const std::vector<Gate> &gates, int numBits, int tileBits, int seedBits,
+                    const std::function<bool(BlockPlan &)> &onBlock, int lookahead) {
     GateDag dag(numBits, true);
     for (const Gate &g : gates) dag.add(g);
     const u64 seed = (1ULL << seedBits) - 1;
     const u64 all = numBits >= 64 ? ~0ULL : ((1ULL << numBits) - 1);
+    const bool look = lookahead < 0 ? lookaheadBySize(numBits) : lookahead > 0;
     while (!dag.empty()) {
         BlockPlan b;
         u64 mask = seed & all;
-        growMask(dag, mask, tileBits, false);
+        growMask(dag, mask, tileBits, false, look);
         // pad to tileBits with the lowest unused bits above the seed
         for (int bit = seedBits; popcount64(mask) < tileBits && bit < numBits; bit++) mask |= 1ULL << bit;
         b.tileMask = mask & all;
         b.gates = dag.takeAllowed(b.tileMask);
-        if (b.gates.empty()) {
-            // only a gate wider than the tile is left: not plannable here
-            if (complete) *complete = false;
-            break;
-        }
-        blocks.push_back(std::move(b));
+        // only a gate wider than the tile is left: not plannable here
+        if (b.gates.empty()) return false;
+        if (!onBlock(b)) return true;
     }
+    return true;
+}
+
+std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete,
+                                  int seedBits, int lookahead) {
+    std::vector<BlockPlan> blocks;
+    const bool ok = planBlocksEach(
+        gates, numBits, tileBits, seedBits,
+        [&](BlockPlan &b) {
+            blocks.push_back(std::move(b));
+            return true;
+        },
+        lookahead);
+    if (complete) *complete = ok;
     return blocks;
 }
 

@@ -11,6 +11,7 @@
 // QuEST_gpu_kernel.cu:504-509), then phases of 4 register bits.
 #pragma once
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -42,8 +43,20 @@ struct MatrixPool {
 // seedBits: the lowest address bits every tile holds (5: the coalesced bits
 // of complex128 tiles; 6 for the complex64 paired form, whose tile-local
 // bit 0 is the pair inside a slot and bits 1..5 the coalesced slot bits).
+// lookahead: 1 scores each candidate addition of tile bits by the best
+// follow-up addition as well (fewer sweeps on deep circuits, 3x the
+// planning time), 0 does not, -1 uses it for registers of >= 24 address bits
+// (DGQ_PLAN_LOOKAHEAD_BITS overrides the 24).
 std::vector<BlockPlan> planBlocks(const std::vector<Gate> &gates, int numBits, int tileBits, bool *complete = nullptr,
-                                  int seedBits = kCoalescedBits);
+                                  int seedBits = kCoalescedBits, int lookahead = -1);
+// The same blocks, handed to `onBlock` one at a time as they are chosen
+// (a caller can encode and launch a sweep while the next one is planned);
+// stops early when onBlock returns false. Returns false when gates are left
+// that no tile can hold.
+bool planBlocksEach(const std::vector<Gate> &gates, int numBits, int tileBits, int seedBits,
+                    const std::function<bool(BlockPlan &)> &onBlock, int lookahead = -1);
+// Whether lookahead -1 means lookahead for a register of numBits bits.
+bool lookaheadBySize(int numBits);
 
 // Encodes one block. The gate list may not fit one TileProgram; then the
 // block is emitted as several programs over the same tile (each one more

@@ -2,6 +2,8 @@
 // register API in api.cpp and the batched form in batch_host.cpp).
 #pragma once
 
+#include <functional>
+
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -49,6 +51,7 @@ struct QuregState {
     double *dNorm = nullptr;  // complex64 renormalisation: two running sums of |a|^2
 
     int tileBitsSetting = 0;  // 0 = cost model
+    int planLookahead = -1;   // block selection with lookahead (the cost model's choice; -1: by size)
     bool allowPaired = true;  // complex64: the paired form where it applies
     // matrices of the planned dense sweeps (host copy and device buffer)
     std::vector<double> denseHost;
@@ -67,8 +70,11 @@ namespace dgq {
 // error code with err set. The register is not changed.
 // paired: the complex64 paired form (TileProgram::paired; W counts the
 // in-slot bit, so W - 1 tile bits index 16-byte slots).
+// emit (if set) is called with the index of each program as soon as it is
+// complete, in order; when it returns false, planning stops and
+// buildPrograms returns -1 (the callback has reported its own error).
 int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats &st, std::string &err,
-                  bool paired = false);
+                  bool paired = false, const std::function<bool(size_t)> &emit = nullptr);
 // Drops the pending work that buildPrograms planned (after it has been
 // launched or kept for launching).
 void consumePending(QuregState &s);

@@ -63,6 +63,8 @@ class PlanStats(Structure):
         ("jitReused", ctypes.c_int32),
         ("jitMillis", c_double),
         ("launchBytes", ctypes.c_int64),
+        ("streamedSweeps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

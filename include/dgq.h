@@ -56,6 +56,9 @@ typedef struct dgq_plan_stats {
     double jitMillis;      /* time spent specialising kernels */
     int64_t launchBytes;   /* host->device bytes per launch of the whole plan
                               (one sweep program per kernel parameter block) */
+    int32_t streamedSweeps; /* sweeps launched while the rest of the plan was
+                               still being made (their kernels were compiled) */
+    int32_t reserved;
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
