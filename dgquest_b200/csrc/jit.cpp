@@ -113,6 +113,85 @@ void emitOp(std::ostringstream &o, const KOp &op) {
     }
 }
 
+// Thread/CTA condition of an op (its controls among non-register bits), or "".
+std::string thrCond(const KOp &op) {
+    if (!op.thrCtl) return std::string();
+    std::ostringstream cond;
+    bool any = false;
+    if (op.ctrlLoc) {
+        cond << "((loc & " << op.ctrlLoc << "u) == " << op.ctrlLoc << "u)";
+        any = true;
+    }
+    if (op.ctrlCta) {
+        cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+        any = true;
+    }
+    return any ? cond.str() : std::string("true");
+}
+
+// Selector of KC_Z2T / KC_PH1T (a thread or CTA bit) as a condition.
+std::string selCond(const KOp &op) {
+    std::ostringstream sel;
+    bool any = false;
+    if (op.selLoc) {
+        sel << "((loc & " << op.selLoc << "u) != 0u)";
+        any = true;
+    }
+    if (op.selCta >= 0) {
+        sel << (any ? " || " : "") << "(((cta >> " << (int) op.selCta << ") & 1u) != 0u)";
+        any = true;
+    }
+    return any ? sel.str() : std::string("false");
+}
+
+// 1: the op multiplies every amplitude of a thread by one phase factor
+// that depends only on thread and CTA bits; 2: by -1 or +-i (integer sign
+// flips when applied on their own); 0: neither.
+int scalarKind(const KOp &op) {
+    const bool allAmps = op.ctrlReg == 0;
+    if (op.code == KC_PH1T) return 1;
+    if ((op.code == KC_Z2T || op.code == KC_PH) || ((op.code == KC_Z2T + 1 || op.code == KC_PH + 1) && allAmps))
+        return 1;
+    if ((op.code == KC_NEG || op.code == KC_MULI || op.code == KC_MULNI) ||
+        ((op.code == KC_NEG + 1 || op.code == KC_MULI + 1 || op.code == KC_MULNI + 1) && allAmps))
+        return 2;
+    return 0;
+}
+
+// A scalar op (scalarKind != 0) multiplied into the phase factor acc_.
+void emitScalarAcc(std::ostringstream &o, const KOp &op) {
+    const std::string tc = thrCond(op);
+    const std::string on = tc.empty() ? std::string("true") : tc;
+    const int off = op.coef;
+    const int base = op.code & ~1;
+    if (op.code == KC_PH1T) {
+        o << "    dgq::jAccPhase(acc_, (" << on << ") && (" << selCond(op) << "), prog.coef[" << off << "], prog.coef["
+          << off + 1 << "]);\n";
+    } else if (base == KC_Z2T) {
+        o << "    dgq::jAccPhase(acc_, " << on << ", prog.coef[" << off << "], (" << selCond(op) << ") ? prog.coef["
+          << off + 1 << "] : -prog.coef[" << off + 1 << "]);\n";
+    } else if (base == KC_PH) {
+        o << "    dgq::jAccPhase(acc_, " << on << ", prog.coef[" << off << "], prog.coef[" << off + 1 << "]);\n";
+    } else if (base == KC_NEG) {
+        o << "    dgq::jAccNeg(acc_, " << on << ");\n";
+    } else {
+        o << "    dgq::jAccMulI(acc_, " << on << ", " << (base == KC_MULI ? "1.0" : "-1.0") << ");\n";
+    }
+}
+
+// Whether the scalar ops of ops [b, e) go into one factor: when at least two
+// of them are phase factors, or one is and there are sign flips besides
+// (a lone sign flip stays on the integer pipe).
+bool foldScalars(const TileProgram &prog, int b, int e) {
+    int nPhase = 0, nSign = 0;
+    for (int k = b; k < e; k++) {
+        const int kind = scalarKind(prog.ops[k]);
+        nPhase += kind == 1;
+        nSign += kind == 2;
+    }
+    return nPhase >= 2 || (nPhase >= 1 && nSign >= 1);
+}
+
 }  // namespace
 
 namespace {
@@ -494,6 +573,17 @@ std::string generateSweepSource(const TileProgram &prog, int W) {
     const int np = prog.numPhases;
     const bool firstDirect = np > 0 && prog.phases[0].direct;
     const bool lastDirect = np > 0 && prog.phases[np - 1].direct;
+    // the sweep's global factor (and renormalisation) is one number for all
+    // amplitudes: it starts the factor of the first phase with a scalar
+    // phase op instead of costing a multiply of its own at the end
+    int gPhase = -1;
+    if (prog.renormIn || prog.hasGlobal)
+        for (int p = 0; p < np && gPhase < 0; p++)
+            for (int k = prog.phases[p].opBegin; k < prog.phases[p].opEnd; k++)
+                if (scalarKind(prog.ops[k]) == 1) {
+                    gPhase = p;
+                    break;
+                }
     if (firstDirect) {
         emitDirectAddressing(o, prog.phases[0], W, "gIn", "rbIn");
         o << "    dgq::jLoadDirect<" << prog.initKind << ", " << (prog.hasRestrict ? "true" : "false")
@@ -512,7 +602,21 @@ std::string generateSweepSource(const TileProgram &prog, int W) {
         o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc);\n    (void) sb;\n";
         if (readSmem)
             for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = sm[sb ^ " << ph.regOff[j] << "u];\n";
-        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOp(o, prog.ops[k]);
+        const bool fold = p == gPhase || foldScalars(prog, ph.opBegin, ph.opEnd);
+        if (p == gPhase && prog.renormIn)
+            o << "    double2 acc_;\n    { const double sc_ = rsqrt(*prog.normIn); acc_ = make_double2(prog.globalRe * "
+                 "sc_, prog.globalIm * sc_); }\n";
+        else if (p == gPhase)
+            o << "    double2 acc_ = make_double2(prog.globalRe, prog.globalIm);\n";
+        else if (fold)
+            o << "    double2 acc_ = make_double2(1.0, 0.0);\n";
+        for (int k = ph.opBegin; k < ph.opEnd; k++) {
+            if (fold && scalarKind(prog.ops[k]))
+                emitScalarAcc(o, prog.ops[k]);
+            else
+                emitOp(o, prog.ops[k]);
+        }
+        if (fold) o << "    dgq::jGlobal(a, acc_.x, acc_.y);\n";
         if (writeSmem) {
             for (int j = 0; j < kRegs; j++) o << "    sm[sb ^ " << ph.regOff[j] << "u] = a[" << j << "];\n";
             o << "    __syncthreads();\n";
@@ -520,7 +624,9 @@ std::string generateSweepSource(const TileProgram &prog, int W) {
         o << "  }\n";
     }
     if (np > 0 && !lastDirect) o << "    dgq::jFromSmem<W>(sm, tid, a);\n";
-    if (prog.renormIn) {
+    if (gPhase >= 0) {
+        // applied with the factor of phase gPhase
+    } else if (prog.renormIn) {
         o << "    { const double sc_ = rsqrt(*prog.normIn); dgq::jGlobal(a, prog.globalRe * sc_, prog.globalIm * sc_); }\n";
     } else if (prog.hasGlobal) {
         o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";

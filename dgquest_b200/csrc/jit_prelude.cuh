@@ -149,6 +149,27 @@ __device__ __forceinline__ void jPhaseMul(V &x, double csd, double snd) {
     x.y = fma(cs, x.y, u);
 }
 
+// Per-thread factor of a register phase: diagonal ops whose condition
+// involves only thread and CTA bits multiply every amplitude the thread
+// holds by the same number, and they commute with every other op of the
+// phase (those act on register bits); they are multiplied into one factor
+// (a few scalar operations each) that is applied once, at the end.
+__device__ __forceinline__ void jAccPhase(double2 &acc, bool on, double cs, double sn) {
+    const double r = fma(acc.x, cs, -acc.y * sn), i = fma(acc.x, sn, acc.y * cs);
+    acc.x = on ? r : acc.x;
+    acc.y = on ? i : acc.y;
+}
+__device__ __forceinline__ void jAccNeg(double2 &acc, bool on) {
+    acc.x = on ? -acc.x : acc.x;
+    acc.y = on ? -acc.y : acc.y;
+}
+// times i (sign +1) or -i (sign -1)
+__device__ __forceinline__ void jAccMulI(double2 &acc, bool on, double sign) {
+    const double r = -sign * acc.y, i = sign * acc.x;
+    acc.x = on ? r : acc.x;
+    acc.y = on ? i : acc.y;
+}
+
 // diag(c - i s, c + i s) selected by register bit K
 template <int K, bool CTRL, uint32_t CR, class V>
 __device__ __forceinline__ void jZ2R(V (&a)[kRegs], const double *c) {
