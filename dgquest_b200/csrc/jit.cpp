@@ -455,6 +455,54 @@ void emitOpPaired(std::ostringstream &o, const KOp &op) {
     }
 }
 
+// scalarKind for the paired form: conditions on address bit 0 (the pair
+// inside a slot) select one amplitude of each slot, so those ops are not
+// scalars of the thread.
+int scalarKindPaired(const KOp &op) {
+    if ((op.ctrlLoc & 1u) != 0 || op.ctrlReg != 0) return 0;
+    switch (op.kind) {
+        case KOP_PH: return 1;
+        case KOP_Z2: return op.code >= KC_Z2T && op.selLoc != 1u ? 1 : 0;
+        case KOP_PH1: return op.code >= KC_PH1T && op.selLoc != 1u ? 1 : 0;
+        case KOP_NEG:
+        case KOP_MULI:
+        case KOP_MULNI: return 2;
+        default: return 0;
+    }
+}
+
+void emitScalarAccPaired(std::ostringstream &o, const KOp &op) {
+    const unsigned cl = op.ctrlLoc & ~1u;
+    std::ostringstream cond;
+    bool any = false;
+    if (cl) {
+        cond << "((loc & " << cl << "u) == " << cl << "u)";
+        any = true;
+    }
+    if (op.ctrlCta) {
+        cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+        any = true;
+    }
+    const std::string on = any ? cond.str() : std::string("true");
+    const int off = op.coef;
+    switch (op.kind) {
+        case KOP_PH:
+            o << "    dgq::jAccPhase(acc_, " << on << ", prog.coef[" << off << "], prog.coef[" << off + 1 << "]);\n";
+            break;
+        case KOP_Z2:
+            o << "    dgq::jAccPhase(acc_, " << on << ", prog.coef[" << off << "], (" << selExpr(op) << ") ? prog.coef["
+              << off + 1 << "] : -prog.coef[" << off + 1 << "]);\n";
+            break;
+        case KOP_PH1:
+            o << "    dgq::jAccPhase(acc_, (" << on << ") && (" << selExpr(op) << "), prog.coef[" << off
+              << "], prog.coef[" << off + 1 << "]);\n";
+            break;
+        case KOP_NEG: o << "    dgq::jAccNeg(acc_, " << on << ");\n"; break;
+        case KOP_MULI: o << "    dgq::jAccMulI(acc_, " << on << ", 1.0);\n"; break;
+        default: o << "    dgq::jAccMulI(acc_, " << on << ", -1.0);\n"; break;
+    }
+}
+
 // Address bit of tile-local bit l of a paired tile (bits 0..5 are address bits 0..5).
 std::string pairedAddr(int l) {
     if (l < kCoalescedBits) return std::to_string(l);
@@ -494,6 +542,18 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
                             (prog.hasRestrict ? "true" : "false") + ">(prog, g_, R[j], I[j]);";
     const bool needFix = prog.initKind != INIT_NONE || prog.hasRestrict;
     const std::string load = prog.initKind == INIT_NONE ? "dgq::pLoadSlot(st, g_, R[j], I[j]); " : "";
+    // scalar diagonal ops fold into one factor per phase, as in the unpaired
+    // form; the sweep's global factor starts the first such phase's factor
+    int nPhaseOps[kMaxPhases] = {0}, nSignOps[kMaxPhases] = {0};
+    int gPhase = -1;
+    for (int p = 0; p < np; p++) {
+        for (int k = prog.phases[p].opBegin; k < prog.phases[p].opEnd; k++) {
+            const int kind = scalarKindPaired(prog.ops[k]);
+            nPhaseOps[p] += kind == 1;
+            nSignOps[p] += kind == 2;
+        }
+        if (gPhase < 0 && nPhaseOps[p] > 0 && (prog.renormIn || prog.hasGlobal)) gPhase = p;
+    }
     if (firstDirect) {
         emitPairedLayoutAddressing(o, prog.phases[0], W, "gIn", "rbIn");
         o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) { const uint64_t g_ = dgq::jIdx(gIn, rbIn, j); "
@@ -522,7 +582,21 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
             for (int j = 0; j < kRegs; j++)
                 o << "    { const float4 q_ = sm[sb ^ " << ph.regOff[j] << "u]; R[" << j << "] = make_float2(q_.x, q_.y); I["
                   << j << "] = make_float2(q_.z, q_.w); }\n";
-        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOpPaired(o, prog.ops[k]);
+        const bool fold = p == gPhase || nPhaseOps[p] >= 2 || (nPhaseOps[p] >= 1 && nSignOps[p] >= 1);
+        if (p == gPhase && prog.renormIn)
+            o << "    double2 acc_;\n    { const double sc_ = rsqrt(*prog.normIn); acc_ = make_double2(prog.globalRe * "
+                 "sc_, prog.globalIm * sc_); }\n";
+        else if (p == gPhase)
+            o << "    double2 acc_ = make_double2(prog.globalRe, prog.globalIm);\n";
+        else if (fold)
+            o << "    double2 acc_ = make_double2(1.0, 0.0);\n";
+        for (int k = ph.opBegin; k < ph.opEnd; k++) {
+            if (fold && scalarKindPaired(prog.ops[k]))
+                emitScalarAccPaired(o, prog.ops[k]);
+            else
+                emitOpPaired(o, prog.ops[k]);
+        }
+        if (fold) o << "    dgq::pGlobal(R, I, acc_.x, acc_.y);\n";
         if (writeSmem) {
             for (int j = 0; j < kRegs; j++)
                 o << "    sm[sb ^ " << ph.regOff[j] << "u] = make_float4(R[" << j << "].x, R[" << j << "].y, I[" << j
@@ -534,7 +608,9 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
     if (np > 0 && !lastDirect)
         o << "#pragma unroll\n    for (int j = 0; j < dgq::kRegs; j++) { const float4 q_ = sm[dgq::swz(tid + T * "
              "(uint32_t) j)]; R[j] = make_float2(q_.x, q_.y); I[j] = make_float2(q_.z, q_.w); }\n";
-    if (prog.renormIn) {
+    if (gPhase >= 0) {
+        // applied with the factor of phase gPhase
+    } else if (prog.renormIn) {
         o << "    { const double sc_ = rsqrt(*prog.normIn); dgq::pGlobal(R, I, prog.globalRe * sc_, prog.globalIm * sc_); }\n";
     } else if (prog.hasGlobal) {
         o << "    dgq::pGlobal(R, I, prog.globalRe, prog.globalIm);\n";
