@@ -497,9 +497,42 @@ def run_precision_form(args, world):
     out["max_abs_err_sampled"] = err
     out["amplitudes_sampled"] = len(idx)
     out["speedup_complex64"] = out["complex128"]["ms_per_circuit"] / out["complex64"]["ms_per_circuit"]
-    out["arithmetic"] = "complex64 paired form (packed FP32 SIMT); the tensor-core dense-block GEMM is not built"
-    for q in (q64, q32):
+    out["arithmetic"] = "complex64 paired form (packed FP32 SIMT register phases)"
+    Q.destroyQureg(q32, env)
+    if not args.no_tc_blocks:
+        # the same circuit fused into dense 6-qubit blocks, each a 3xTF32 GEMM
+        # on the tensor cores (one warm-up and one timed run: seconds each)
+        q = Q.dgq_createQuregF32(n, env)
+        Q.dgq_setDenseFusion(q, 6)
+        Q.initZeroState(q)
+        Q.apply_circuit(q, ops)
+        Q.dgq_planPending(q)
+        st = Q.plan_stats(q)
+        stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+        Q.dgq_launchPlanned(q)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Q.dgq_launchPlanned(q)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        err = 0.0
+        for i in idx:
+            a = Q.getAmp(q64, int(i))
+            b = Q.getAmp(q, int(i))
+            err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
+        out["complex64_tensor_core_blocks"] = {
+            "ms_per_circuit": ms, "dense_blocks": int(st.denseBlocks), "sweeps": st.sweeps,
+            "tensor_tflops_algorithmic": st.denseBlocks * (1 << n) * 1536.0 / (ms / 1e3) / 1e12,
+            "fidelity": Q.calcFidelity(q64, q), "max_abs_err_sampled": err,
+            "device_errors": int(Q.dgq_getDeviceErrors()),
+            "vs_paired_form": ms / out["complex64"]["ms_per_circuit"],
+            "note": "gates fused into dense 6-qubit unitaries (FP64 composition), one tcgen05 kind::tf32 "
+                    "3xTF32 GEMM sweep per block; warm-up 1, timed 1"}
         Q.destroyQureg(q, env)
+    Q.destroyQureg(q64, env)
     Q.destroyQuESTEnv(env)
     return out
 
@@ -613,6 +646,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
+    ap.add_argument("--no-tc-blocks", action="store_true", help="skip the dense-block tensor-core run of the grid circuit")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--dense-qubits", type=int, default=30)
     ap.add_argument("--batch-circuits", type=int, default=4096)

@@ -27,6 +27,7 @@
 #include "QuEST.h"
 #include "dgq.h"
 #include "dag.h"
+#include "fuse.h"
 #include "ir.h"
 #include "jit.h"
 #include "kernels.h"
@@ -506,6 +507,9 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     s.plannedFns.clear();
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
+    int denseBlocks = 0;
+    if (s.denseFusion > 0 && s.numBits >= s.denseFusion + 2 && !s.pending.empty())
+        s.pending = dgq::fuseDenseBlocks(s.pending, s.numBits, s.denseFusion, s.pool, &denseBlocks);
     const bool jitOn = dgq::jitEnabled();
     const bool wantJit = jitOn && (!specialise || s.numBits >= jitMinBits());
     // complex64 registers of >= 2^10 amplitudes run the paired form (two
@@ -630,6 +634,7 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     s.stats.launchBytes = (int64_t) st.sweeps * (int64_t) sizeof(dgq::TileProgram);
     s.stats.planMillis = nowMillis() - t0;
     s.stats.streamedSweeps = (int) launched;
+    s.stats.denseBlocks = denseBlocks;
     dgq::consumePending(s);
     return !launch || launchPlanned(s, func, launched);
 }
@@ -1598,6 +1603,18 @@ int dgq_getPlanStats(Qureg q, dgq_plan_stats *out) {
     return 0;
 }
 
+int dgq_setDenseFusion(Qureg q, int qubits) {
+    if (!vQureg(q, __func__)) return -1;
+    if (qubits != 0 && (qubits < dgq::kMinDenseTargets || qubits > dgq::kMaxDenseTargets)) {
+        raise(E_INVALID_ARGUMENT, __func__, "dense fusion takes 0 or 5..7 qubits");
+        return -1;
+    }
+    QuregState &s = *stateOf(q);
+    const int prev = s.denseFusion;
+    s.denseFusion = qubits;
+    return prev;
+}
+
 int dgq_planPending(Qureg q) {
     if (!vQureg(q, __func__)) return -1;
     return planPending(*stateOf(q), __func__) ? 0 : -1;
@@ -1703,6 +1720,46 @@ int dgq_measureFp64Peak(double *tflops) {
     const double fmas = (double) blocks * 256.0 * iters * 16.0 * 8.0;
     *tflops = 2.0 * fmas / (best * 1e-3) / 1e12;
     return 0;
+}
+
+int dgq_fuseApplyHost(int numQubits, int K, int count, const int32_t *types, const uint64_t *targetMasks,
+                      const uint64_t *controlMasks, const double *operands, double *re, double *im) {
+    if (numQubits < 1 || numQubits > 20 || K < 1 || K > 7 || K > numQubits || count < 0 ||
+        (count > 0 && (!types || !targetMasks || !controlMasks || !operands)) || !re || !im) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
+    }
+    const u64 all = (1ULL << numQubits) - 1;
+    std::vector<Gate> gates;
+    for (int i = 0; i < count; i++) {
+        Gate g;
+        g.type = (dgq::GateType) types[i];
+        g.targetMask = targetMasks[i];
+        g.controlMask = controlMasks[i];
+        if ((g.targetMask | g.controlMask) & ~all || g.type < 0 || g.type >= dgq::OP_MULTI_UNITARY) {
+            raise(E_INVALID_ARGUMENT, __func__);
+            return -1;
+        }
+        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
+        gates.push_back(g);
+    }
+    dgq::MatrixPool pool;
+    int blocks = 0;
+    const std::vector<Gate> fused = dgq::fuseDenseBlocks(gates, numQubits, K, pool, &blocks);
+    const size_t D = (size_t) 1 << numQubits;
+    std::vector<double> v(2 * D);
+    for (size_t i = 0; i < D; i++) {
+        v[2 * i] = re[i];
+        v[2 * i + 1] = im[i];
+    }
+    int local[64];
+    for (int b = 0; b < 64; b++) local[b] = b < numQubits ? b : -1;
+    for (const Gate &g : fused) dgq::applyGateLocal(g, pool, local, numQubits, v.data(), 1);
+    for (size_t i = 0; i < D; i++) {
+        re[i] = v[2 * i];
+        im[i] = v[2 * i + 1];
+    }
+    return blocks;
 }
 
 int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,

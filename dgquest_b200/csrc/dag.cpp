@@ -236,8 +236,9 @@ void GateDag::refreshFlat() const {
     flatCost_.clear();
     for (const Node &nd : nodes_) {
         if (!nd.alive) continue;
-        flatTouch_.push_back(nd.g.targetMask | nd.g.controlMask);
-        flatCost_.push_back(isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask);
+        const u64 touch = nd.g.targetMask | nd.g.controlMask;
+        flatTouch_.push_back(touch);
+        flatCost_.push_back(touchCost_ ? touch : isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask);
     }
     flatValid_ = true;
 }
@@ -295,7 +296,8 @@ std::vector<Gate> GateDag::takeAllowed(u64 allowed) {
     for (size_t i = 0; i < nodes_.size(); i++) {
         const Node &nd = nodes_[i];
         if (!nd.alive) continue;
-        const u64 cost = isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
+        const u64 cost = touchCost_ ? (nd.g.targetMask | nd.g.controlMask)
+                                    : isDiagonalType(nd.g.type) ? 0 : nd.g.targetMask;
         bool all = (cost & ~allowed) == 0;
         for (int p : nd.prev)
             if (all && !ok[(size_t) p]) all = false;

@@ -48,6 +48,14 @@ public:
     u64 frontierTargets(u64 allowed) const;
     // The distinct sets of missing target bits of those next gates.
     std::vector<u64> frontierSets(u64 allowed) const;
+    // With touchCost, the queries above count every qubit a gate touches
+    // (targets, controls, diagonal gates' qubits) instead of its
+    // non-diagonal targets: the selection of gates that a dense unitary on
+    // the allowed qubits can absorb.
+    void setTouchCost(bool on) {
+        touchCost_ = on;
+        flatValid_ = false;
+    }
 
 private:
     // Alive nodes in insertion order as (touched qubits, non-diagonal
@@ -57,6 +65,7 @@ private:
     // The scans below run over this flat copy, rebuilt after a change.
     void refreshFlat() const;
     mutable bool flatValid_ = false;
+    bool touchCost_ = false;
     mutable std::vector<u64> flatTouch_, flatCost_;
 
     struct Node {

@@ -53,6 +53,7 @@ struct QuregState {
     int tileBitsSetting = 0;  // 0 = cost model
     int planLookahead = -1;   // block selection with lookahead (the cost model's choice; -1: by size)
     bool allowPaired = true;  // complex64: the paired form where it applies
+    int denseFusion = 0;      // > 0: gates fused into dense blocks of this many qubits
     // matrices of the planned dense sweeps (host copy and device buffer)
     std::vector<double> denseHost;
     double *dDense = nullptr;

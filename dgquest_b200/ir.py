@@ -63,6 +63,26 @@ def ops_to_ir(ops, n):
             np.array(opnd, dtype=np.float64).reshape(-1, 8))
 
 
+def fuse_apply_host(n, k, types, tm, cm, opnd, amps):
+    """The dense-block form on the host: gates (IR arrays) fused into blocks
+    of k qubits and applied in FP64 to amps (length 2^n); returns (new amps,
+    number of blocks)."""
+    from .quest import _check, _library
+    P = ctypes.POINTER
+    re = np.ascontiguousarray(amps.real, dtype=np.float64).copy()
+    im = np.ascontiguousarray(amps.imag, dtype=np.float64).copy()
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    tm = np.ascontiguousarray(tm, dtype=np.uint64)
+    cm = np.ascontiguousarray(cm, dtype=np.uint64)
+    o = np.ascontiguousarray(opnd, dtype=np.float64).reshape(-1, 8)
+    nb = _library().dgq_fuseApplyHost(n, k, len(t), t.ctypes.data_as(P(ctypes.c_int32)),
+                                      tm.ctypes.data_as(P(ctypes.c_uint64)), cm.ctypes.data_as(P(ctypes.c_uint64)),
+                                      o.ctypes.data_as(P(ctypes.c_double)), re.ctypes.data_as(P(ctypes.c_double)),
+                                      im.ctypes.data_as(P(ctypes.c_double)))
+    _check()
+    return re + 1j * im, nb
+
+
 def plan(ops, n, tile_bits=0, want_merged=False):
     """Host-only plan statistics of an op list (no GPU needed)."""
     from .quest import PlanStats, _check, _library

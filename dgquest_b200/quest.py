@@ -64,7 +64,7 @@ class PlanStats(Structure):
         ("jitMillis", c_double),
         ("launchBytes", ctypes.c_int64),
         ("streamedSweeps", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("denseBlocks", ctypes.c_int32),
     ]
 
 
@@ -172,6 +172,7 @@ _SIGS = {
     "dgq_setTileBits": (I, [Q, I]),
     "dgq_getPlanStats": (I, [Q, P(PlanStats)]),
     "dgq_planPending": (I, [Q]),
+    "dgq_setDenseFusion": (I, [Q, I]),
     "dgq_launchPlanned": (I, [Q]),
     "dgq_sync": (I, [Q]),
     "dgq_getStream": (c_void_p, [Q]),
@@ -190,6 +191,7 @@ _SIGS = {
     "dgq_setTensorCores": (I, [I]),
     "dgq_getDeviceErrors": (I, []),
     "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
+    "dgq_fuseApplyHost": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(D), P(D)]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),
     "dgq_applyCircuit": (I, [Q, c_void_p, I, P(I)]),

@@ -58,9 +58,19 @@ typedef struct dgq_plan_stats {
                               (one sweep program per kernel parameter block) */
     int32_t streamedSweeps; /* sweeps launched while the rest of the plan was
                                still being made (their kernels were compiled) */
-    int32_t reserved;
+    int32_t denseBlocks;    /* dense fused blocks (dgq_setDenseFusion) */
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
+
+/* Dense-block form. qubits = 5, 6 or 7: the register's gates are fused into
+ * dense unitaries on that many qubits (dgQuEST's greedy block rule,
+ * DAG.cpp:219-259, with every qubit a gate touches counted), composed in
+ * FP64 on the host and applied one per sweep as a complex GEMM over the
+ * state: on the tensor cores (tcgen05, 3xTF32) for complex64 registers and
+ * 6 qubits, the SIMT dense kernel otherwise. 0 (the default) runs gates in
+ * register-phase sweeps. Registers of fewer than qubits + 2 address bits
+ * are not fused. Returns the previous setting, or -1 on a bad argument. */
+int dgq_setDenseFusion(Qureg qureg, int qubits);
 
 /* Plans the pending gates (and pending initialisation / collapse) into
  * sweep programs and keeps them; dgq_launchPlanned launches them on the
@@ -120,6 +130,15 @@ int dgq_calcProbOfAllZeroNoAlloc(const void *deviceState, int numBits, double *d
 int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
                   const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
                   int32_t *numMerged);
+
+/* Host-only view of the dense-block form (no GPU call): fuses the gates
+ * (dgq_planGates encoding) into dense blocks of K = 1..7 qubits as
+ * dgq_setDenseFusion does and applies the fused gates in FP64 on the host
+ * to the state (re, im) of numQubits <= 20 qubits, in place. Returns the
+ * number of dense blocks, or -1 on a bad argument. For tests of the
+ * fusion; the product path applies the blocks on the GPU. */
+int dgq_fuseApplyHost(int numQubits, int K, int count, const int32_t *types, const uint64_t *targetMasks,
+                      const uint64_t *controlMasks, const double *operands, double *re, double *im);
 
 /* Registers with at least minBits address bits run runtime-specialised
  * sweep kernels (default 22, or DGQ_JIT_MIN_BITS; DGQ_JIT=0 disables
