@@ -492,6 +492,7 @@ __device__ __forceinline__ float2 b2(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
 // sign flip on the integer pipe (standalone negations: CZ, S, Y), leaving
 // the FMA pipe to the arithmetic
 __device__ __forceinline__ float2 flip2(float2 a) {
@@ -654,16 +655,13 @@ __device__ __forceinline__ void pRY1(PRegs &R, PRegs &I, const double *c) {
         niy = fma2(t, ix, iy);
     })
 }
-// [[u, -1], [1, u]] = [[0, -1], [1, 0]] [[1, u], [-u, 1]]: the second
-// factor takes one FMA per component, the first is a swap and a sign flip
-// on the integer pipe (a packed negation would take the FMA pipe)
 template <int K>
 __device__ __forceinline__ void pRY2(PRegs &R, PRegs &I, const double *c) {
     constexpr bool HI = false;
-    const float2 u = b2((float) c[0]), nu = b2(-(float) c[0]);
+    const float2 u = b2((float) c[0]);
     DGQP_PAIR_LOOP(K, false, 0u, {
-        nrx = flip2(fma2(nu, rx, ry));
-        nix = flip2(fma2(nu, ix, iy));
+        nrx = fma2(u, rx, neg2(ry));
+        nix = fma2(u, ix, neg2(iy));
         nry = fma2(u, ry, rx);
         niy = fma2(u, iy, ix);
     })
@@ -679,17 +677,15 @@ __device__ __forceinline__ void pRX1(PRegs &R, PRegs &I, const double *c) {
         niy = fma2(nt, rx, iy);
     })
 }
-// [[u, -i], [-i, u]] = [[0, -i], [-i, 0]] [[1, i u], [i u, 1]], the first
-// factor again a swap and sign flips
 template <int K>
 __device__ __forceinline__ void pRX2(PRegs &R, PRegs &I, const double *c) {
     constexpr bool HI = false;
-    const float2 u = b2((float) c[0]), nu = b2(-(float) c[0]);
+    const float2 u = b2((float) c[0]);
     DGQP_PAIR_LOOP(K, false, 0u, {
         nrx = fma2(u, rx, iy);
-        nix = flip2(fma2(nu, ix, ry));
+        nix = fma2(u, ix, neg2(ry));
         nry = fma2(u, ry, ix);
-        niy = flip2(fma2(nu, iy, rx));
+        niy = fma2(u, iy, neg2(rx));
     })
 }
 template <int K>
