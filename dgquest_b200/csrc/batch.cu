@@ -94,7 +94,7 @@ __device__ __noinline__ void addExpectationSums(double tot, const double (&rs)[4
 
 // One tile of one sweep, run by the first 2^(W-4) threads of the CTA; h is
 // the sweep header staged in shared memory.
-template <class V, int W>
+template <class V, int W, bool DENSE>
 __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSweep &h, V *__restrict__ st, uint32_t tile,
                                           V *sm, double *zs) {
     constexpr uint32_t T = 1u << (W - kRegBits);
@@ -163,7 +163,7 @@ __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSwee
                 const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(ops + o));
                 KOp op;
                 memcpy(&op, &raw, sizeof(op));
-                applyOp(op, coef, a, loc, tile);
+                applyOp<V, DENSE>(op, coef, a, loc, tile);
             }
 #pragma unroll
             for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];
@@ -210,7 +210,7 @@ __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSwee
 // Sweeps [w0, w1) of one register on tile `tile` (one sweep for a tile
 // item, all of them for a whole-register item); each header is copied to
 // shared memory first, so the phase loop holds no header registers.
-template <class V, int W>
+template <class V, int W, bool DENSE>
 __device__ __forceinline__ void runSweeps(const BatchArgs &args, const BatchCircuit &C, uint32_t w0, uint32_t w1,
                                        uint32_t tile, V *sm, BatchSweep *hs) {
     constexpr uint32_t T = 1u << (W - kRegBits);
@@ -220,11 +220,14 @@ __device__ __forceinline__ void runSweeps(const BatchArgs &args, const BatchCirc
         uint32_t *dst = reinterpret_cast<uint32_t *>(hs);
         for (uint32_t i = threadIdx.x; i < sizeof(BatchSweep) / 4; i += T) dst[i] = __ldg(src + i);
         groupBarrier(T);
-        sweepTile<V, W>(args, *hs, st, tile, sm, w + 1 == C.numSweeps ? args.zsum + C.zOff : nullptr);
+        sweepTile<V, W, DENSE>(args, *hs, st, tile, sm, w + 1 == C.numSweeps ? args.zsum + C.zOff : nullptr);
     }
 }
 
-template <class V>
+// DENSE: the batch's programs hold dense ops (multi-qubit unitaries of up to
+// 4 targets inside a register phase); without them the kernel is compiled
+// without that case (FP64: no spills instead of 1.3 KB of spill stores).
+template <class V, bool DENSE>
 __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
     batchKernel(const __grid_constant__ BatchArgs args) {
     extern __shared__ __align__(16) unsigned char smRaw[];
@@ -265,10 +268,10 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
             const uint32_t w0 = s == kBatchWhole ? 0u : s, w1 = s == kBatchWhole ? C.numSweeps : s + 1;
             const uint32_t tile = s == kBatchWhole ? 0u : t;
             switch (C.tileBits) {
-                case 9: runSweeps<V, 9>(args, C, w0, w1, tile, sm, &sHead); break;
-                case 10: runSweeps<V, 10>(args, C, w0, w1, tile, sm, &sHead); break;
-                case 11: runSweeps<V, 11>(args, C, w0, w1, tile, sm, &sHead); break;
-                default: runSweeps<V, 12>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 9: runSweeps<V, 9, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 10: runSweeps<V, 10, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 11: runSweeps<V, 11, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
+                default: runSweeps<V, 12, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
             }
             __threadfence();
         }
@@ -281,30 +284,41 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
 // by ctasPerSmV (called before any launch is recorded), so that launches
 // recorded in graphs stay valid whatever tile width later batches use.
 template <class V>
-cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, cudaStream_t s) {
+cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, bool dense, cudaStream_t s) {
     const size_t smem = sizeof(V) << maxTileBits;
-    batchKernel<V><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
+    if (dense)
+        batchKernel<V, true><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
+    else
+        batchKernel<V, false><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
     return cudaGetLastError();
 }
 
+// Both forms have the same launch bounds and shared memory; the occupancy
+// is the smaller of the two.
 template <class V>
 int ctasPerSmV(int maxTileBits) {
     const size_t smem = sizeof(V) << maxTileBits;
-    if (cudaFuncSetAttribute(batchKernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int) (sizeof(V) << kBatchMaxTileBits)) != cudaSuccess)
+    const int smemMax = (int) (sizeof(V) << kBatchMaxTileBits);
+    if (cudaFuncSetAttribute(batchKernel<V, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(batchKernel<V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax) !=
+            cudaSuccess)
         return 0;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<V>, 1 << (maxTileBits - kRegBits), smem) !=
-        cudaSuccess)
+    int n0 = 0, n1 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, batchKernel<V, true>, 1 << (maxTileBits - kRegBits),
+                                                      smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, batchKernel<V, false>, 1 << (maxTileBits - kRegBits),
+                                                      smem) != cudaSuccess)
         return 0;
-    return n;
+    return n0 < n1 ? n0 : n1;
 }
 
 }  // namespace
 
-cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, cudaStream_t s) {
+cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, bool dense, cudaStream_t s) {
     if (maxTileBits < kMinTileBits || maxTileBits > kBatchMaxTileBits || grid < 1) return cudaErrorInvalidValue;
-    return single ? launchBatchV<float2>(a, maxTileBits, grid, s) : launchBatchV<double2>(a, maxTileBits, grid, s);
+    return single ? launchBatchV<float2>(a, maxTileBits, grid, dense, s)
+                  : launchBatchV<double2>(a, maxTileBits, grid, dense, s);
 }
 
 int batchCtasPerSm(bool single, int maxTileBits) {

@@ -99,7 +99,10 @@ __device__ __forceinline__ void denseApply(V (&a)[kRegs], uint32_t ctrlReg, cons
     }
 }
 
-template <class V>
+// DENSE = false drops the dense-op case (KOP_DENSE), whose 2^k-amplitude
+// temporaries otherwise set the register budget of every other op: callers
+// that know their programs hold no dense op compile without it.
+template <class V, bool DENSE = true>
 __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a)[kRegs], uint32_t loc,
                                         uint32_t cta) {
     typedef typename Real<V>::T R;
@@ -251,11 +254,13 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             break;
         }
         case KOP_DENSE:
-            switch (op.k) {
-                case 1: denseApply<1>(a, cr, c); break;
-                case 2: denseApply<2>(a, cr, c); break;
-                case 3: denseApply<3>(a, cr, c); break;
-                default: denseApply<4>(a, cr, c); break;
+            if constexpr (DENSE) {
+                switch (op.k) {
+                    case 1: denseApply<1>(a, cr, c); break;
+                    case 2: denseApply<2>(a, cr, c); break;
+                    case 3: denseApply<3>(a, cr, c); break;
+                    default: denseApply<4>(a, cr, c); break;
+                }
             }
             break;
         default:

@@ -191,3 +191,43 @@ def test_apply_circuit_matches_replay(quest, env):
         Q.apply_circuit(q2, bad)
     Q.destroyQureg(q1, env)
     Q.destroyQureg(q2, env)
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_batch_with_register_phase_dense_ops(quest, env, single):
+    """Registers with multi-qubit unitaries of 2..4 targets (dense ops inside
+    a register phase) select the batch kernel form that handles them."""
+    Q = quest
+    sizes = [10, 13, 12, 15]
+    gen = np.random.default_rng(21)
+    regs, refs = [], []
+    for i, n in enumerate(sizes):
+        targs = [[1, 4], [0, 7, 3], [11, 2, 5, 8], [14, 6, 9][: 2 + i % 2]][i]
+        u = C.random_unitary(gen, 1 << len(targs))
+        pre = C.hea(n, 3, C.config_seed(4, 40 + i))
+        q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+        Q.initZeroState(q)
+        C.replay(q, pre)
+        m = Q.matrixN(u)
+        Q.multiQubitUnitary(q, Q.int_array(targs), len(targs), m)
+        Q.destroyComplexMatrixN(m)
+        post = C.hea(n, 2, C.config_seed(4, 50 + i))
+        C.replay(q, post)
+        o = oracle.Oracle(n)
+        o.apply(pre)
+        o.multi_qubit_unitary(targs, u)
+        o.apply(post)
+        refs.append(o.amps())
+        o.close()
+        regs.append(q)
+    b = Q.Batch(regs)
+    b.launch()
+    b.wait()
+    for q, ref in zip(regs, refs):
+        amps = Q.state_vector(q)
+        if single:
+            assert abs(np.vdot(ref, amps)) ** 2 >= 1 - 1e-6
+        else:
+            assert np.abs(amps - ref).max() <= 1e-12
+    b.close()
+    destroy(Q, env, regs)
