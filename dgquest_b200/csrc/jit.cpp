@@ -245,91 +245,6 @@ static int ctasPerSm(int T, bool single) {
     return 65536 / (regs * T) > 0 ? 65536 / (regs * T) : 1;
 }
 
-// Off by default: measured on B200 at 30 qubits, one 256-thread CTA per SM
-// with two 64 KiB buffers hides less latency than two plain CTAs per SM
-// (204 ms vs 158 ms per circuit). DGQ_JIT_PERSISTENT=1 selects it.
-bool jitPersistent() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("DGQ_JIT_PERSISTENT");
-        v = (e && e[0] == '1') ? 1 : 0;
-    }
-    return v == 1;
-}
-
-// Persistent form: each CTA walks tiles blockIdx.x, +gridDim.x, ...; the
-// next tile streams into the other of two shared buffers by cp.async while
-// the current one runs its phases, so HBM reads overlap the FP64 work.
-static std::string generatePersistent(const TileProgram &prog, int W) {
-    const int T = 1 << (W - kRegBits);
-    const int np = prog.numPhases;
-    const bool load = prog.initKind == INIT_NONE;
-    const bool lastDirect = prog.phases[np - 1].direct;
-    std::ostringstream o;
-    o << "#include \"jit_prelude.cuh\"\n";
-    o << "typedef " << (prog.isSingle ? "float2" : "double2") << " V;\n";
-    o << "extern \"C\" __global__ void __launch_bounds__(" << T << ", 1"
-      << ") dgq_sweep(V *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
-    o << "    constexpr int W = " << W << ";\n";
-    o << "    constexpr uint32_t TILE = 1u << W;\n";
-    o << "    extern __shared__ V smAll[];\n";
-    o << "    const uint32_t tid = threadIdx.x;\n";
-    o << "    const uint32_t numTiles = 1u << (prog.numBits - W);\n";
-    o << "    V a[dgq::kRegs];\n";
-    if (load) o << "    if (blockIdx.x < numTiles) dgq::jPrefetch<W>(st, prog, tid, blockIdx.x, smAll);\n    dgq::jCpAsyncCommit();\n";
-    o << "    int it = 0;\n";
-    o << "    for (uint32_t cta = blockIdx.x; cta < numTiles; cta += gridDim.x, it++) {\n";
-    o << "    V *sm = smAll + (size_t) (it & 1) * TILE;\n";
-    o << "    __syncthreads();\n";
-    if (load) {
-        o << "    { const uint32_t nx = cta + gridDim.x; if (nx < numTiles) dgq::jPrefetch<W>(st, prog, tid, nx, smAll + "
-             "(size_t) ((it + 1) & 1) * TILE); }\n";
-        o << "    dgq::jCpAsyncCommit();\n    dgq::jCpAsyncWait1();\n    __syncthreads();\n";
-    }
-    for (int p = 0; p < np; p++) {
-        const KPhase &ph = prog.phases[p];
-        const bool writeSmem = !(p == np - 1 && lastDirect);
-        o << "  {\n    const uint32_t loc = 0u";
-        for (int i = 0; i < W - kRegBits; i++) o << " | (((tid >> " << i << ") & 1u) << " << (int) ph.thrPos[i] << ")";
-        o << ";\n    (void) loc;\n    const uint32_t sb = dgq::swz(loc);\n";
-        if (p == 0 && !load) {
-            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "].x = 0; a[" << j << "].y = 0;\n";
-        } else {
-            for (int j = 0; j < kRegs; j++) o << "    a[" << j << "] = sm[sb ^ " << ph.regOff[j] << "u];\n";
-        }
-        if (p == 0 && (!load || prog.hasRestrict)) {
-            emitLayoutAddressing(o, ph, W, "cta", "gF", "rbF");
-            o << "    dgq::jFixup<" << prog.initKind << ", " << (prog.hasRestrict ? "true" : "false")
-              << ">(prog, gF, rbF, a);\n";
-        }
-        for (int k = ph.opBegin; k < ph.opEnd; k++) emitOp(o, prog.ops[k]);
-        if (writeSmem) {
-            for (int j = 0; j < kRegs; j++) o << "    sm[sb ^ " << ph.regOff[j] << "u] = a[" << j << "];\n";
-            o << "    __syncthreads();\n";
-        }
-        o << "  }\n";
-    }
-    if (!lastDirect) o << "    dgq::jFromSmem<W>(sm, tid, a);\n";
-    if (prog.hasGlobal) o << "    dgq::jGlobal(a, prog.globalRe, prog.globalIm);\n";
-    if (lastDirect) {
-        o << "  {\n";
-        emitDirectAddressing(o, prog.phases[np - 1], W, "gOut", "rbOut");
-        o << "    dgq::jStoreDirect(st, gOut, rbOut, a);\n  }\n";
-    } else {
-        o << "    dgq::jStore<W>(st, prog, tid, cta, a);\n";
-    }
-    o << "    }\n";
-    if (load) o << "    dgq::jCpAsyncWait0();\n";
-    o << "}\n";
-    return o.str();
-}
-
-// The persistent form has no renormalisation step, so complex64 programs
-// (which renormalise every sweep) always use the plain form.
-static bool usePersistent(const TileProgram &prog) {
-    return jitPersistent() && prog.numPhases > 0 && !prog.renormIn && !prog.renormOut && !prog.paired;
-}
-
 // ------------------------------------------------------------ paired form
 namespace {
 
@@ -531,7 +446,7 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
     o << "    constexpr int W = " << W << ";\n";
     o << "    constexpr uint32_t T = " << T << "u;\n";
     o << "    extern __shared__ float4 sm[];\n";
-    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x;\n";
+    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x + prog.ctaOffset;\n";
     o << "    (void) cta;\n    (void) T;\n";
     o << "    float2 R[dgq::kRegs], I[dgq::kRegs];\n";
     o << "    const uint64_t cb = dgq::jCtaBase(prog, cta, W);\n";
@@ -633,7 +548,6 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
 std::string generateSweepSource(const TileProgram &prog, int W) {
     if (prog.denseK) return std::string();  // dense sweeps run the dense kernel (dense.cu)
     if (prog.paired) return generatePairedSource(prog, W);
-    if (usePersistent(prog)) return generatePersistent(prog, W);
     const int T = 1 << (W - kRegBits);
     const int minBlocks = ctasPerSm(T, prog.isSingle != 0);
     std::ostringstream o;
@@ -643,7 +557,7 @@ std::string generateSweepSource(const TileProgram &prog, int W) {
       << ") dgq_sweep(V *__restrict__ st, const __grid_constant__ dgq::TileProgram prog) {\n";
     o << "    constexpr int W = " << W << ";\n";
     o << "    extern __shared__ V sm[];\n";
-    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x;\n";
+    o << "    const uint32_t tid = threadIdx.x, cta = blockIdx.x + prog.ctaOffset;\n";
     o << "    (void) cta;\n";
     o << "    V a[dgq::kRegs];\n";
     const int np = prog.numPhases;
@@ -1002,22 +916,13 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
 cudaError_t launchJitSweep(CUfunction fn, void *st, int W, const TileProgram &prog, cudaStream_t s) {
     // paired complex64 form: 16 slots of 2 amplitudes per thread
     const int T = 1 << (W - kRegBits - (prog.paired ? 1 : 0));
-    const bool persistent = usePersistent(prog);
-    const unsigned smem = (unsigned) (((prog.isSingle ? sizeof(float2) : sizeof(double2)) << W) * (persistent ? 2 : 1));
+    const unsigned smem = (unsigned) ((prog.isSingle ? sizeof(float2) : sizeof(double2)) << W);
     // one attribute call per function: cheap and idempotent
     const Driver &drv = driver();
     if (!drv.ok) return cudaErrorNotSupported;
     CUresult r = drv.funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int) smem);
     if (r != CUDA_SUCCESS) return cudaErrorLaunchFailure;
-    unsigned grid = 1u << (prog.numBits - W);
-    if (persistent) {
-        int perSm = 0, dev = 0, sms = 0;
-        if (drv.occupancy(&perSm, fn, T, smem) != CUDA_SUCCESS || perSm < 1) perSm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const unsigned cap = (unsigned) (perSm * sms);
-        if (grid > cap) grid = cap;
-    }
+    const unsigned grid = prog.ctaCount ? prog.ctaCount : 1u << (prog.numBits - W);
     void *args[2] = {(void *) &st, (void *) &prog};
     r = drv.launchKernel(fn, grid, 1, 1, (unsigned) T, 1, 1, smem, (CUstream) s, args, nullptr);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;

@@ -448,24 +448,6 @@ __device__ __forceinline__ void jFixup(const TileProgram &prog, uint64_t gt, con
     }
 }
 
-__device__ __forceinline__ void jCpAsync16(void *smemPtr, const void *gptr) {
-    const uint32_t s = (uint32_t) __cvta_generic_to_shared(smemPtr);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gptr) : "memory");
-}
-__device__ __forceinline__ void jCpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void jCpAsyncWait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void jCpAsyncWait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// cp.async of tile `cta`'s canonical elements into buffer buf
-template <int W, class V>
-__device__ __forceinline__ void jPrefetch(const V *__restrict__ st, const TileProgram &prog, uint32_t tid,
-                                          uint32_t cta, V *buf) {
-    constexpr uint32_t T = 1u << (W - kRegBits);
-    const uint64_t base = jBase<W>(prog, tid, cta);
-#pragma unroll
-    for (int j = 0; j < kRegs; j++) jCpAsync16(&buf[swz(tid + T * (uint32_t) j)], st + jIndex<W>(prog, base, j));
-}
-
 template <int W, class V>
 __device__ __forceinline__ void jToSmem(V *sm, uint32_t tid, const V (&a)[kRegs]) {
     constexpr uint32_t T = 1u << (W - kRegBits);

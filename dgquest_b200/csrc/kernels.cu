@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
     extern __shared__ __align__(16) unsigned char smRaw[];
     V *sm = reinterpret_cast<V *>(smRaw);
     const uint32_t tid = threadIdx.x;
-    const uint32_t cta = blockIdx.x;
+    const uint32_t cta = blockIdx.x + prog.ctaOffset;
 
     // address of canonical element (tid, j): base | lane bits | thread high bits | j bits
     uint64_t tpart = tid & 31u;
@@ -143,7 +143,7 @@ static cudaError_t launchTileW(V *st, const TileProgram &prog, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attrSet = true;
     }
-    const unsigned grid = 1u << (prog.numBits - W);
+    const unsigned grid = prog.ctaCount ? prog.ctaCount : 1u << (prog.numBits - W);
     tileKernel<W, V><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
     return cudaGetLastError();
 }

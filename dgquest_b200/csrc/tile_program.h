@@ -147,6 +147,10 @@ struct TileProgram {
     // op.k == 4 act on the pair inside a slot (target address bit 0).
     uint8_t paired;
     uint8_t pad0[1];
+    // the launch covers CTAs ctaOffset .. ctaOffset + ctaCount (0: all): a
+    // sweep over one page of a state held in host memory, whose page-index
+    // bits are the top blockIdx bits
+    uint32_t ctaOffset, ctaCount;
     // > 0: not a tile sweep but a dense 2^denseK x 2^denseK unitary on the
     // address bits denseTargets[0..denseK) (bit 0 of the matrix index first);
     // its matrix is at denseOff doubles into the register's matrix buffer
