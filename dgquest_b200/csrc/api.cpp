@@ -485,7 +485,9 @@ bool launchPlanned(QuregState &s, const char *func, size_t from = 0) {
 void setRenorm(QuregState &s, size_t i, size_t last, int &event) {
     dgq::TileProgram &p = s.planned[i];
     p.isSingle = s.single ? 1 : 0;
-    if (!s.single) return;
+    // (a register in host memory runs each sweep page by page: no sweep sees
+    // the whole output's norm before the next one starts)
+    if (!s.single || s.hostTier) return;
     const dgq::TileProgram *prev = i > 0 ? &s.planned[i - 1] : nullptr;
     if (prev && prev->renormOut) {
         p.renormIn = 1;
@@ -691,12 +693,33 @@ void freeOn(void *ptr, cudaStream_t st) {
 
 bool flush(QuregState &s, const char *func) {
     if (s.pending.empty() && !s.initPending) return true;
+    if (s.hostTier) return dgq::hostTierFlush(s, func);
     return planPending(s, func, true, true);
+}
+
+// Entry points that need the state in HBM.
+bool vDeviceResident(const QuregState &s, const char *func) {
+    if (!s.hostTier) return true;
+    return raise(E_UNSUPPORTED, func, "not available for a register held in host memory (larger than the device budget)");
 }
 
 bool ensureProbs(QuregState &s, const char *func) {
     if (s.probsValid) return true;
     if (!flush(s, func)) return false;
+    if (s.hostTier) {
+        std::vector<double> p0;
+        double total = 0.0;
+        if (!dgq::hostTierProbs(s, p0, total, func)) return false;
+        const double sc2 = s.restrictActive ? s.rScale * s.rScale : 1.0;
+        s.totalProb = total * sc2;
+        s.p0.assign((size_t) s.numBits, 0.0);
+        for (int b = 0; b < s.numBits; b++) s.p0[(size_t) b] = p0[(size_t) b] * sc2;
+        if (s.restrictActive)
+            for (int b = 0; b < s.numBits; b++)
+                if ((s.rMask >> b) & 1ULL) s.p0[(size_t) b] = ((s.rValue >> b) & 1ULL) ? 0.0 : s.totalProb;
+        s.probsValid = true;
+        return true;
+    }
     dgq::ProbArgs a;
     std::memset(&a, 0, sizeof(a));
     int nf = 0;
@@ -813,7 +836,15 @@ void recordMatrix(const Qureg &q, u64 targets, u64 controls, const ComplexMatrix
 
 u64 bit(int q) { return 1ULL << q; }
 
+// Device budget for new registers (dgq_setDeviceBudget; 0: free HBM):
+// larger states go to the host tier.
+std::atomic<int64_t> g_deviceBudget{0};
+
 }  // namespace
+
+namespace dgq {
+bool planForPages(QuregState &s, const char *func) { return planPending(s, func, true, false); }
+}  // namespace dgq
 
 // ====================================================================
 // C API
@@ -895,6 +926,7 @@ int dgq_sampleOutcomes(Qureg q, int numSamples, uint32_t seed, uint64_t *outcome
     if (numSamples < 0 || (numSamples > 0 && !outcomes))
         return raise(E_INVALID_ARGUMENT, __func__, "numSamples < 0 or null output") ? 0 : -1;
     QuregState &s = *stateOf(q);
+    if (!vDeviceResident(s, __func__)) return -1;
     if (!flush(s, __func__)) return -1;
     if (numSamples == 0) return 0;
     dgq::Mt19937 rng;
@@ -1027,16 +1059,24 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
         delete s;
         return q;
     }
-    if (bytes + (64u << 20) > freeB + poolSpare()) {
-        delete s;
-        raise(E_SYS_TOO_BIG_FOR_DEVICE, func);
-        return q;
+    const size_t avail = freeB + poolSpare() > (64u << 20) ? freeB + poolSpare() - (64u << 20) : 0;
+    const int64_t setBudget = g_deviceBudget.load();
+    const size_t budget = setBudget > 0 ? std::min<size_t>(avail, (size_t) setBudget) : avail;
+    if (bytes > budget) {
+        // the host tier: the state in pinned host memory, paged through HBM
+        std::string err;
+        if (!dgq::hostTierAttach(*s, budget, err)) {
+            delete s;
+            raise(E_SYS_TOO_BIG_FOR_DEVICE, func, err.c_str());
+            return q;
+        }
     }
     if (!cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func)) {
+        dgq::hostTierRelease(*s);
         delete s;
         return q;
     }
-    if (!registerPool() || !cudaOk(allocOn(&s->dState, bytes, s->stream), func) ||
+    if (!registerPool() || (!s->hostTier && !cudaOk(allocOn(&s->dState, bytes, s->stream), func)) ||
         !cudaOk(allocOn((void **) &s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1), s->stream), func) ||
         !cudaOk(allocOn((void **) &s->dNorm, sizeof(double) * 2, s->stream), func) ||
         !cudaOk(cudaStreamSynchronize(s->stream), func)) {
@@ -1044,6 +1084,7 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
         freeOn(s->dProbOut, s->stream);
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
+        dgq::hostTierRelease(*s);
         delete s;
         return q;
     }
@@ -1091,6 +1132,7 @@ void destroyQureg(Qureg qureg, QuESTEnv env) {
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
     }
+    dgq::hostTierRelease(*s);
     delete s;
 }
 
@@ -1145,6 +1187,17 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
     s.probsValid = false;
     const uint64_t n = 1ULL << s.numQubits;
     const uint64_t total = 1ULL << s.numBits;
+    if (s.hostTier) {
+        cudaOk(dgq::hostTierSync(s, __func__) ? cudaSuccess : cudaErrorUnknown, __func__);
+        for (uint64_t i = 0; i < total; i++) {
+            const double r = i < n ? reals[i] : 0.0, m = i < n ? imags[i] : 0.0;
+            if (s.single)
+                reinterpret_cast<float2 *>(s.hState)[i] = make_float2((float) r, (float) m);
+            else
+                reinterpret_cast<double2 *>(s.hState)[i] = make_double2(r, m);
+        }
+        return;
+    }
     // stage re and im in chunks, interleave on the GPU
     const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 24);
     double *dRe = nullptr, *dIm = nullptr;
@@ -1496,7 +1549,15 @@ Complex getAmp(Qureg q, long long int index) {
         return out;
     }
     double2 a;
-    if (s.single) {
+    if (s.hostTier) {
+        // the flushed state is in pinned host memory
+        if (s.single) {
+            const float2 f = reinterpret_cast<const float2 *>(s.hState)[v];
+            a = make_double2(f.x, f.y);
+        } else {
+            a = reinterpret_cast<const double2 *>(s.hState)[v];
+        }
+    } else if (s.single) {
         float2 f;
         if (!cudaOk(cudaMemcpyAsync(&f, (const float2 *) s.dState + v, sizeof(f), cudaMemcpyDeviceToHost, s.stream),
                     __func__))
@@ -1615,14 +1676,26 @@ int dgq_setDenseFusion(Qureg q, int qubits) {
     return prev;
 }
 
-int dgq_planPending(Qureg q) {
+int64_t dgq_setDeviceBudget(int64_t bytes) { return g_deviceBudget.exchange(bytes > 0 ? bytes : 0); }
+
+int dgq_getHostTierStats(Qureg q, int *pageBits, int64_t *passes, int64_t *exchanges) {
     if (!vQureg(q, __func__)) return -1;
+    const QuregState &s = *stateOf(q);
+    if (pageBits) *pageBits = s.hostTier ? s.pageBits : 0;
+    if (passes) *passes = s.hostTierPasses;
+    if (exchanges) *exchanges = s.hostTierSwaps;
+    return s.hostTier ? 1 : 0;
+}
+
+int dgq_planPending(Qureg q) {
+    if (!vQureg(q, __func__) || !vDeviceResident(*stateOf(q), __func__)) return -1;
     return planPending(*stateOf(q), __func__) ? 0 : -1;
 }
 
 int dgq_launchPlanned(Qureg q) {
     if (!vQureg(q, __func__)) return -1;
     QuregState &s = *stateOf(q);
+    if (!vDeviceResident(s, __func__)) return -1;
     if (!launchPlanned(s, __func__)) return -1;
     s.probsValid = false;
     return 0;
@@ -1642,6 +1715,7 @@ void *dgq_getStream(Qureg q) {
 
 void *dgq_getDeviceState(Qureg q, int *numBits) {
     if (!vQureg(q, __func__)) return nullptr;
+    if (!vDeviceResident(*stateOf(q), __func__)) return nullptr;
     if (numBits) *numBits = stateOf(q)->numBits;
     return (void *) stateOf(q)->dState;
 }
@@ -1651,6 +1725,24 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
     QuregState &s = *stateOf(q);
     if (!flush(s, __func__)) return -1;
     const uint64_t n = 1ULL << s.numQubits;
+    if (s.hostTier) {
+        // logical order through the map, from pinned host memory
+        const double sc = s.restrictActive ? s.rScale : 1.0;
+        for (uint64_t i = 0; i < n; i++) {
+            const uint64_t v = toVirtualIndex(s, i);
+            double2 a;
+            if (s.single) {
+                const float2 f = reinterpret_cast<const float2 *>(s.hState)[v];
+                a = make_double2(f.x, f.y);
+            } else {
+                a = reinterpret_cast<const double2 *>(s.hState)[v];
+            }
+            const bool keep = !s.restrictActive || (v & s.rMask) == s.rValue;
+            re[i] = keep ? a.x * sc : 0.0;
+            im[i] = keep ? a.y * sc : 0.0;
+        }
+        return 0;
+    }
     const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 22);
     double2 *dOut = nullptr;
     if (!cudaOk(cudaMalloc(&dOut, chunk * sizeof(double2)), __func__)) return -1;
@@ -1860,6 +1952,7 @@ Complex calcInnerProduct(Qureg bra, Qureg ket) {
         raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
         return out;
     }
+    if (!vDeviceResident(b, __func__) || !vDeviceResident(k, __func__)) return out;
     if (!flush(b, __func__) || !flush(k, __func__)) return out;
     if (!cudaOk(cudaStreamSynchronize(b.stream), __func__) || !cudaOk(cudaStreamSynchronize(k.stream), __func__))
         return out;

@@ -1,0 +1,346 @@
+// host_tier.cpp -- registers larger than the device budget: the state in
+// pinned host memory, streamed through the GPU a page at a time.
+//
+// dgQuEST keeps every state in pinned host pages and moves them through the
+// GPU per section (page pool QuEST_backend_distributed.cpp:60-73,248-287;
+// H2D prefetch / D2H overlap :332-361,458-492), exchanging qubits between
+// sections with reorder_data_kernel (QuEST_gpu_kernel.cu:589-654). Here that
+// tier only serves states that do not fit in HBM:
+//
+//  * a page is 2^pageBits consecutive amplitudes; the bits above pageBits
+//    (page-index bits) are the top blockIdx bits of every sweep whose tile
+//    bits lie inside the page, so one plan serves every page: a page's
+//    launches cover its CTA range (TileProgram::ctaOffset / ctaCount) on a
+//    state pointer rebased so that the page's global indices land in its
+//    device buffer, and controls, selectors and collapses on page-index
+//    bits resolve per page exactly as in HBM;
+//  * the pending gates are cut into segments whose non-diagonal targets are
+//    all inside the page; a segment runs ALL its sweeps on a page while the
+//    page is on the device (one copy in, one copy out per page);
+//  * a gate that acts on a page-index bit h first exchanges h with the page
+//    bit whose next use is furthest away (Belady's rule), in a pass over
+//    page pairs that differ in h (launchPageSwap), and the logical-virtual
+//    map records the exchange;
+//  * the passes pipeline over kPageBufs device buffers, one stream each:
+//    copy in, kernels and copy out of different pages overlap.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "jit.h"
+#include "kernels.h"
+#include "qureg_state.h"
+
+namespace dgq {
+
+bool raiseExternal(int code, const char *func, const char *detail);
+
+namespace {
+
+constexpr int kErrUnsupported = 102;  // E_UNSUPPORTED
+constexpr int kMinPageBits = 14;      // holds a paired complex64 tile (W <= 13) and more
+
+size_t ampBytesOf(const QuregState &s) { return s.single ? sizeof(float2) : sizeof(double2); }
+
+bool ok(cudaError_t e, const char *func) {
+    if (e == cudaSuccess) return true;
+    return raiseExternal(kErrUnsupported, func, cudaGetErrorString(e));
+}
+
+char *hostPage(const QuregState &s, uint64_t page) {
+    return reinterpret_cast<char *>(s.hState) + (page << s.pageBits) * ampBytesOf(s);
+}
+
+// non-diagonal target bits of a gate (the bits a page must hold)
+u64 nonDiagonal(const Gate &g) { return isDiagonalType(g.type) ? 0 : g.targetMask; }
+
+void swapBitsOf(Gate &g, int a, int b) {
+    auto sw = [&](u64 m) {
+        const u64 ba = (m >> a) & 1ULL, bb = (m >> b) & 1ULL;
+        m &= ~((1ULL << a) | (1ULL << b));
+        return m | (ba << b) | (bb << a);
+    };
+    g.targetMask = sw(g.targetMask);
+    g.controlMask = sw(g.controlMask);
+    for (int i = 0; i < g.numMultiTargets; i++) {
+        if (g.multiTargets[i] == a)
+            g.multiTargets[i] = b;
+        else if (g.multiTargets[i] == b)
+            g.multiTargets[i] = a;
+    }
+}
+
+struct Segment {
+    std::vector<Gate> gates;
+    std::vector<std::pair<int, int>> swapsAfter;  // (page-index bit, page bit) exchanged after the segment
+};
+
+// Cuts the gates into page-local segments; the gates after each exchange
+// are rewritten in the exchanged bits.
+std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
+    std::vector<Segment> segs(1);
+    const u64 local = (1ULL << pageBits) - 1;
+    for (size_t i = 0; i < g.size(); i++) {
+        const u64 glob = nonDiagonal(g[i]) & ~local;
+        if (glob) {
+            u64 taken = nonDiagonal(g[i]) & local;
+            for (u64 m = glob; m; m &= m - 1) {
+                const int h = __builtin_ctzll(m);
+                int victim = -1;
+                size_t victimNext = 0;
+                for (int l = pageBits - 1; l >= 0; l--) {
+                    if ((taken >> l) & 1ULL) continue;
+                    size_t next = g.size();
+                    for (size_t j = i; j < g.size(); j++)
+                        if ((nonDiagonal(g[j]) >> l) & 1ULL) {
+                            next = j;
+                            break;
+                        }
+                    if (victim < 0 || next > victimNext) {
+                        victim = l;
+                        victimNext = next;
+                    }
+                }
+                taken |= 1ULL << victim;
+                segs.back().swapsAfter.emplace_back(h, victim);
+                for (size_t j = i; j < g.size(); j++) swapBitsOf(g[j], h, victim);
+            }
+            segs.emplace_back();
+        }
+        segs.back().gates.push_back(g[i]);
+    }
+    return segs;
+}
+
+// Whether a program touches only its page: tile bits below pageBits, the
+// blockIdx bits in ascending address order with the page-index bits on top
+// (then CTA range [page << (pageBits - W), ...) covers exactly the page).
+bool pageLocal(const TileProgram &p, int W, int pageBits, int numBits) {
+    if (p.denseK || W > pageBits || numBits - W > kMaxStateBits) return false;
+    for (int i = 0; i < W - kCoalescedBits; i++)
+        if (p.highPos[i] >= pageBits) return false;
+    for (int i = 0; i < numBits - W; i++) {
+        const int want = i < pageBits - W ? -1 : pageBits + (i - (pageBits - W));
+        if (want < 0 ? p.ctaPos[i] >= pageBits : p.ctaPos[i] != want) return false;
+        if (i > 0 && p.ctaPos[i] <= p.ctaPos[i - 1]) return false;
+    }
+    return true;
+}
+
+// Runs s.planned on every page: copy in (unless the first sweep writes the
+// whole page), the plan's sweeps, copy out.
+bool runPagePass(QuregState &s, const char *func) {
+    const int W = s.plannedTileBits;
+    for (const TileProgram &p : s.planned)
+        if (!pageLocal(p, W, s.pageBits, s.numBits))
+            return raiseExternal(kErrUnsupported, func, "internal: a sweep of the host tier reaches outside its page");
+    const uint64_t pages = 1ULL << (s.numBits - s.pageBits);
+    const uint32_t ctas = 1u << (s.pageBits - W);
+    const size_t pageBytes = ampBytesOf(s) << s.pageBits;
+    const bool load = s.planned.empty() || s.planned[0].initKind == INIT_NONE;
+    for (uint64_t page = 0; page < pages; page++) {
+        const int b = (int) (page % QuregState::kPageBufs);
+        cudaStream_t st = s.pageStream[b];
+        if (load && !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, page), pageBytes, cudaMemcpyHostToDevice, st), func))
+            return false;
+        // global index (page << pageBits) | i lands on buffer element i
+        const uintptr_t base = reinterpret_cast<uintptr_t>(s.dPage[b]) - (uintptr_t) ((page << s.pageBits) * ampBytesOf(s));
+        void *rebased = reinterpret_cast<void *>(base);
+        for (size_t i = 0; i < s.planned.size(); i++) {
+            TileProgram p = s.planned[i];
+            p.ctaOffset = (uint32_t) page * ctas;
+            p.ctaCount = ctas;
+            const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+            const cudaError_t e =
+                fn ? launchJitSweep(fn, rebased, W, p, st) : launchTile(rebased, s.single, W, p, st);
+            if (!ok(e, func)) return false;
+        }
+        if (!ok(cudaMemcpyAsync(hostPage(s, page), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
+            return false;
+    }
+    s.hostTierPasses++;
+    return hostTierSync(s, func);
+}
+
+// Exchanges page-index bit h with page bit l over all page pairs.
+bool runSwapPass(QuregState &s, int h, int l, const char *func) {
+    const uint64_t pages = 1ULL << (s.numBits - s.pageBits);
+    const uint64_t hb = 1ULL << (h - s.pageBits);
+    const size_t pageBytes = ampBytesOf(s) << s.pageBits;
+    int pair = 0;
+    for (uint64_t p0 = 0; p0 < pages; p0++) {
+        if (p0 & hb) continue;
+        const uint64_t p1 = p0 | hb;
+        const int a = 2 * (pair % (QuregState::kPageBufs / 2)), b = a + 1;
+        cudaStream_t st = s.pageStream[a];
+        if (!ok(cudaMemcpyAsync(s.dPage[a], hostPage(s, p0), pageBytes, cudaMemcpyHostToDevice, st), func) ||
+            !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, p1), pageBytes, cudaMemcpyHostToDevice, st), func) ||
+            !ok(launchPageSwap(s.dPage[a], s.dPage[b], s.single, s.pageBits, l, st), func) ||
+            !ok(cudaMemcpyAsync(hostPage(s, p0), s.dPage[a], pageBytes, cudaMemcpyDeviceToHost, st), func) ||
+            !ok(cudaMemcpyAsync(hostPage(s, p1), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
+            return false;
+        pair++;
+    }
+    if (!hostTierSync(s, func)) return false;
+    // the qubits at virtual bits h and l trade places
+    const int qa = s.v2l[h], qb = s.v2l[l];
+    s.v2l[h] = qb;
+    s.v2l[l] = qa;
+    if (qa >= 0) s.l2v[qa] = l;
+    if (qb >= 0) s.l2v[qb] = h;
+    s.hostTierSwaps++;
+    return true;
+}
+
+}  // namespace
+
+bool hostTierSync(QuregState &s, const char *func) {
+    for (int b = 0; b < QuregState::kPageBufs; b++)
+        if (s.pageStream[b] && !ok(cudaStreamSynchronize(s.pageStream[b]), func)) return false;
+    return true;
+}
+
+bool hostTierAttach(QuregState &s, size_t budgetBytes, std::string &err) {
+    const size_t ab = ampBytesOf(s);
+    int p = s.numBits - 1;
+    while (p >= kMinPageBits && (size_t) QuregState::kPageBufs * (ab << p) > budgetBytes) p--;
+    if (p < kMinPageBits) {
+        err = "the device budget holds no page buffers";
+        return false;
+    }
+    if (s.numBits > 40) {
+        err = "more than 2^40 amplitudes";
+        return false;
+    }
+    s.pageBits = p;
+    if (cudaHostAlloc(&s.hState, ab << s.numBits, cudaHostAllocDefault) != cudaSuccess) {
+        s.hState = nullptr;
+        err = "pinned host memory for the state is not available";
+        return false;
+    }
+    for (int b = 0; b < QuregState::kPageBufs; b++) {
+        if (cudaStreamCreateWithFlags(&s.pageStream[b], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaMalloc(&s.dPage[b], ab << p) != cudaSuccess ||
+            cudaMalloc((void **) &s.dPageOut[b], sizeof(double) * (kMaxStateBits + 1)) != cudaSuccess) {
+            hostTierRelease(s);
+            err = "device page buffers are not available";
+            return false;
+        }
+    }
+    s.hostTier = true;
+    return true;
+}
+
+void hostTierRelease(QuregState &s) {
+    for (int b = 0; b < QuregState::kPageBufs; b++) {
+        if (s.pageStream[b]) cudaStreamSynchronize(s.pageStream[b]);
+        if (s.dPage[b]) cudaFree(s.dPage[b]);
+        if (s.dPagePartial[b]) cudaFree(s.dPagePartial[b]);
+        if (s.dPageOut[b]) cudaFree(s.dPageOut[b]);
+        if (s.pageStream[b]) cudaStreamDestroy(s.pageStream[b]);
+        s.dPage[b] = nullptr;
+        s.dPagePartial[b] = nullptr;
+        s.dPageOut[b] = nullptr;
+        s.pageStream[b] = nullptr;
+    }
+    if (s.hState) cudaFreeHost(s.hState);
+    s.hState = nullptr;
+    s.hostTier = false;
+}
+
+bool hostTierFlush(QuregState &s, const char *func) {
+    if (s.pending.empty() && !s.initPending) return true;
+    for (const Gate &g : s.pending)
+        if (g.type == OP_MULTI_UNITARY && g.numMultiTargets > kRegBits)
+            return raiseExternal(kErrUnsupported, func,
+                                 "a multi-qubit unitary of more than 4 targets on a register in host memory");
+    std::vector<Segment> segs = cutSegments(s.pending, s.pageBits);
+    const MatrixPool pool = s.pool;
+    const bool denseFusion = s.denseFusion;
+    s.denseFusion = 0;
+    bool good = true;
+    for (size_t k = 0; k < segs.size() && good; k++) {
+        // the first segment carries the pending initialisation or collapse
+        // (a header-only pass when it holds no gates)
+        const bool header = k == 0 && (s.initPending || s.restrictActive);
+        if (!segs[k].gates.empty() || header) {
+            s.pending = segs[k].gates;
+            s.pool = pool;
+            good = planForPages(s, func) && runPagePass(s, func);
+        }
+        for (const auto &sw : segs[k].swapsAfter)
+            if (good) good = runSwapPass(s, sw.first, sw.second, func);
+    }
+    s.denseFusion = denseFusion;
+    s.pending.clear();
+    s.pool.mats.clear();
+    s.planned.clear();
+    s.plannedFns.clear();
+    s.probsValid = false;
+    return good;
+}
+
+bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const char *func) {
+    const int p = s.pageBits;
+    const uint64_t pages = 1ULL << (s.numBits - p);
+    const u64 localMask = (1ULL << p) - 1;
+    const u64 rMask = s.restrictActive ? s.rMask : 0, rValue = s.restrictActive ? s.rValue : 0;
+    ProbArgs a;
+    std::memset(&a, 0, sizeof(a));
+    int nf = 0;
+    for (int b = 0; b < p; b++) {
+        if ((rMask >> b) & 1ULL) continue;
+        a.freePos[nf++] = (uint8_t) b;
+    }
+    a.nFree = nf;
+    a.kappa = std::min(4, std::max(0, nf - 12));
+    a.rValue = rValue & localMask;
+    const size_t need = (size_t) probNumCtas(a) * 17;
+    if (need > s.pagePartialCap) {
+        for (int b = 0; b < QuregState::kPageBufs; b++) {
+            if (s.dPagePartial[b]) cudaFree(s.dPagePartial[b]);
+            s.dPagePartial[b] = nullptr;
+            if (!ok(cudaMalloc((void **) &s.dPagePartial[b], need * sizeof(double)), func)) return false;
+        }
+        s.pagePartialCap = need;
+    }
+    const size_t pageBytes = ampBytesOf(s) << p;
+    std::vector<double> sums(pages * (size_t) (nf + 1), 0.0);
+    std::vector<char> used(pages, 0);
+    for (uint64_t page = 0; page < pages; page++) {
+        // pages outside a collapse on page-index bits hold no probability
+        if (((page << p) & rMask & ~localMask) != (rValue & ~localMask)) continue;
+        used[page] = 1;
+        const int b = (int) (page % QuregState::kPageBufs);
+        cudaStream_t st = s.pageStream[b];
+        if (!ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, page), pageBytes, cudaMemcpyHostToDevice, st), func) ||
+            !ok(launchProb(s.dPage[b], s.single, a, s.dPagePartial[b], s.dPageOut[b], st), func) ||
+            !ok(cudaMemcpyAsync(&sums[page * (size_t) (nf + 1)], s.dPageOut[b], sizeof(double) * (size_t) (nf + 1),
+                                cudaMemcpyDeviceToHost, st),
+                func))
+            return false;
+    }
+    if (!hostTierSync(s, func)) return false;
+    s.hostTierPasses++;
+    p0.assign((size_t) s.numBits, 0.0);
+    total = 0.0;
+    for (uint64_t page = 0; page < pages; page++) {
+        if (!used[page]) continue;
+        const double *o = &sums[page * (size_t) (nf + 1)];
+        const double t = o[nf];
+        total += t;
+        for (int i = 0; i < nf; i++) p0[a.freePos[i]] += o[i];
+        for (int b = p; b < s.numBits; b++)
+            if (!(((page << p) >> b) & 1ULL)) p0[(size_t) b] += t;
+    }
+    // collapsed page bits: all the probability on their fixed value
+    for (int b = 0; b < p; b++)
+        if ((rMask >> b) & 1ULL) p0[(size_t) b] = ((rValue >> b) & 1ULL) ? 0.0 : total;
+    return true;
+}
+
+}  // namespace dgq

@@ -13,6 +13,7 @@
 // The state is 2^numBits double2 (re, im) amplitudes in HBM, in place.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "interp.cuh"
@@ -291,6 +292,25 @@ int probNumCtas(const ProbArgs &args) {
     return args.nFree > 12 + args.kappa ? (1 << (args.nFree - 12 - args.kappa)) : 1;
 }
 
+// Page-pair exchange of the host tier: pages a and b differ only in the
+// page-index bit that is being exchanged with local bit `bit`; every
+// amplitude of a whose local index has `bit` = 1 trades places with the
+// amplitude of b at the same index with `bit` = 0 (the two halves that the
+// exchange of the two address bits moves).
+template <class V>
+__global__ void pageSwapKernel(V *__restrict__ a, V *__restrict__ b, int pageBits, int bit) {
+    const uint64_t half = 1ULL << (pageBits - 1);
+    const uint64_t lo = (1ULL << bit) - 1;
+    for (uint64_t k = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; k < half;
+         k += (uint64_t) gridDim.x * blockDim.x) {
+        const uint64_t i = ((k & ~lo) << 1) | (1ULL << bit) | (k & lo);
+        const uint64_t j = i ^ (1ULL << bit);
+        const V x = a[i];
+        a[i] = b[j];
+        b[j] = x;
+    }
+}
+
 // --------------------------------------------------- bit-pair exchange
 // For every index whose bits at a[i] read pattern p and at b[i] read q with
 // p > q (as integers over the k pairs), exchange it with the index whose
@@ -316,6 +336,17 @@ __global__ void swapBitsKernel(double2 *__restrict__ st, const __grid_constant__
         st[i] = y;
         st[j] = x;
     }
+}
+
+cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit, cudaStream_t s) {
+    if (pageBits < 1 || bit < 0 || bit >= pageBits) return cudaErrorInvalidValue;
+    const uint64_t half = 1ULL << (pageBits - 1);
+    const unsigned grid = (unsigned) std::min<uint64_t>((half + 255) / 256, 148u * 16u);
+    if (single)
+        pageSwapKernel<float2><<<grid, 256, 0, s>>>((float2 *) a, (float2 *) b, pageBits, bit);
+    else
+        pageSwapKernel<double2><<<grid, 256, 0, s>>>((double2 *) a, (double2 *) b, pageBits, bit);
+    return cudaGetLastError();
 }
 
 cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s) {

@@ -95,6 +95,9 @@ cudaError_t launchProb(const void *st, bool single, const ProbArgs &args, double
                        cudaStream_t s);
 int probNumCtas(const ProbArgs &args);
 cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s);
+// Host tier: exchanges local bit `bit` with the page-index bit in which the
+// pages a and b (2^pageBits amplitudes each) differ.
+cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit, cudaStream_t s);
 cudaError_t launchGather(const void *st, bool single, const GatherArgs &args, double2 *out, cudaStream_t s);
 cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s);
 cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, void *out,

@@ -62,6 +62,23 @@ struct QuregState {
     std::vector<CUfunction> plannedFns;  // runtime-specialised kernel per program (or null)
     int plannedTileBits = 0;
     dgq_plan_stats stats{};
+
+    // host tier (states larger than the device budget): the state lives in
+    // pinned host memory in pages of 2^pageBits amplitudes (address bits
+    // below pageBits); every pass streams the pages through device buffers,
+    // one CUDA stream per buffer, and gates on page-index bits are first
+    // brought into the page by a page-pair exchange of two address bits
+    bool hostTier = false;
+    void *hState = nullptr;
+    int pageBits = 0;
+    static constexpr int kPageBufs = 4;
+    void *dPage[kPageBufs] = {};
+    cudaStream_t pageStream[kPageBufs] = {};
+    double *dPagePartial[kPageBufs] = {};
+    double *dPageOut[kPageBufs] = {};
+    size_t pagePartialCap = 0;
+    int64_t hostTierSwaps = 0;   // page-pair exchange passes run so far
+    int64_t hostTierPasses = 0;  // page passes (sweep segments and read-outs) run so far
 };
 
 namespace dgq {
@@ -79,5 +96,21 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
 // Drops the pending work that buildPrograms planned (after it has been
 // launched or kept for launching).
 void consumePending(QuregState &s);
+
+// Plans the register's pending gates (and pending initialisation or
+// collapse) into s.planned / s.plannedFns, compiling kernels as needed,
+// without launching (api.cpp).
+bool planForPages(QuregState &s, const char *func);
+
+// host tier (host_tier.cpp). attach: allocates the pinned state and the
+// page buffers for a device budget of budgetBytes (false with err set when
+// they cannot be had); flush: runs the pending work over the pages;
+// probs: P(bit = 0) for every address bit and the total probability of the
+// (collapsed, unscaled) state.
+bool hostTierAttach(QuregState &s, size_t budgetBytes, std::string &err);
+void hostTierRelease(QuregState &s);
+bool hostTierFlush(QuregState &s, const char *func);
+bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const char *func);
+bool hostTierSync(QuregState &s, const char *func);
 
 }  // namespace dgq

@@ -173,6 +173,8 @@ _SIGS = {
     "dgq_getPlanStats": (I, [Q, P(PlanStats)]),
     "dgq_planPending": (I, [Q]),
     "dgq_setDenseFusion": (I, [Q, I]),
+    "dgq_setDeviceBudget": (ctypes.c_int64, [ctypes.c_int64]),
+    "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64)]),
     "dgq_launchPlanned": (I, [Q]),
     "dgq_sync": (I, [Q]),
     "dgq_getStream": (c_void_p, [Q]),
@@ -289,6 +291,16 @@ def plan_stats(q):
     st = PlanStats()
     dgq_getPlanStats(q, ctypes.byref(st))
     return st
+
+
+def host_tier_stats(q):
+    """(page bits, page passes, qubit exchanges) of a host-tier register, or
+    None for a register in HBM."""
+    pb = ctypes.c_int(0)
+    passes = ctypes.c_int64(0)
+    ex = ctypes.c_int64(0)
+    r = dgq_getHostTierStats(q, ctypes.byref(pb), ctypes.byref(passes), ctypes.byref(ex))
+    return (pb.value, passes.value, ex.value) if r == 1 else None
 
 
 def seed(keys):

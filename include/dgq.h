@@ -62,6 +62,21 @@ typedef struct dgq_plan_stats {
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
+/* Host tier. A register whose state is larger than the device budget
+ * (free HBM, or the smaller budget set here for registers created later;
+ * 0 restores free HBM) keeps its state in pinned host memory in pages of
+ * 2^pageBits amplitudes and streams the pages through four device buffers
+ * (copy in, sweeps, copy out, overlapped on four streams). A gate on a qubit
+ * outside the page first exchanges that qubit with a page qubit in a pass
+ * over page pairs. Gates, read-outs and measurement work as in HBM; dense
+ * sweeps (multi-qubit unitaries of more than 4 targets), sampling, inner
+ * products, batches and the plan/launch split report E_UNSUPPORTED for
+ * such registers. Returns the previous budget. */
+int64_t dgq_setDeviceBudget(int64_t bytes);
+/* 1 for a host-tier register (with its page width, page passes and qubit
+ * exchanges so far), 0 for a register in HBM, -1 on error. */
+int dgq_getHostTierStats(Qureg qureg, int *pageBits, int64_t *passes, int64_t *exchanges);
+
 /* Dense-block form. qubits = 5, 6 or 7: the register's gates are fused into
  * dense unitaries on that many qubits (dgQuEST's greedy block rule,
  * DAG.cpp:219-259, with every qubit a gate touches counted), composed in
