@@ -386,6 +386,67 @@ def run_ncu_case(args):
     Q.destroyQuESTEnv(env)
 
 
+def run_host_tier_form(args, world):
+    """Host tier: the random circuit (28 qubits, depth 8, complex128: 4 GiB)
+    on a register held in pinned host memory under a 2 GiB device budget
+    (pages of 2^25 amplitudes through four device buffers), against the same
+    circuit in HBM; host<->device traffic is every pass's pages both ways."""
+    import torch
+
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    n, depth, budget = 28, 8, 2 << 30
+    ops = C.random_layers(n, depth, C.config_seed(2, 500))
+    env = Q.createQuESTEnv()
+    out = {"workload": f"random circuit n={n} depth={depth}, complex128, device budget {budget >> 30} GiB",
+           "qubits": n, "depth": depth}
+    # reference run in HBM
+    q = Q.createQureg(n, env)
+    Q.initZeroState(q)
+    C.replay(q, ops)
+    Q.getAmp(q, 0)
+    t0 = time.perf_counter()
+    Q.initZeroState(q)
+    C.replay(q, ops)
+    Q.getAmp(q, 0)
+    out["hbm_ms"] = (time.perf_counter() - t0) * 1e3
+    idx = np.random.RandomState(5).randint(0, 1 << n, size=1024)
+    ref = [Q.getAmp(q, int(i)) for i in idx]
+    Q.destroyQureg(q, env)
+    prev = Q.dgq_setDeviceBudget(budget)
+    try:
+        q = Q.createQureg(n, env)
+    finally:
+        Q.dgq_setDeviceBudget(prev)
+    st = Q.host_tier_stats(q)
+    out["page_bits"] = st[0]
+    for rep in range(2):
+        p0 = Q.host_tier_stats(q)
+        t0 = time.perf_counter()
+        Q.initZeroState(q)
+        C.replay(q, ops)
+        Q.getAmp(q, 0)
+        dt = time.perf_counter() - t0
+    p1 = Q.host_tier_stats(q)
+    passes, exchanges = p1[1] - p0[1], p1[2] - p0[2]
+    page_bytes = 16 << out["page_bits"]
+    pages = 1 << (n - out["page_bits"])
+    # sweep passes copy every page in and out (the first writes without
+    # reading); exchange passes do both for every page
+    moved = (2 * passes - 1) * pages * page_bytes + 2 * exchanges * pages * page_bytes
+    out.update({"ms_per_circuit": dt * 1e3, "page_passes": int(passes), "qubit_exchanges": int(exchanges),
+                "host_device_bytes": int(moved), "host_device_gbs": moved / dt / 1e9,
+                "vs_hbm": dt * 1e3 / out["hbm_ms"]})
+    err = 0.0
+    for i, a in zip(idx, ref):
+        b = Q.getAmp(q, int(i))
+        err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
+    out["max_abs_err_vs_hbm_sampled"] = err
+    Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+    return out
+
+
 def run_dense_form(args, world):
     """Dense 6-qubit blocks: multiQubitUnitary with 6 targets on a 30-qubit
     register, complex64 on the tensor cores (tcgen05, 3xTF32) and on the SIMT
@@ -646,6 +707,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
+    ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
     ap.add_argument("--no-tc-blocks", action="store_true", help="skip the dense-block tensor-core run of the grid circuit")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--dense-qubits", type=int, default=30)
@@ -676,6 +738,8 @@ def main():
         dense = run_dense_form(args, world)
         if rank == 0:
             line["dense_blocks"] = dense
+    if not args.no_host_tier and rank == 0 and world == 1:
+        line["host_tier"] = run_host_tier_form(args, world)
     if not args.no_grid32:
         grid = run_precision_form(args, world)
         if rank == 0:
