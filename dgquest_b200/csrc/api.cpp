@@ -836,6 +836,48 @@ void recordMatrix(const Qureg &q, u64 targets, u64 controls, const ComplexMatrix
 
 u64 bit(int q) { return 1ULL << q; }
 
+// Runs the pending work, applies a pending collapse to the amplitudes, and
+// moves amplitudes so that virtual bit = logical qubit (swapGate relabels
+// undone in HBM by swapBitsKernel, disjoint bit pairs per pass): afterwards
+// the buffer is the state in logical order, as dgQuEST's reorder at a
+// section boundary leaves it (QuEST_gpu_kernel.cu:589-654).
+bool normaliseLayout(QuregState &s, const char *func) {
+    if (s.restrictActive && s.pending.empty() && !s.initPending) {
+        // an empty program carries the collapse header into one sweep
+        dgq::Gate g;
+        g.type = dgq::OP_ONE;
+        s.pending.push_back(g);
+    }
+    if (!flush(s, func)) return false;
+    if (s.hostTier) return true;  // read through the map from host memory
+    for (;;) {
+        dgq::SwapArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.numBits = s.numBits;
+        uint64_t used = 0;
+        for (int q = 0; q < s.numQubits && a.numPairs < 32; q++) {
+            const int v = s.l2v[q];
+            if (v == q || ((used >> q) & 1ULL) || ((used >> v) & 1ULL)) continue;
+            a.a[a.numPairs] = (uint8_t) q;
+            a.b[a.numPairs] = (uint8_t) v;
+            a.numPairs++;
+            used |= (1ULL << q) | (1ULL << v);
+        }
+        if (a.numPairs == 0) break;
+        if (!cudaOk(dgq::launchSwapBits(s.dState, s.single, a, s.stream), func)) return false;
+        g_launches++;
+        for (int k = 0; k < a.numPairs; k++) {
+            // the qubits at virtual bits a[k] and b[k] trade places
+            const int qa = s.v2l[a.a[k]], qb = s.v2l[a.b[k]];
+            s.v2l[a.a[k]] = qb;
+            s.v2l[a.b[k]] = qa;
+            s.l2v[qa] = a.b[k];
+            s.l2v[qb] = a.a[k];
+        }
+    }
+    return cudaOk(cudaStreamSynchronize(s.stream), func);
+}
+
 // Device budget for new registers (dgq_setDeviceBudget; 0: free HBM):
 // larger states go to the host tier.
 std::atomic<int64_t> g_deviceBudget{0};
@@ -1219,6 +1261,138 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
     cudaOk(cudaStreamSynchronize(s.stream), __func__);
     cudaFree(dRe);
     cudaFree(dIm);
+}
+
+// include/QuEST.h:257 (declared only in dgQuEST): amplitudes [startInd,
+// startInd + numAmps) in logical order, the others kept
+void setAmps(Qureg qureg, long long int startInd, qreal *reals, qreal *imags, long long int numAmps) {
+    if (!vQureg(qureg, __func__) || !vStateIndex(qureg, startInd, __func__)) return;
+    QuregState &s = *stateOf(qureg);
+    if (numAmps < 0 || numAmps > (1LL << s.numQubits)) {
+        raise(E_INVALID_NUM_AMPS, __func__);
+        return;
+    }
+    if (startInd + numAmps > (1LL << s.numQubits)) {
+        raise(E_INVALID_OFFSET_NUM_AMPS, __func__);
+        return;
+    }
+    if (numAmps > 0 && (!reals || !imags)) {
+        raise(E_INVALID_ARGUMENT, __func__, "null amplitude array");
+        return;
+    }
+    if (!normaliseLayout(s, __func__)) return;
+    s.probsValid = false;
+    if (s.hostTier) {
+        for (long long k = 0; k < numAmps; k++) {
+            const uint64_t v = toVirtualIndex(s, (uint64_t) (startInd + k));
+            if (s.single)
+                reinterpret_cast<float2 *>(s.hState)[v] = make_float2((float) reals[k], (float) imags[k]);
+            else
+                reinterpret_cast<double2 *>(s.hState)[v] = make_double2(reals[k], imags[k]);
+        }
+        return;
+    }
+    const uint64_t chunk = std::min<uint64_t>((uint64_t) std::max<long long>(numAmps, 1), 1ULL << 24);
+    double *dRe = nullptr, *dIm = nullptr;
+    if (!cudaOk(cudaMalloc(&dRe, chunk * sizeof(double)), __func__)) return;
+    if (!cudaOk(cudaMalloc(&dIm, chunk * sizeof(double)), __func__)) {
+        cudaFree(dRe);
+        return;
+    }
+    for (uint64_t off = 0; off < (uint64_t) numAmps; off += chunk) {
+        const uint64_t c = std::min(chunk, (uint64_t) numAmps - off);
+        char *dst = (char *) s.dState + ((uint64_t) startInd + off) * ampBytes(s);
+        if (!cudaOk(cudaMemcpyAsync(dRe, reals + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__) ||
+            !cudaOk(cudaMemcpyAsync(dIm, imags + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__) ||
+            !cudaOk(dgq::launchInterleave(dRe, dIm, c, c, dst, s.single, s.stream), __func__))
+            break;
+        g_launches++;
+    }
+    cudaOk(cudaStreamSynchronize(s.stream), __func__);
+    cudaFree(dRe);
+    cudaFree(dIm);
+}
+
+// include/QuEST.h:267 (declared only in dgQuEST): targetQureg := copyQureg
+// (same qubit count and precision); the copy's pending work runs first
+void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
+    if (!vQureg(targetQureg, __func__) || !vQureg(copyQureg, __func__)) return;
+    QuregState &t = *stateOf(targetQureg);
+    QuregState &c = *stateOf(copyQureg);
+    if (t.numQubits != c.numQubits) {
+        raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
+        return;
+    }
+    if (t.single != c.single || t.hostTier != c.hostTier) {
+        raise(E_MISMATCHING_QUREG_TYPES, __func__);
+        return;
+    }
+    if (&t == &c) return;
+    if (!flush(c, __func__) || !cudaOk(cudaStreamSynchronize(c.stream), __func__)) return;
+    // the target's own pending work is dropped: its state is replaced
+    t.pending.clear();
+    t.pool.mats.clear();
+    t.initPending = false;
+    if (t.hostTier) {
+        if (!dgq::hostTierSync(t, __func__)) return;
+        std::memcpy(t.hState, c.hState, ampBytes(t) << t.numBits);
+    } else if (!cudaOk(cudaMemcpyAsync(t.dState, c.dState, ampBytes(t) << t.numBits, cudaMemcpyDeviceToDevice,
+                                       t.stream),
+                       __func__) ||
+               !cudaOk(cudaStreamSynchronize(t.stream), __func__)) {
+        return;
+    }
+    std::memcpy(t.l2v, c.l2v, sizeof(t.l2v));
+    std::memcpy(t.v2l, c.v2l, sizeof(t.v2l));
+    t.restrictActive = c.restrictActive;
+    t.rMask = c.rMask;
+    t.rValue = c.rValue;
+    t.rScale = c.rScale;
+    t.probsValid = false;
+}
+
+// include/QuEST.h:229: for state-vectors, the pure state's amplitudes
+void initPureState(Qureg qureg, Qureg pure) { cloneQureg(qureg, pure); }
+
+// include/QuEST.h:183
+void reportQuregParams(Qureg qureg) {
+    if (!vQureg(qureg, __func__)) return;
+    const QuregState &s = *stateOf(qureg);
+    printf("QUBITS:\n");
+    printf("Number of qubits is %d.\n", s.numQubits);
+    printf("Number of amps is %llu.\n", 1ULL << s.numQubits);
+    printf("Precision: %s, state in %s.\n", s.single ? "complex64" : "complex128",
+           s.hostTier ? "pinned host memory (host tier)" : "HBM");
+}
+
+// include/QuEST.h:177: every amplitude, for small registers
+void reportStateToScreen(Qureg qureg, QuESTEnv env, int reportRank) {
+    (void) env;
+    (void) reportRank;
+    if (!vQureg(qureg, __func__)) return;
+    QuregState &s = *stateOf(qureg);
+    if (s.numQubits > 5) {
+        printf("Error: reportStateToScreen will not print output for systems of more than 5 qubits.\n");
+        return;
+    }
+    const uint64_t n = 1ULL << s.numQubits;
+    std::vector<double> re(n), im(n);
+    if (dgq_getStateVector(qureg, re.data(), im.data()) != 0) return;
+    printf("Reporting state from rank 0 [\n");
+    printf("real, imag\n");
+    for (uint64_t i = 0; i < n; i++) printf("%.14f, %.14f\n", re[i], im[i]);
+    printf("]\n");
+}
+
+// include/QuEST.h:538
+void getEnvironmentString(QuESTEnv env, Qureg qureg, char str[200]) {
+    (void) env;
+    if (!str) return;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    snprintf(str, 200, "CUDA=1 OpenMP=0 MPI=0 threads=%d ranks=1 device=%d SMs=%d qubits=%d", 1, dev, sms,
+             qureg.state ? qureg.state->numQubits : 0);
 }
 
 // ---------------------------------------------------------------- gates
@@ -1716,6 +1890,7 @@ void *dgq_getStream(Qureg q) {
 void *dgq_getDeviceState(Qureg q, int *numBits) {
     if (!vQureg(q, __func__)) return nullptr;
     if (!vDeviceResident(*stateOf(q), __func__)) return nullptr;
+    if (!normaliseLayout(*stateOf(q), __func__)) return nullptr;
     if (numBits) *numBits = stateOf(q)->numBits;
     return (void *) stateOf(q)->dState;
 }

@@ -315,7 +315,8 @@ __global__ void pageSwapKernel(V *__restrict__ a, V *__restrict__ b, int pageBit
 // For every index whose bits at a[i] read pattern p and at b[i] read q with
 // p > q (as integers over the k pairs), exchange it with the index whose
 // patterns are swapped. Every orbit has length 1 or 2, so this is in place.
-__global__ void swapBitsKernel(double2 *__restrict__ st, const __grid_constant__ SwapArgs args) {
+template <class V>
+__global__ void swapBitsKernel(V *__restrict__ st, const __grid_constant__ SwapArgs args) {
     const uint64_t numAmps = 1ULL << args.numBits;
     for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < numAmps;
          i += (uint64_t) gridDim.x * blockDim.x) {
@@ -331,8 +332,8 @@ __global__ void swapBitsKernel(double2 *__restrict__ st, const __grid_constant__
             j |= (uint64_t) ((q >> k) & 1u) << args.a[k];
             j |= (uint64_t) ((p >> k) & 1u) << args.b[k];
         }
-        const double2 x = st[i];
-        const double2 y = st[j];
+        const V x = st[i];
+        const V y = st[j];
         st[i] = y;
         st[j] = x;
     }
@@ -349,11 +350,14 @@ cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit,
     return cudaGetLastError();
 }
 
-cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s) {
+cudaError_t launchSwapBits(void *st, bool single, const SwapArgs &args, cudaStream_t s) {
     const uint64_t numAmps = 1ULL << args.numBits;
     uint64_t blocks = (numAmps + 255) / 256;
     if (blocks > 148ULL * 64) blocks = 148ULL * 64;
-    swapBitsKernel<<<(unsigned) blocks, 256, 0, s>>>(st, args);
+    if (single)
+        swapBitsKernel<float2><<<(unsigned) blocks, 256, 0, s>>>((float2 *) st, args);
+    else
+        swapBitsKernel<double2><<<(unsigned) blocks, 256, 0, s>>>((double2 *) st, args);
     return cudaGetLastError();
 }
 

@@ -94,7 +94,8 @@ cudaError_t launchTile(void *st, bool single, int tileBits, const TileProgram &p
 cudaError_t launchProb(const void *st, bool single, const ProbArgs &args, double *partial, double *out,
                        cudaStream_t s);
 int probNumCtas(const ProbArgs &args);
-cudaError_t launchSwapBits(double2 *st, const SwapArgs &args, cudaStream_t s);
+// Exchanges address bits a[k] <-> b[k] (disjoint pairs) of the whole state, in place.
+cudaError_t launchSwapBits(void *st, bool single, const SwapArgs &args, cudaStream_t s);
 // Host tier: exchanges local bit `bit` with the page-index bit in which the
 // pages a and b (2^pageBits amplitudes each) differ.
 cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit, cudaStream_t s);

@@ -118,6 +118,12 @@ _SIGS = {
     "initPlusState": (None, [Q]),
     "initClassicalState": (None, [Q, c_longlong]),
     "initStateFromAmps": (None, [Q, P(D), P(D)]),
+    "initPureState": (None, [Q, Q]),
+    "setAmps": (None, [Q, c_longlong, P(D), P(D), c_longlong]),
+    "cloneQureg": (None, [Q, Q]),
+    "reportQuregParams": (None, [Q]),
+    "reportStateToScreen": (None, [Q, QuESTEnv, I]),
+    "getEnvironmentString": (None, [QuESTEnv, Q, ctypes.c_char_p]),
     "phaseShift": (None, [Q, I, D]),
     "controlledPhaseShift": (None, [Q, I, I, D]),
     "multiControlledPhaseShift": (None, [Q, P(I), I, D]),

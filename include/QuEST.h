@@ -91,6 +91,13 @@ void initZeroState(Qureg qureg);                      /* include/QuEST.h:199 */
 void initPlusState(Qureg qureg);                      /* include/QuEST.h:210 */
 void initClassicalState(Qureg qureg, long long int stateInd); /* include/QuEST.h:220 */
 void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags); /* include/QuEST.h:242 */
+/* declared only in dgQuEST (no body there); state-vector semantics of upstream QuEST */
+void initPureState(Qureg qureg, Qureg pure);           /* include/QuEST.h:229 */
+void setAmps(Qureg qureg, long long int startInd, qreal *reals, qreal *imags, long long int numAmps); /* :257 */
+void cloneQureg(Qureg targetQureg, Qureg copyQureg);  /* include/QuEST.h:267 */
+void reportQuregParams(Qureg qureg);                  /* include/QuEST.h:183 */
+void reportStateToScreen(Qureg qureg, QuESTEnv env, int reportRank); /* include/QuEST.h:177 */
+void getEnvironmentString(QuESTEnv env, Qureg qureg, char str[200]); /* include/QuEST.h:538 */
 
 /* ---- gates -------------------------------------------------------------- */
 void phaseShift(Qureg qureg, const int targetQubit, qreal angle);                       /* :299 */

@@ -99,9 +99,11 @@ int dgq_sync(Qureg qureg);
 
 /* The CUDA stream (cudaStream_t) all of this register's kernels run on. */
 void *dgq_getStream(Qureg qureg);
-/* Device pointer of the state buffer (interleaved re/im doubles) and its
- * number of address bits (>= numQubits; extra bits are always |0>). The
- * state is in virtual order; see dgq_getStateVector for logical order. */
+/* Device pointer of the state buffer (interleaved re/im doubles, or floats
+ * for complex64 registers) and its number of address bits (>= numQubits;
+ * extra bits are always |0>). Pending gates run first, a pending collapse
+ * is applied and swapGate relabels are undone in HBM, so the buffer holds
+ * the state in logical index order until the next gate call. */
 void *dgq_getDeviceState(Qureg qureg, int *numBits);
 
 /* Copies all 2^n amplitudes, in logical index order, into re[] and im[]. */
