@@ -199,15 +199,63 @@ uint64_t toVirtualIndex(const QuregState &s, uint64_t logical) {
 // ansatz, each at W = 10, 11, 12): 2.6 ms per sweep and 1.8 ms per phase
 // for 2^30 amplitudes. For circuits of equal gates the FP64 work is the same
 // at every W, so it lives in those two rates.
+// The rates can be replaced by a calibration of this GPU
+// (dgquest_b200/calibrate.py measures them; dgq_setCostModel installs them,
+// dgq_loadCostModel or DGQ_COST_FILE reads the file it writes).
 struct CostModel {
     double sweepSecondsPerAmp = 2.6e-3 / 1073741824.0;
     double phaseSecondsPerAmp = 1.8e-3 / 1073741824.0;
     double launchSeconds = 3e-6;
 };
 
+std::mutex g_costMutex;
+CostModel g_cost;
+bool g_costFileTried = false;
+
+// "dgq_cost 1" then "sweep_ms_per_2p30 <x>" and "phase_ms_per_2p30 <y>"
+// lines (any order, '#' comments); returns false on a malformed file.
+bool readCostFile(const char *path, double &sweepMs, double &phaseMs) {
+    FILE *f = fopen(path, "r");
+    if (!f) return false;
+    char line[256];
+    bool header = false, haveS = false, haveP = false;
+    while (fgets(line, sizeof(line), f)) {
+        char key[64];
+        double v = 0.0;
+        if (line[0] == '#' || line[0] == '\n') continue;
+        if (sscanf(line, "%63s %lf", key, &v) != 2) continue;
+        if (!strcmp(key, "dgq_cost") && v == 1.0) header = true;
+        if (!strcmp(key, "sweep_ms_per_2p30")) {
+            sweepMs = v;
+            haveS = true;
+        }
+        if (!strcmp(key, "phase_ms_per_2p30")) {
+            phaseMs = v;
+            haveP = true;
+        }
+    }
+    fclose(f);
+    return header && haveS && haveP && sweepMs > 0.0 && phaseMs >= 0.0 && std::isfinite(sweepMs) &&
+           std::isfinite(phaseMs);
+}
+
+CostModel costModel() {
+    std::lock_guard<std::mutex> lk(g_costMutex);
+    if (!g_costFileTried) {
+        g_costFileTried = true;
+        const char *path = getenv("DGQ_COST_FILE");
+        double sw = 0.0, ph = 0.0;
+        if (path && readCostFile(path, sw, ph)) {
+            g_cost.sweepSecondsPerAmp = sw * 1e-3 / 1073741824.0;
+            g_cost.phaseSecondsPerAmp = ph * 1e-3 / 1073741824.0;
+        }
+    }
+    return g_cost;
+}
+
 double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, const dgq::MatrixPool &pool,
                           int lookahead) {
-    const CostModel cm;
+    const CostModel cm = costModel();
     std::vector<dgq::BlockPlan> blocks = dgq::planBlocks(gates, numBits, W, nullptr, dgq::kCoalescedBits, lookahead);
     const double amps = std::ldexp(1.0, numBits);
     std::vector<dgq::TileProgram> progs;
@@ -1848,6 +1896,31 @@ int dgq_setDenseFusion(Qureg q, int qubits) {
     const int prev = s.denseFusion;
     s.denseFusion = qubits;
     return prev;
+}
+
+int dgq_setCostModel(double sweepMsPer2p30, double phaseMsPer2p30) {
+    if (!(sweepMsPer2p30 > 0.0) || !(phaseMsPer2p30 >= 0.0) || !std::isfinite(sweepMsPer2p30) ||
+        !std::isfinite(phaseMsPer2p30))
+        return raise(E_INVALID_ARGUMENT, __func__, "rates must be finite, sweep > 0, phase >= 0") ? 0 : -1;
+    std::lock_guard<std::mutex> lk(g_costMutex);
+    g_costFileTried = true;
+    g_cost.sweepSecondsPerAmp = sweepMsPer2p30 * 1e-3 / 1073741824.0;
+    g_cost.phaseSecondsPerAmp = phaseMsPer2p30 * 1e-3 / 1073741824.0;
+    return 0;
+}
+
+int dgq_loadCostModel(const char *path) {
+    double sw = 0.0, ph = 0.0;
+    if (!path || !readCostFile(path, sw, ph))
+        return raise(E_INVALID_ARGUMENT, __func__, "missing or malformed cost file") ? 0 : -1;
+    return dgq_setCostModel(sw, ph);
+}
+
+int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30) {
+    const CostModel cm = costModel();
+    if (sweepMsPer2p30) *sweepMsPer2p30 = cm.sweepSecondsPerAmp * 1073741824.0 * 1e3;
+    if (phaseMsPer2p30) *phaseMsPer2p30 = cm.phaseSecondsPerAmp * 1073741824.0 * 1e3;
+    return 0;
 }
 
 int64_t dgq_setDeviceBudget(int64_t bytes) { return g_deviceBudget.exchange(bytes > 0 ? bytes : 0); }

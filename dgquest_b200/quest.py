@@ -180,6 +180,9 @@ _SIGS = {
     "dgq_planPending": (I, [Q]),
     "dgq_setDenseFusion": (I, [Q, I]),
     "dgq_setDeviceBudget": (ctypes.c_int64, [ctypes.c_int64]),
+    "dgq_setCostModel": (I, [D, D]),
+    "dgq_loadCostModel": (I, [ctypes.c_char_p]),
+    "dgq_getCostModel": (I, [P(D), P(D)]),
     "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64)]),
     "dgq_launchPlanned": (I, [Q]),
     "dgq_sync": (I, [Q]),

@@ -62,6 +62,18 @@ typedef struct dgq_plan_stats {
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
+/* Cost model of the tile-width choice (the recast of dgQuEST's time
+ * predictor and its predict_data.txt calibration, time_predictor.cpp:397-476):
+ * a plan costs sweepMs per sweep plus phaseMs per register phase, per 2^30
+ * amplitudes. Built-in rates were fitted on B200 (2.6 and 1.8 ms);
+ * dgquest_b200/calibrate.py measures them on the GPU at hand and writes a
+ * cost file ("dgq_cost 1", "sweep_ms_per_2p30 x", "phase_ms_per_2p30 y"),
+ * read by dgq_loadCostModel or, at the first plan, from DGQ_COST_FILE.
+ * Return 0, or -1 on a bad argument or file. */
+int dgq_setCostModel(double sweepMsPer2p30, double phaseMsPer2p30);
+int dgq_loadCostModel(const char *path);
+int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30);
+
 /* Host tier. A register whose state is larger than the device budget
  * (free HBM, or the smaller budget set here for registers created later;
  * 0 restores free HBM) keeps its state in pinned host memory in pages of

@@ -1,0 +1,58 @@
+"""The tile-width cost model and its calibration file (host only): the
+file format is read and checked, and the planner's width choice is the
+argmin of sweeps x sweep_ms + phases x phase_ms (+ 3 us per launch) over the
+widths, for whichever rates are installed."""
+import ctypes
+
+import pytest
+
+from dgquest_b200 import calibrate as CAL
+from dgquest_b200 import circuits as C
+from dgquest_b200 import ir
+from dgquest_b200 import quest as Q
+
+
+@pytest.fixture
+def restore_rates():
+    prev = CAL.current()
+    yield
+    Q.dgq_setCostModel(*prev)
+
+
+def predicted(st, n, sweep_ms, phase_ms):
+    amps = float(1 << n)
+    return st.sweeps * (amps * sweep_ms * 1e-3 / 2**30 + 3e-6) + st.phases * amps * phase_ms * 1e-3 / 2**30
+
+
+@pytest.mark.parametrize("rates", [(2.6, 1.8), (10.0, 0.01), (0.01, 10.0)])
+def test_width_choice_is_the_model_argmin(rates, restore_rates):
+    n = 20  # below the lookahead threshold: one candidate per width
+    Q.dgq_setCostModel(*rates)
+    for ops in (C.random_layers(n, 12, C.config_seed(2, 710)), C.grid_sqrt(4, 5, 10, C.config_seed(3, 711))):
+        cands = {w: ir.plan(ops, n, w) for w in (9, 10, 11, 12)}
+        best = min(cands, key=lambda w: (predicted(cands[w], n, *rates), w))
+        assert ir.plan(ops, n, 0).tileBits == best
+
+
+def test_cost_file_round_trip(tmp_path, restore_rates):
+    path = tmp_path / "cost.txt"
+    CAL.write(str(path), 3.25, 0.75, note="test")
+    assert Q.dgq_loadCostModel(str(path).encode()) == 0
+    s, p = CAL.current()
+    assert abs(s - 3.25) < 1e-9 and abs(p - 0.75) < 1e-9
+    bad = tmp_path / "bad.txt"
+    bad.write_text("sweep_ms_per_2p30 1.0\n")  # no header, no phase rate
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_loadCostModel(str(bad).encode())
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_setCostModel(-1.0, 1.0)
+    assert CAL.current() == pytest.approx((3.25, 0.75))
+
+
+def test_fit_recovers_rates():
+    rows = []
+    for s, p in [(17, 52), (19, 55), (21, 57), (8, 23), (14, 44), (20, 49)]:
+        rows.append({"sweeps": s, "phases": p, "ms": (s * 2.5 + p * 1.5) / 16.0})  # n = 26
+    sweep_ms, phase_ms = CAL.fit(rows, 26)
+    assert abs(sweep_ms - 2.5) < 1e-9 and abs(phase_ms - 1.5) < 1e-9
+    assert ctypes.sizeof(ctypes.c_double) == 8
