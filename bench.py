@@ -672,16 +672,26 @@ def run_serving_form(args, world):
     (complex64) or [16, 32] (complex128), 40/30/30 random / GHZ+QFT / BV,
     1024 samples and <Z> on 4 qubits per request; the first --serve-requests
     requests of the stream, admitted by state bytes against free HBM."""
+    from dgquest_b200 import circuits as C
     from dgquest_b200 import quest as Q
     from dgquest_b200 import serving as S
     env = Q.createQuESTEnv()
     out = {"workload": "Poisson arrivals 200/s; random(depth 8-24)/GHZ+QFT/BV 40/30/30; 1024 samples + <Z> on 4 qubits",
-           "requests_per_precision": args.serve_requests}
+           "requests_per_precision": args.serve_requests, "warmup_requests": args.serve_warmup}
     for name, single in (("complex64", True), ("complex128", False)):
         reqs = S.make_requests(args.serve_requests, rate=200.0, single=single)
         srv = S.Server(env, workers=args.serve_workers)
+        # a running server: memory pool grown, then a warm-up stream of other
+        # requests (same distribution, another seed) before the measured one
+        srv.prewarm(single)
+        warm = S.make_requests(args.serve_warmup, rate=200.0, single=single, seed=C.config_seed(5, 900000),
+                               first_id=200000)
+        cold = S.summarize(srv.serve(warm, realtime=True)) if warm else None
         res = srv.serve(reqs, realtime=True)
         st = S.summarize(res)
+        if cold:
+            st["warmup_stream"] = {"requests": cold["requests"], "p50_ms": cold["p50_ms"], "p99_ms": cold["p99_ms"],
+                                   "circuits_per_s": cold["circuits_per_s"]}
         st.update({"peak_in_flight": srv.peak_in_flight, "peak_state_gb": srv.peak_in_use / 1e9,
                    "budget_gb": srv.budget / 1e9, "offered_rate": 200.0,
                    "offered_state_gb_per_s": sum(S.state_bytes(r) for r in reqs) / reqs[-1].arrival / 1e9,
@@ -707,6 +717,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
+    ap.add_argument("--serve-warmup", type=int, default=60, help="requests of the serving warm-up stream")
     ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
     ap.add_argument("--no-tc-blocks", action="store_true", help="skip the dense-block tensor-core run of the grid circuit")
     ap.add_argument("--no-dense", action="store_true")

@@ -1923,6 +1923,8 @@ int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30) {
     return 0;
 }
 
+void dgq_shutdown(void) { dgq::jitStopBackground(); }
+
 int64_t dgq_setDeviceBudget(int64_t bytes) { return g_deviceBudget.exchange(bytes > 0 ? bytes : 0); }
 
 int dgq_getHostTierStats(Qureg q, int *pageBits, int64_t *passes, int64_t *exchanges) {

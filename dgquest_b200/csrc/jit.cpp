@@ -727,13 +727,19 @@ namespace {
 // Compiled but not yet loaded kernels (from background compiles), and the
 // background compile queue. Heap-allocated and never destroyed, so a
 // compile still running at process exit touches no destroyed object.
+// Background compiles run on a pool of worker threads that wait for work on
+// a condition variable; at process exit the pool is stopped and JOINED, so
+// no worker is inside NVRTC, or still tearing down its thread state, while
+// the process destroys NVRTC's and the CUDA runtime's globals.
 struct CubinCache {
     std::mutex mu;
-    std::condition_variable idle;
+    std::condition_variable work;
     std::unordered_map<size_t, std::vector<std::pair<std::string, std::vector<char>>>> cubins;
     std::vector<std::string> queue;
     std::unordered_map<size_t, int> queued;  // source hash -> pending count
-    int workers = 0;
+    std::vector<std::thread> pool;
+    int alive = 0;  // workers that have not returned
+    std::condition_variable gone;
     bool stopping = false;
 };
 CubinCache &cubinCache() {
@@ -759,10 +765,11 @@ void backgroundWorker() {
     for (;;) {
         std::string src;
         {
-            std::lock_guard<std::mutex> lk(c.mu);
-            if (c.queue.empty() || c.stopping) {
-                c.workers--;
-                c.idle.notify_all();
+            std::unique_lock<std::mutex> lk(c.mu);
+            c.work.wait(lk, [&]() { return c.stopping || !c.queue.empty(); });
+            if (c.stopping) {
+                c.alive--;
+                c.gone.notify_all();
                 return;
             }
             src = std::move(c.queue.back());
@@ -788,15 +795,32 @@ bool jitAllReady(const std::vector<std::string> &sources) {
     return true;
 }
 
-// At process exit: drop the queue and wait for compiles in progress, so no
-// background thread is inside NVRTC while the process tears down.
-static void stopBackgroundCompiles() {
+// Drops the queue, lets compiles in progress finish (30 s at most) and joins
+// the workers. Called by dgq_shutdown (the Python binding calls it from its
+// exit hook, while NVRTC and the CUDA runtime are still intact) and, as a
+// fallback, from a C atexit handler.
+void jitStopBackground() {
     CubinCache &c = cubinCache();
-    std::unique_lock<std::mutex> lk(c.mu);
-    c.stopping = true;
-    c.queue.clear();
-    c.idle.wait_for(lk, std::chrono::seconds(60), [&]() { return c.workers == 0; });
+    std::vector<std::thread> pool;
+    bool all = false;
+    {
+        std::unique_lock<std::mutex> lk(c.mu);
+        c.stopping = true;
+        c.queue.clear();
+        c.work.notify_all();
+        all = c.gone.wait_for(lk, std::chrono::seconds(30), [&]() { return c.alive == 0; });
+        pool.swap(c.pool);
+    }
+    for (auto &t : pool) {
+        if (!t.joinable()) continue;
+        if (all)
+            t.join();
+        else
+            t.detach();
+    }
 }
+
+static void stopBackgroundCompiles() { jitStopBackground(); }
 
 void jitCompileInBackground(const std::vector<std::string> &sources) {
     static std::once_flag registered;
@@ -816,11 +840,12 @@ void jitCompileInBackground(const std::vector<std::string> &sources) {
         c.queue.push_back(src);
     }
     unsigned hw = std::thread::hardware_concurrency();
-    const int maxWorkers = (int) std::max(1u, std::min(8u, hw / 2));
-    while (c.workers < maxWorkers && (int) c.queue.size() > c.workers) {
-        c.workers++;
-        std::thread(backgroundWorker).detach();
+    const size_t maxWorkers = std::max(1u, std::min(8u, hw / 2));
+    while (c.pool.size() < maxWorkers && c.queue.size() > c.pool.size()) {
+        c.alive++;
+        c.pool.emplace_back(backgroundWorker);
     }
+    c.work.notify_all();
 }
 
 bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log) {

@@ -44,6 +44,10 @@ bool jitAllReady(const std::vector<std::string> &sources);
 // jitGetKernels calls load the results instead of compiling.
 void jitCompileInBackground(const std::vector<std::string> &sources);
 
+// Stops the background compiles: drops the queue, waits for compiles in
+// progress (30 s at most) and joins the worker threads.
+void jitStopBackground();
+
 // NVRTC compile only (no GPU needed).
 bool jitCompileOnly(const std::string &src, std::vector<char> &cubin, std::string &log);
 

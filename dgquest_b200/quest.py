@@ -8,6 +8,7 @@ This mirror switches the library to status recording and raises
 ``QuESTError(code, message)`` instead, so a Python process survives bad
 input; ``code`` is QuEST's error code.
 """
+import atexit
 import ctypes
 from ctypes import POINTER, Structure, c_double, c_int, c_int64, c_longlong, c_ulong, c_ulonglong, c_void_p
 
@@ -180,6 +181,7 @@ _SIGS = {
     "dgq_planPending": (I, [Q]),
     "dgq_setDenseFusion": (I, [Q, I]),
     "dgq_setDeviceBudget": (ctypes.c_int64, [ctypes.c_int64]),
+    "dgq_shutdown": (None, []),
     "dgq_setCostModel": (I, [D, D]),
     "dgq_loadCostModel": (I, [ctypes.c_char_p]),
     "dgq_getCostModel": (I, [P(D), P(D)]),
@@ -254,6 +256,16 @@ def _wrap(name):
 
 for _name in _SIGS:
     globals()[_name] = _wrap(_name)
+
+
+def _shutdown():
+    # runs at interpreter exit, before C-level teardown: stop and join the
+    # library's background compile threads while NVRTC is intact
+    if _lib is not None:
+        _lib.dgq_shutdown()
+
+
+atexit.register(_shutdown)
 
 
 # ---------------------------------------------------------------- helpers

@@ -56,7 +56,9 @@ class Result:
         return self.done - self.arrival
 
 
-def make_requests(count, rate=200.0, single=False, seed=None, n_range=None):
+def make_requests(count, rate=200.0, single=False, seed=None, n_range=None, first_id=0):
+    """Request stream: `seed` drives arrivals, sizes and kinds; circuit and
+    sample seeds follow the request ids first_id, first_id + 1, ..."""
     rng = C.Mt19937(C.config_seed(5) if seed is None else seed)
     lo, hi = n_range or ((16, 33) if single else (16, 32))
     t = 0.0
@@ -72,7 +74,8 @@ def make_requests(count, rate=200.0, single=False, seed=None, n_range=None):
             q = rng.below(n)
             if q not in zq:
                 zq.append(q)
-        out.append(Request(i, kind, n, depth, C.config_seed(5, i), t, tuple(zq), C.config_seed(5, 100000 + i),
+        rid = first_id + i
+        out.append(Request(rid, kind, n, depth, C.config_seed(5, rid), t, tuple(zq), C.config_seed(5, 100000 + rid),
                            single))
     return out
 
@@ -124,6 +127,27 @@ class Server:
         self.budget = int(hbm_budget)
         self.workers = int(workers)
         self.max_bypass = int(max_bypass)
+
+    def prewarm(self, single=False):
+        """Grows the register memory pool to the budget once (registers are
+        stream-ordered allocations from a pool that keeps freed memory), so
+        that the first requests do not pay for mapping fresh device memory.
+        Returns the bytes touched."""
+        regs, used = [], 0
+        n = 33 if single else 32
+        try:
+            while n >= 16:
+                b = (8 if single else 16) << n
+                if used + b > self.budget:
+                    n -= 1
+                    continue
+                q = Q.dgq_createQuregF32(n, self.env) if single else Q.createQureg(n, self.env)
+                regs.append(q)
+                used += b
+        finally:
+            for q in regs:
+                Q.destroyQureg(q, self.env)
+        return used
 
     def serve(self, requests, realtime=True):
         """Runs the stream; returns results in request order. With realtime,

@@ -62,6 +62,13 @@ typedef struct dgq_plan_stats {
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
+/* Stops the library's background kernel compiles (specialisation policy 1)
+ * and joins their threads. Call it before the process exits (the Python
+ * binding does, from its exit hook): process teardown destroys NVRTC's
+ * state in an order a compile still running on another thread cannot
+ * survive. Registers stay usable; later plans compile in the foreground. */
+void dgq_shutdown(void);
+
 /* Cost model of the tile-width choice (the recast of dgQuEST's time
  * predictor and its predict_data.txt calibration, time_predictor.cpp:397-476):
  * a plan costs sweepMs per sweep plus phaseMs per register phase, per 2^30

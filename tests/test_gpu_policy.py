@@ -52,3 +52,27 @@ def test_cached_only_policy(quest, env, single):
     finally:
         Q.dgq_setSpecialisationPolicy(prev)
         Q.dgq_setSpecialisationMinBits(-1 if prev_bits == 22 else prev_bits)
+
+
+def test_exit_with_background_compiles_in_flight(quest):
+    """A process that exits while background compiles are still queued or
+    running (specialisation policy 1) ends cleanly: the binding's exit hook
+    stops and joins the compile threads before process teardown."""
+    import subprocess
+    import sys
+    code = """
+import sys
+sys.path.insert(0, %r)
+from dgquest_b200 import quest as Q, circuits as C
+env = Q.createQuESTEnv()
+Q.dgq_setSpecialisationPolicy(1)
+for i in range(6):
+    q = Q.createQureg(23, env)
+    C.replay(q, C.random_layers(23, 6, 4000 + i))
+    Q.getAmp(q, 0)
+    Q.destroyQureg(q, env)
+print("ok")
+""" % (str(__import__("pathlib").Path(__file__).resolve().parents[1]),)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().endswith("ok")
