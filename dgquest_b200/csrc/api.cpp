@@ -566,10 +566,13 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     // amplitudes per slot, packed FP32 arithmetic) when specialised, unless a
     // sweep cannot be encoded that way (a multi-qubit unitary on address bit 0)
     const bool pairedOk = wantJit && s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
-    // policy 1 still compiles for registers of >= 2^28 amplitudes: their
-    // sweeps take longer than a compile, and the interpreting kernel runs
-    // them 2-3x slower than specialised code
-    const bool cachedOnly = specialise && wantJit && g_specPolicy.load() == 1 && s.numBits < 28;
+    // policy 1 compiles first only for registers of >= 2^34 amplitudes (more
+    // than HBM holds in complex64): below that the interpreting kernel, 2-3x
+    // slower than specialised code, still finishes a one-off circuit before
+    // its kernels would have compiled when several requests compile at once
+    // (measured in the serving loop: compiling first, complex64 requests of
+    // 28..33 qubits took 2.8 s on average)
+    const bool cachedOnly = specialise && wantJit && g_specPolicy.load() == 1 && s.numBits < 34;
     // launching while planning: not when the plan may be redone (policy 1
     // falls back to the interpreting kernel when a kernel is missing; the
     // paired form falls back on a multi-qubit unitary on bit 0) nor with dense
