@@ -680,7 +680,7 @@ def run_serving_form(args, world):
            "requests_per_precision": args.serve_requests, "warmup_requests": args.serve_warmup}
     for name, single in (("complex64", True), ("complex128", False)):
         reqs = S.make_requests(args.serve_requests, rate=200.0, single=single)
-        srv = S.Server(env, workers=args.serve_workers)
+        srv = S.Server(env, workers=args.serve_workers, keep_resident=True, spec_policy=args.serve_policy)
         # a running server: memory pool grown, then a warm-up stream of other
         # requests (same distribution, another seed) before the measured one
         srv.prewarm(single)
@@ -689,6 +689,8 @@ def run_serving_form(args, world):
         cold = S.summarize(srv.serve(warm, realtime=True)) if warm else None
         res = srv.serve(reqs, realtime=True)
         st = S.summarize(res)
+        st["registers_reused"] = srv.reused
+        srv.close()
         if cold:
             st["warmup_stream"] = {"requests": cold["requests"], "p50_ms": cold["p50_ms"], "p99_ms": cold["p99_ms"],
                                    "circuits_per_s": cold["circuits_per_s"]}
@@ -718,6 +720,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
     ap.add_argument("--serve-warmup", type=int, default=60, help="requests of the serving warm-up stream")
+    ap.add_argument("--serve-policy", type=int, default=1, choices=[1, 2],
+                    help="specialisation policy of the serving loop (2: no background compiles)")
     ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
     ap.add_argument("--no-tc-blocks", action="store_true", help="skip the dense-block tensor-core run of the grid circuit")
     ap.add_argument("--no-dense", action="store_true")

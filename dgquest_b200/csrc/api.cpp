@@ -566,13 +566,15 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     // amplitudes per slot, packed FP32 arithmetic) when specialised, unless a
     // sweep cannot be encoded that way (a multi-qubit unitary on address bit 0)
     const bool pairedOk = wantJit && s.single && s.allowPaired && pairedEnabled() && s.numBits >= 10;
-    // policy 1 compiles first only for registers of >= 2^34 amplitudes (more
-    // than HBM holds in complex64): below that the interpreting kernel, 2-3x
-    // slower than specialised code, still finishes a one-off circuit before
-    // its kernels would have compiled when several requests compile at once
-    // (measured in the serving loop: compiling first, complex64 requests of
-    // 28..33 qubits took 2.8 s on average)
-    const bool cachedOnly = specialise && wantJit && g_specPolicy.load() == 1 && s.numBits < 34;
+    // policies 1 and 2 compile first only for registers of >= 2^32
+    // amplitudes: below that the interpreting kernel, 2-3x slower than
+    // specialised code, finishes a one-off circuit before its kernels would
+    // have compiled while several requests compile at once (measured in the
+    // serving loop: compiling first from 2^28 amplitudes on, complex64
+    // requests of 28..33 qubits took 2.8 s on average); at 2^32 and above
+    // the interpreted sweeps themselves take seconds
+    const int policy = g_specPolicy.load();
+    const bool cachedOnly = specialise && wantJit && policy >= 1 && s.numBits < 32;
     // launching while planning: not when the plan may be redone (policy 1
     // falls back to the interpreting kernel when a kernel is missing; the
     // paired form falls back on a multi-qubit unitary on bit 0) nor with dense
@@ -646,7 +648,7 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
                 which.push_back(i);
             }
         if (cachedOnly && !dgq::jitAllReady(sources)) {
-            dgq::jitCompileInBackground(sources);
+            if (policy == 1) dgq::jitCompileInBackground(sources);
             if (paired || W > dgq::kMaxTileBitsF64) {
                 // the interpreting kernel runs unpaired programs of W <= 12
                 code = build(false, true);
@@ -1058,8 +1060,8 @@ int dgq_sampleOutcomes(Qureg q, int numSamples, uint32_t seed, uint64_t *outcome
 }
 
 int dgq_setSpecialisationPolicy(int policy) {
-    if (policy != 0 && policy != 1) {
-        raise(E_INVALID_ARGUMENT, __func__, "policy must be 0 or 1");
+    if (policy < 0 || policy > 2) {
+        raise(E_INVALID_ARGUMENT, __func__, "policy must be 0, 1 or 2");
         return -1;
     }
     return g_specPolicy.exchange(policy);

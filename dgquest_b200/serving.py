@@ -92,15 +92,21 @@ def state_bytes(r):
     return (8 if r.single else 16) << max(r.n, 9)
 
 
-def run_request(r, env, ops=None):
-    """One request on its own register: samples and <Z> (2 P(q=0) - 1)."""
-    q = Q.dgq_createQuregF32(r.n, env) if r.single else Q.createQureg(r.n, env)
+def run_request(r, env, ops=None, q=None):
+    """One request: samples and <Z> (2 P(q=0) - 1). With q (a register of the
+    request's size and precision, lent by the server) the register is reset
+    to |0...0> and kept; otherwise the request creates and destroys its own."""
+    own = q is None
+    if own:
+        q = Q.dgq_createQuregF32(r.n, env) if r.single else Q.createQureg(r.n, env)
     try:
+        Q.initZeroState(q)
         Q.apply_circuit(q, request_ops(r) if ops is None else ops)
         samples = Q.sample(q, SAMPLES, r.sample_seed)
         expz = np.array([2.0 * Q.calcProbOfOutcome(q, k, 0) - 1.0 for k in r.zq])
     finally:
-        Q.destroyQureg(q, env)
+        if own:
+            Q.destroyQureg(q, env)
     return samples, expz
 
 
@@ -110,14 +116,30 @@ class Server:
     A waiting request is admitted when its state fits in the budget next to
     the states in flight; requests behind one that does not fit may go first
     (first fit in arrival order) until it has been passed over `max_bypass`
-    times, after which nothing else is admitted before it."""
+    times, after which nothing else is admitted before it.
 
-    def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None, cached_kernels_only=True):
+    States stay resident: a finished request's register goes back to an idle
+    set and the next request of the same size and precision reuses it (reset
+    to |0...0>), so requests do not pay for creating and destroying device
+    state under load. Idle registers are destroyed, largest first, when a new
+    register would not fit in the budget beside them."""
+
+    def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None, cached_kernels_only=True,
+                 keep_resident=False, spec_policy=1):
         self.env = env
         # one-off circuit structures run the interpreting kernel instead of
         # waiting for a kernel compile; their kernels compile in the background
         self.cached_kernels_only = cached_kernels_only and runner is None
-        self.runner = runner or (lambda r: run_request(r, env))
+        # 1: kernels of new structures compile in the background for later
+        # requests; 2: nothing is compiled (structures that never repeat)
+        self.spec_policy = spec_policy
+        self.custom_runner = runner
+        self.runner = runner or (lambda r, q=None: run_request(r, env, q=q))
+        self.idle = collections.defaultdict(list)  # (n, single) -> registers
+        self.idle_bytes = 0
+        self.reused = 0
+        # keep_resident: idle registers outlive serve() (until close())
+        self.keep_resident = keep_resident
         self.peak_in_use = 0
         self.peak_in_flight = 0
         if hbm_budget is None:
@@ -148,6 +170,32 @@ class Server:
             for q in regs:
                 Q.destroyQureg(q, self.env)
         return used
+
+    def _take(self, r, in_use):
+        """With the lock held: an idle register for r (or None: create one),
+        and the idle registers to destroy so that a new one fits."""
+        key = (r.n, r.single)
+        if self.idle[key]:
+            self.idle_bytes -= state_bytes(r)
+            self.reused += 1
+            return self.idle[key].pop(), []
+        evict = []
+        # in_use already counts r: keep idle + in_use within the budget
+        order = sorted(((n, single) for (n, single), regs in self.idle.items() if regs),
+                       key=lambda k: -((8 if k[1] else 16) << max(k[0], 9)))
+        for k in order:
+            while self.idle[k] and self.idle_bytes + in_use > self.budget:
+                evict.append(self.idle[k].pop())
+                self.idle_bytes -= (8 if k[1] else 16) << max(k[0], 9)
+        return None, evict
+
+    def close(self):
+        """Destroys the idle registers."""
+        for regs in self.idle.values():
+            for q in regs:
+                Q.destroyQureg(q, self.env)
+        self.idle.clear()
+        self.idle_bytes = 0
 
     def serve(self, requests, realtime=True):
         """Runs the stream; returns results in request order. With realtime,
@@ -204,21 +252,36 @@ class Server:
                     self.peak_in_use = max(self.peak_in_use, state["in_use"])
                     self.peak_in_flight = max(self.peak_in_flight, state["in_flight"])
                     admitted = now()
+                    q, evict = None, []
+                    if self.custom_runner is None:
+                        q, evict = self._take(r, state["in_use"])
                 try:
-                    samples, expz = self.runner(r)
+                    for e in evict:
+                        Q.destroyQureg(e, self.env)
+                    if self.custom_runner is not None:
+                        samples, expz = self.runner(r)
+                    else:
+                        if q is None:
+                            q = Q.dgq_createQuregF32(r.n, self.env) if r.single else Q.createQureg(r.n, self.env)
+                        samples, expz = self.runner(r, q)
                 except Exception as exc:  # noqa: BLE001
+                    if q is not None:
+                        Q.destroyQureg(q, self.env)
                     with cond:
                         state["error"] = exc
                         cond.notify_all()
                     return
                 with cond:
+                    if q is not None:
+                        self.idle[(r.n, r.single)].append(q)
+                        self.idle_bytes += state_bytes(r)
                     state["in_use"] -= state_bytes(r)
                     state["in_flight"] -= 1
                     state["finished"] += 1
                     results[r.rid] = Result(r.rid, samples, expz, r.arrival, admitted, now())
                     cond.notify_all()
 
-        prev_policy = Q.dgq_setSpecialisationPolicy(1) if self.cached_kernels_only else None
+        prev_policy = Q.dgq_setSpecialisationPolicy(self.spec_policy) if self.cached_kernels_only else None
         feeder = threading.Thread(target=arrivals, daemon=True)
         pool = [threading.Thread(target=worker, daemon=True) for _ in range(self.workers)]
         feeder.start()
@@ -229,6 +292,8 @@ class Server:
             t.join()
         if prev_policy is not None:
             Q.dgq_setSpecialisationPolicy(prev_policy)
+        if not self.keep_resident:
+            self.close()
         if state["error"] is not None:
             raise state["error"]
         return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]

@@ -184,8 +184,9 @@ int dgq_setSpecialisationMinBits(int minBits);
  * running. 1: a plan runs specialised only if its kernels are compiled
  * already; otherwise it runs the interpreting kernel while its kernels
  * compile on background host threads for later plans of the same structure
- * (for serving one-off circuits); registers of >= 34 address bits still
- * compile first. Returns the previous policy. */
+ * (for serving one-off circuits); registers of >= 32 address bits still
+ * compile first. 2: as 1 without the background compiles (a stream of
+ * circuits whose structures do not repeat). Returns the previous policy. */
 int dgq_setSpecialisationPolicy(int policy);
 /* multiQubitUnitary with 6 targets on a complex64 register of >= 12 qubits
  * runs on the tensor cores (tcgen05, 3xTF32 split, FP32 accumulation) when

@@ -69,3 +69,22 @@ def test_head_of_line_request_is_not_starved():
     assert len(out) == 40
     admitted_order = sorted(out, key=lambda r: r.admitted)
     assert [r.rid for r in admitted_order].index(0) <= 3 + 1
+
+
+def test_idle_registers_reused_and_evicted_largest_first():
+    """Resident registers: a request reuses an idle register of its size and
+    precision; a request that needs a new register evicts idle ones, largest
+    first, until the new one fits beside them (host logic only)."""
+    budget = (16 << 20) + (16 << 18) + (8 << 18)
+    srv = S.Server(env=None, hbm_budget=budget, workers=2, runner=lambda r: (None, None))
+    mk = lambda n, single: S.Request(0, "bv", n, 0, 1, 0.0, (0,), 2, single)  # noqa: E731
+    srv.idle[(20, False)].append("reg20")
+    srv.idle[(18, False)].append("reg18")
+    srv.idle[(18, True)].append("reg18f")
+    srv.idle_bytes = (16 << 20) + (16 << 18) + (8 << 18)
+    q, ev = srv._take(mk(18, False), in_use=16 << 18)
+    assert q == "reg18" and ev == [] and srv.reused == 1
+    # a new 19-qubit complex128 register: the 20-qubit idle one goes first
+    q, ev = srv._take(mk(19, False), in_use=(16 << 18) + (16 << 19))
+    assert q is None and ev == ["reg20"]
+    assert srv.idle_bytes == 8 << 18
