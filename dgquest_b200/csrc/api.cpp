@@ -109,11 +109,12 @@ const char *errorMessage(int code) {
     }
 }
 
-std::mutex g_errMutex;
-int g_errMode = DGQ_ERRORS_EXIT;
-int g_lastError = 0;
-std::string g_lastMessage;
-std::atomic<int64_t> g_errorCount{0};  // errors raised in record mode
+std::atomic<int> g_errMode{DGQ_ERRORS_EXIT};
+// the last recorded error is per thread: registers driven from several host
+// threads (the serving loop) each see the errors of their own calls
+thread_local int g_lastError = 0;
+thread_local std::string g_lastMessage;
+thread_local int64_t g_errorCount = 0;  // errors raised in record mode by this thread
 std::atomic<int64_t> g_launches{0};
 dgq::Mt19937 g_rng;
 
@@ -127,7 +128,6 @@ bool raise(int code, const char *func, const char *detail = nullptr) {
         fflush(stdout);
         exit(code);
     }
-    std::lock_guard<std::mutex> lk(g_errMutex);
     g_lastError = code;
     g_errorCount++;
     g_lastMessage = msg;
@@ -957,7 +957,7 @@ int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes
     if (count < 0 || (count > 0 && !r)) return raise(E_INVALID_ARGUMENT, __func__, "null records") ? 0 : -1;
     int m = 0;
     for (int i = 0; i < count; i++) {
-        const int64_t before = g_errorCount.load();
+        const int64_t before = g_errorCount;
         const dgq_gate_record &g = r[i];
         const int a = g.q0, b = g.q1;
         const double *p = g.p;
@@ -999,7 +999,7 @@ int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes
             case 23: swapGate(q, a, b); break;
             case 24: {
                 const int o = measure(q, a);
-                if (outcomes && g_errorCount.load() == before) outcomes[m] = o;
+                if (outcomes && g_errorCount == before) outcomes[m] = o;
                 m++;
                 break;
             }
@@ -1011,7 +1011,7 @@ int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes
                 return -1;
             }
         }
-        if (g_errorCount.load() != before) return -1;
+        if (g_errorCount != before) return -1;
     }
     return count;
 }
@@ -1083,7 +1083,6 @@ int64_t dgq_getAvailableMemory(void) {
 }
 
 int dgq_getLastError(char *msg, int len) {
-    std::lock_guard<std::mutex> lk(g_errMutex);
     const int code = g_lastError;
     if (msg && len > 0) {
         std::strncpy(msg, g_lastMessage.c_str(), (size_t) len - 1);

@@ -32,8 +32,9 @@ int dgq_getPrecision(Qureg qureg);
 #define DGQ_ERRORS_EXIT 0
 #define DGQ_ERRORS_RECORD 1
 int dgq_setErrorMode(int mode);
-/* Returns the last error code (0 = none) and clears it; copies the message
- * into msg (if msg != NULL and len > 0). */
+/* Returns the calling thread's last error code (0 = none) and clears it;
+ * copies the message into msg (if msg != NULL and len > 0). Errors are
+ * recorded per host thread. */
 int dgq_getLastError(char *msg, int len);
 
 /* Tile width W (address bits per CTA tile, 9..12) used for this register.

@@ -56,3 +56,20 @@ def test_fit_recovers_rates():
     sweep_ms, phase_ms = CAL.fit(rows, 26)
     assert abs(sweep_ms - 2.5) < 1e-9 and abs(phase_ms - 1.5) < 1e-9
     assert ctypes.sizeof(ctypes.c_double) == 8
+
+
+def test_errors_are_recorded_per_thread(restore_rates):
+    """An error raised on one host thread is reported to that thread only."""
+    import threading
+    lib = Q._library()
+    seen = {}
+
+    def fail():
+        lib.dgq_setCostModel(-1.0, 1.0)  # raw call: the error stays recorded
+        seen["other"] = lib.dgq_getLastError(None, 0)
+
+    t = threading.Thread(target=fail)
+    t.start()
+    t.join()
+    assert seen["other"] != 0
+    assert lib.dgq_getLastError(None, 0) == 0
