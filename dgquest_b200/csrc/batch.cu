@@ -9,6 +9,7 @@
 // the register's expectation slots with one atomic per address bit per CTA.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 
@@ -94,7 +95,7 @@ __device__ __noinline__ void addExpectationSums(double tot, const double (&rs)[4
 
 // One tile of one sweep, run by the first 2^(W-4) threads of the CTA; h is
 // the sweep header staged in shared memory.
-template <class V, int W, bool DENSE>
+template <class V, int W, bool DENSE, bool LEAN>
 __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSweep &h, V *__restrict__ st, uint32_t tile,
                                           V *sm, double *zs) {
     constexpr uint32_t T = 1u << (W - kRegBits);
@@ -163,7 +164,7 @@ __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSwee
                 const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(ops + o));
                 KOp op;
                 memcpy(&op, &raw, sizeof(op));
-                applyOp<V, DENSE>(op, coef, a, loc, tile);
+                applyOp<V, DENSE, LEAN>(op, coef, a, loc, tile);
             }
 #pragma unroll
             for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];
@@ -210,7 +211,7 @@ __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSwee
 // Sweeps [w0, w1) of one register on tile `tile` (one sweep for a tile
 // item, all of them for a whole-register item); each header is copied to
 // shared memory first, so the phase loop holds no header registers.
-template <class V, int W, bool DENSE>
+template <class V, int W, bool DENSE, bool LEAN>
 __device__ __forceinline__ void runSweeps(const BatchArgs &args, const BatchCircuit &C, uint32_t w0, uint32_t w1,
                                        uint32_t tile, V *sm, BatchSweep *hs) {
     constexpr uint32_t T = 1u << (W - kRegBits);
@@ -220,14 +221,15 @@ __device__ __forceinline__ void runSweeps(const BatchArgs &args, const BatchCirc
         uint32_t *dst = reinterpret_cast<uint32_t *>(hs);
         for (uint32_t i = threadIdx.x; i < sizeof(BatchSweep) / 4; i += T) dst[i] = __ldg(src + i);
         groupBarrier(T);
-        sweepTile<V, W, DENSE>(args, *hs, st, tile, sm, w + 1 == C.numSweeps ? args.zsum + C.zOff : nullptr);
+        sweepTile<V, W, DENSE, LEAN>(args, *hs, st, tile, sm, w + 1 == C.numSweeps ? args.zsum + C.zOff : nullptr);
     }
 }
 
 // DENSE: the batch's programs hold dense ops (multi-qubit unitaries of up to
 // 4 targets inside a register phase); without them the kernel is compiled
 // without that case (FP64: no spills instead of 1.3 KB of spill stores).
-template <class V, bool DENSE>
+// LEAN: every op kind is one of kLeanKinds (rotations, CNOT, CZ, phases).
+template <class V, bool DENSE, bool LEAN>
 __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
     batchKernel(const __grid_constant__ BatchArgs args) {
     extern __shared__ __align__(16) unsigned char smRaw[];
@@ -268,10 +270,10 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
             const uint32_t w0 = s == kBatchWhole ? 0u : s, w1 = s == kBatchWhole ? C.numSweeps : s + 1;
             const uint32_t tile = s == kBatchWhole ? 0u : t;
             switch (C.tileBits) {
-                case 9: runSweeps<V, 9, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
-                case 10: runSweeps<V, 10, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
-                case 11: runSweeps<V, 11, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
-                default: runSweeps<V, 12, DENSE>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 9: runSweeps<V, 9, DENSE, LEAN>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 10: runSweeps<V, 10, DENSE, LEAN>(args, C, w0, w1, tile, sm, &sHead); break;
+                case 11: runSweeps<V, 11, DENSE, LEAN>(args, C, w0, w1, tile, sm, &sHead); break;
+                default: runSweeps<V, 12, DENSE, LEAN>(args, C, w0, w1, tile, sm, &sHead); break;
             }
             __threadfence();
         }
@@ -284,41 +286,46 @@ __global__ void __launch_bounds__(1 << (kBatchMaxTileBits - kRegBits), 2)
 // by ctasPerSmV (called before any launch is recorded), so that launches
 // recorded in graphs stay valid whatever tile width later batches use.
 template <class V>
-cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, bool dense, cudaStream_t s) {
+cudaError_t launchBatchV(const BatchArgs &a, int maxTileBits, int grid, int form, cudaStream_t s) {
     const size_t smem = sizeof(V) << maxTileBits;
-    if (dense)
-        batchKernel<V, true><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
+    const int T = 1 << (maxTileBits - kRegBits);
+    if (form == kBatchFormDense)
+        batchKernel<V, true, false><<<grid, T, smem, s>>>(a);
+    else if (form == kBatchFormLean)
+        batchKernel<V, false, true><<<grid, T, smem, s>>>(a);
     else
-        batchKernel<V, false><<<grid, 1 << (maxTileBits - kRegBits), smem, s>>>(a);
+        batchKernel<V, false, false><<<grid, T, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-// Both forms have the same launch bounds and shared memory; the occupancy
-// is the smaller of the two.
-template <class V>
-int ctasPerSmV(int maxTileBits) {
+// All forms have the same launch bounds and shared memory; the occupancy
+// is the smallest of them.
+template <class V, bool DENSE, bool LEAN>
+int ctasPerSmForm(int maxTileBits) {
     const size_t smem = sizeof(V) << maxTileBits;
-    const int smemMax = (int) (sizeof(V) << kBatchMaxTileBits);
-    if (cudaFuncSetAttribute(batchKernel<V, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(batchKernel<V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax) !=
-            cudaSuccess)
+    if (cudaFuncSetAttribute(batchKernel<V, DENSE, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int) (sizeof(V) << kBatchMaxTileBits)) != cudaSuccess)
         return 0;
-    int n0 = 0, n1 = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, batchKernel<V, true>, 1 << (maxTileBits - kRegBits),
-                                                      smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, batchKernel<V, false>, 1 << (maxTileBits - kRegBits),
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<V, DENSE, LEAN>, 1 << (maxTileBits - kRegBits),
                                                       smem) != cudaSuccess)
         return 0;
-    return n0 < n1 ? n0 : n1;
+    return n;
+}
+
+template <class V>
+int ctasPerSmV(int maxTileBits) {
+    const int a = ctasPerSmForm<V, true, false>(maxTileBits), b = ctasPerSmForm<V, false, false>(maxTileBits),
+              c = ctasPerSmForm<V, false, true>(maxTileBits);
+    return std::min(a, std::min(b, c));
 }
 
 }  // namespace
 
-cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, bool dense, cudaStream_t s) {
+cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, int form, cudaStream_t s) {
     if (maxTileBits < kMinTileBits || maxTileBits > kBatchMaxTileBits || grid < 1) return cudaErrorInvalidValue;
-    return single ? launchBatchV<float2>(a, maxTileBits, grid, dense, s)
-                  : launchBatchV<double2>(a, maxTileBits, grid, dense, s);
+    return single ? launchBatchV<float2>(a, maxTileBits, grid, form, s)
+                  : launchBatchV<double2>(a, maxTileBits, grid, form, s);
 }
 
 int batchCtasPerSm(bool single, int maxTileBits) {

@@ -82,8 +82,11 @@ inline uint64_t batchItem(uint32_t c, uint32_t s, uint32_t t) {
 
 // One launch of the persistent batch kernel: grid CTAs of 2^(maxTileBits-4)
 // threads with 2^maxTileBits amplitudes of shared memory.
-// dense: some program holds a dense op (selects the kernel form with that case)
-cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, bool dense, cudaStream_t s);
+// Kernel forms: with the dense-op case (a program holds a dense op), the
+// general form, and the lean form (every op kind is a rotation, CNOT, CZ or
+// phase kind).
+constexpr int kBatchFormDense = 0, kBatchFormGeneral = 1, kBatchFormLean = 2;
+cudaError_t launchBatch(const BatchArgs &a, bool single, int maxTileBits, int grid, int form, cudaStream_t s);
 // CTAs of that kernel resident per SM (0 on error). Also sets the kernel's
 // shared-memory limit: call it before the first launch (and before a launch
 // is recorded into a graph).

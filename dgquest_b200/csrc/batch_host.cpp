@@ -229,8 +229,12 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
     }
     d.numSweeps = (int) sweeps.size();
     d.numCounters = doneOff;
-    bool dense = false;
-    for (const KOp &op : ops) dense = dense || op.kind == dgq::KOP_DENSE;
+    bool dense = false, lean = true;
+    for (const KOp &op : ops) {
+        dense = dense || op.kind == dgq::KOP_DENSE;
+        lean = lean && ((dgq::kLeanKinds >> op.kind) & 1u);
+    }
+    const int form = dense ? dgq::kBatchFormDense : lean ? dgq::kBatchFormLean : dgq::kBatchFormGeneral;
     d.numZ = std::max<uint32_t>(1, zOff);
 
     // work list: largest registers first; registers of several tiles in
@@ -297,7 +301,7 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
     cudaError_t e1 = cudaMemsetAsync(d.counters, 0, d.numCounters * sizeof(uint32_t), stream);
     if (e1 == cudaSuccess) e1 = cudaMemsetAsync(d.zsum, 0, d.numZ * sizeof(double), stream);
     if (e1 == cudaSuccess) e1 = cudaMemsetAsync(d.error, 0, sizeof(uint32_t), stream);
-    if (e1 == cudaSuccess && d.numItems > 0) e1 = dgq::launchBatch(a, single, maxTileBits, d.grid, dense, stream);
+    if (e1 == cudaSuccess && d.numItems > 0) e1 = dgq::launchBatch(a, single, maxTileBits, d.grid, form, stream);
     e = cudaStreamEndCapture(stream, &d.graph);
     if (e1 != cudaSuccess) return e1;
     if (e != cudaSuccess) return e;

@@ -102,7 +102,11 @@ __device__ __forceinline__ void denseApply(V (&a)[kRegs], uint32_t ctrlReg, cons
 // DENSE = false drops the dense-op case (KOP_DENSE), whose 2^k-amplitude
 // temporaries otherwise set the register budget of every other op: callers
 // that know their programs hold no dense op compile without it.
-template <class V, bool DENSE = true>
+// LEAN = true keeps only the kinds of rotation / CNOT / CZ circuits
+// (kLeanKinds, tile_program.h): every case is a path that updates the thread's amplitudes in
+// place, and fewer paths leave the compiler fewer register moves to
+// reconcile after the switch.
+template <class V, bool DENSE = true, bool LEAN = false>
 __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a)[kRegs], uint32_t loc,
                                         uint32_t cta) {
     typedef typename Real<V>::T R;
@@ -110,7 +114,8 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
     const uint32_t cr = op.ctrlReg;
     const double *c = coef + op.coef;
     switch (op.kind) {
-        case KOP_M2R: {
+        case KOP_M2R:
+            if constexpr (LEAN) break; {
             const R m0 = (R) c[0], m1 = (R) c[1], m2 = (R) c[2], m3 = (R) c[3];
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](V &x, V &y) {
                 const V nx = mk<V>(m0 * x.x + m1 * y.x, m0 * x.y + m1 * y.y);
@@ -120,7 +125,8 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }));
             break;
         }
-        case KOP_M2I: {
+        case KOP_M2I:
+            if constexpr (LEAN) break; {
             // [[a, i b], [i c, d]]
             const R m0 = (R) c[0], m1 = (R) c[1], m2 = (R) c[2], m3 = (R) c[3];
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](V &x, V &y) {
@@ -131,7 +137,8 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }));
             break;
         }
-        case KOP_M2C: {
+        case KOP_M2C:
+            if constexpr (LEAN) break; {
             const R u0 = (R) c[0], u1 = (R) c[1], u2 = (R) c[2], u3 = (R) c[3], u4 = (R) c[4], u5 = (R) c[5], u6 = (R) c[6], u7 = (R) c[7];
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](V &x, V &y) {
                 const V nx = mk<V>(u0 * x.x - u1 * x.y + u2 * y.x - u3 * y.y,
@@ -151,6 +158,7 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }));
             break;
         case KOP_Y:
+            if constexpr (LEAN) break;
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](V &x, V &y) {
                 const V t = x;
                 x = mk<V>(y.y, -y.x);
@@ -158,6 +166,7 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }));
             break;
         case KOP_YC:
+            if constexpr (LEAN) break;
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, cr, [&](V &x, V &y) {
                 const V t = x;
                 x = mk<V>(-y.y, y.x);
@@ -168,9 +177,11 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             forAll(a, cr, [&](V &x, int) { x = mk<V>(-x.x, -x.y); });
             break;
         case KOP_MULI:
+            if constexpr (LEAN) break;
             forAll(a, cr, [&](V &x, int) { x = mk<V>(-x.y, x.x); });
             break;
         case KOP_MULNI:
+            if constexpr (LEAN) break;
             forAll(a, cr, [&](V &x, int) { x = mk<V>(x.y, -x.x); });
             break;
         case KOP_PH: {
@@ -244,7 +255,8 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
             }
             break;
         }
-        case KOP_RN1: {
+        case KOP_RN1:
+            if constexpr (LEAN) break; {
             const R pr = (R) c[0], pi = (R) c[1];
             DGQ_DISPATCH_K(op.k, forPairs<K>(a, 0u, [&](V &x, V &y) {
                 const V x0 = x;

@@ -58,6 +58,12 @@ enum KOpKind : uint8_t {
                    // (sqrt X, sqrt Y, sqrt W, ...) divided by their equal diagonal entry
 };
 
+// The op kinds of rotation / CNOT / CZ / phase circuits (the interpreting
+// kernels' lean form handles these only).
+constexpr uint32_t kLeanKinds = (1u << KOP_X) | (1u << KOP_NEG) | (1u << KOP_PH) | (1u << KOP_Z2) |
+                                (1u << KOP_RY1) | (1u << KOP_RY2) | (1u << KOP_RX1) | (1u << KOP_RX2) |
+                                (1u << KOP_H1) | (1u << KOP_PH1);
+
 // Dispatch codes of the tile kernel: one straight-line case per
 // (operation, target register bit, register-control present). Pair
 // operations: base + k (+4 when some control bit is a register bit).
