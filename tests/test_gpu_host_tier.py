@@ -112,3 +112,26 @@ def test_host_tier_unsupported_calls(quest, env, small_budget):
     small = quest.createQureg(16, env)
     assert quest.host_tier_stats(small) is None
     quest.destroyQureg(small, env)
+
+
+def test_host_tier_measurement_mid_circuit(quest, env, small_budget):
+    """Measurements between gate batches: each collapse stays lazy until the
+    next pass, which applies it before any qubit exchange; probabilities of
+    qubits above the page read the collapsed pages only."""
+    n = 18
+    kinds = [k for k in range(C.CY + 1) if k not in (C.SWAP,)]
+    ops = C.mixed_ops(n, 260, 95, kinds=kinds, with_measure=True)
+    quest.seed([7, 8])
+    q = quest.createQureg(n, env)
+    try:
+        out = C.replay(q, ops)
+        amps = quest.state_vector(q)
+        p0 = quest.prob_all_zero(q)
+        _, _, exchanges = quest.host_tier_stats(q)
+    finally:
+        quest.destroyQureg(q, env)
+    ref, ref_p0, ref_out = oracle.run(n, ops, seed_keys=[7, 8])
+    assert out == ref_out
+    assert np.abs(amps - ref).max() <= 1e-12
+    assert np.abs(p0 - ref_p0).max() <= 1e-12
+    assert exchanges >= 1
