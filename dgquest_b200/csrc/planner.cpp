@@ -289,7 +289,7 @@ bool encodeBlock(const BlockPlan &block, int numBits, int numReal, int tileBits,
         while (!dag.empty()) {
             // paired form: address bit 0 is always inside the thread
             u64 mask = paired ? 1ULL : 0ULL;
-            growMask(dag, mask, kRegBits + (paired ? 1 : 0), true);
+            growMask(dag, mask, kRegBits + (paired ? 1 : 0), true, true);
             std::vector<Gate> gs = dag.takeAllowed(mask);
             if (gs.empty()) {
                 // a multi-target gate wider than the register bits
