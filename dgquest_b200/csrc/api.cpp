@@ -1155,15 +1155,24 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
     }
     const size_t avail = freeB + poolSpare() > (64u << 20) ? freeB + poolSpare() - (64u << 20) : 0;
     const int64_t setBudget = g_deviceBudget.load();
-    const size_t budget = setBudget > 0 ? std::min<size_t>(avail, (size_t) setBudget) : avail;
-    if (bytes > budget) {
+    // the host tier serves states beyond a set budget, or beyond what the
+    // device could hold at all; a state that only does not fit next to the
+    // registers alive now is an error (E_SYS_TOO_BIG_FOR_DEVICE), as before
+    const size_t never = totalB > (1ull << 30) ? totalB - (1ull << 30) : totalB;
+    const bool hostTier = setBudget > 0 ? bytes > std::min<size_t>(avail, (size_t) setBudget) : bytes > never;
+    if (hostTier) {
         // the host tier: the state in pinned host memory, paged through HBM
+        const size_t budget = setBudget > 0 ? std::min<size_t>(avail, (size_t) setBudget) : avail;
         std::string err;
         if (!dgq::hostTierAttach(*s, budget, err)) {
             delete s;
             raise(E_SYS_TOO_BIG_FOR_DEVICE, func, err.c_str());
             return q;
         }
+    } else if (bytes > avail) {
+        delete s;
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, func);
+        return q;
     }
     if (!cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func)) {
         dgq::hostTierRelease(*s);

@@ -674,6 +674,20 @@ const Driver &driver() {
     return d;
 }
 
+// Driver calls act on the calling thread's current context. A host thread
+// whose first CUDA work in this library is a module load or a launch of a
+// specialised kernel (a serving worker reusing a register, say) has none
+// yet: bind the runtime's primary context of the current device first
+// (cudaSetDevice makes it current), once per thread.
+bool ensureContext() {
+    thread_local bool bound = false;
+    if (bound) return true;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) return false;
+    bound = true;
+    return true;
+}
+
 struct CacheEntry {
     std::string source;
     CUmodule module;
@@ -906,6 +920,10 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
         if (err) *err = "CUDA driver entry points unavailable";
         return false;
     }
+    if (!todo.empty() && !ensureContext()) {
+        if (err) *err = "no CUDA device context for this thread";
+        return false;
+    }
     for (size_t i : todo) {
         if (!ok[i]) {
             if (err) *err = "NVRTC compile failed: " + logs[i].substr(0, 2000);
@@ -945,6 +963,7 @@ cudaError_t launchJitSweep(CUfunction fn, void *st, int W, const TileProgram &pr
     // one attribute call per function: cheap and idempotent
     const Driver &drv = driver();
     if (!drv.ok) return cudaErrorNotSupported;
+    if (!ensureContext()) return cudaErrorInvalidDevice;
     CUresult r = drv.funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int) smem);
     if (r != CUDA_SUCCESS) return cudaErrorLaunchFailure;
     const unsigned grid = prog.ctaCount ? prog.ctaCount : 1u << (prog.numBits - W);

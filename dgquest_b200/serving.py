@@ -252,12 +252,14 @@ class Server:
                     self.peak_in_use = max(self.peak_in_use, state["in_use"])
                     self.peak_in_flight = max(self.peak_in_flight, state["in_flight"])
                     admitted = now()
-                    q, evict = None, []
+                    q = None
                     if self.custom_runner is None:
                         q, evict = self._take(r, state["in_use"])
+                        # destroyed before the lock is released, so that no
+                        # other worker counts on memory that is not free yet
+                        for e in evict:
+                            Q.destroyQureg(e, self.env)
                 try:
-                    for e in evict:
-                        Q.destroyQureg(e, self.env)
                     if self.custom_runner is not None:
                         samples, expz = self.runner(r)
                     else:

@@ -82,9 +82,9 @@ int dgq_setCostModel(double sweepMsPer2p30, double phaseMsPer2p30);
 int dgq_loadCostModel(const char *path);
 int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30);
 
-/* Host tier. A register whose state is larger than the device budget
- * (free HBM, or the smaller budget set here for registers created later;
- * 0 restores free HBM) keeps its state in pinned host memory in pages of
+/* Host tier. A register whose state is larger than the device's memory (or
+ * than the budget set here for registers created later, capped by free
+ * HBM; 0 restores the default) keeps its state in pinned host memory in pages of
  * 2^pageBits amplitudes and streams the pages through four device buffers
  * (copy in, sweeps, copy out, overlapped on four streams). A gate on a qubit
  * outside the page first exchanges that qubit with a page qubit in a pass

@@ -72,3 +72,31 @@ def test_uncompiled_structure_waits_for_the_plan(quest, env, specialise_small):
         quest.destroyQureg(q, env)
     ref = oracle.run(n, ops)[0]
     assert np.abs(amps - ref).max() <= 1e-12
+
+
+def test_first_cuda_work_of_a_thread_is_a_specialised_launch(quest, env, specialise_small):
+    """A host thread whose first CUDA work is loading and launching a
+    specialised kernel (a register created on another thread) gets the
+    device's primary context bound before the driver calls."""
+    import threading
+    n = 16
+    ops = C.random_layers(n, 6, C.config_seed(2, 886))
+    q = quest.createQureg(n, env)
+    result = {}
+
+    def run():
+        try:
+            C.replay(q, ops)
+            result["amps"] = quest.state_vector(q)
+        except Exception as exc:  # noqa: BLE001
+            result["error"] = exc
+
+    try:
+        t = threading.Thread(target=run)
+        t.start()
+        t.join()
+    finally:
+        quest.destroyQureg(q, env)
+    assert "error" not in result, result.get("error")
+    ref = oracle.run(n, ops)[0]
+    assert np.abs(result["amps"] - ref).max() <= 1e-12
