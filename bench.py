@@ -689,6 +689,14 @@ def run_serving_form(args, world):
         cold = S.summarize(srv.serve(warm, realtime=True)) if warm else None
         res = srv.serve(reqs, realtime=True)
         st = S.summarize(res)
+        if args.serve_low_rate > 0:
+            # the same server below its capacity: latency is service time, not queueing
+            low = S.make_requests(args.serve_low_requests, rate=args.serve_low_rate, single=single,
+                                  seed=C.config_seed(5, 910000), first_id=300000)
+            lo = S.summarize(srv.serve(low, realtime=True))
+            st["below_capacity"] = {"offered_rate": args.serve_low_rate, "requests": lo["requests"],
+                                    "p50_ms": lo["p50_ms"], "p99_ms": lo["p99_ms"],
+                                    "circuits_per_s": lo["circuits_per_s"]}
         st["registers_reused"] = srv.reused
         srv.close()
         if cold:
@@ -720,6 +728,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
     ap.add_argument("--serve-warmup", type=int, default=60, help="requests of the serving warm-up stream")
+    ap.add_argument("--serve-low-rate", type=float, default=4.0,
+                    help="arrival rate (req/s) of a second, below-capacity serving stream (0: skip)")
+    ap.add_argument("--serve-low-requests", type=int, default=40)
     ap.add_argument("--serve-policy", type=int, default=1, choices=[1, 2],
                     help="specialisation policy of the serving loop (2: no background compiles)")
     ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
