@@ -651,7 +651,6 @@ struct Driver {
     CUresult (*launchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                              CUstream, void **, void **) = nullptr;
     CUresult (*getErrorString)(CUresult, const char **) = nullptr;
-    CUresult (*occupancy)(int *, CUfunction, int, size_t) = nullptr;
     bool ok = false;
 };
 
@@ -668,8 +667,7 @@ const Driver &driver() {
                get("cuModuleGetFunction", (void **) &d.moduleGetFunction) &&
                get("cuFuncSetAttribute", (void **) &d.funcSetAttribute) &&
                get("cuLaunchKernel", (void **) &d.launchKernel) &&
-               get("cuGetErrorString", (void **) &d.getErrorString) &&
-               get("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void **) &d.occupancy);
+               get("cuGetErrorString", (void **) &d.getErrorString);
     });
     return d;
 }
