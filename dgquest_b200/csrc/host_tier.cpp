@@ -42,13 +42,14 @@ bool raiseExternal(int code, const char *func, const char *detail);
 namespace {
 
 constexpr int kErrUnsupported = 102;  // E_UNSUPPORTED
+constexpr int kErrCuda = 103;         // E_CUDA
 constexpr int kMinPageBits = 14;      // holds a paired complex64 tile (W <= 13) and more
 
 size_t ampBytesOf(const QuregState &s) { return s.single ? sizeof(float2) : sizeof(double2); }
 
 bool ok(cudaError_t e, const char *func) {
     if (e == cudaSuccess) return true;
-    return raiseExternal(kErrUnsupported, func, cudaGetErrorString(e));
+    return raiseExternal(kErrCuda, func, cudaGetErrorString(e));
 }
 
 char *hostPage(const QuregState &s, uint64_t page) {
