@@ -428,12 +428,7 @@ def run_host_tier_form(args, world):
         Q.getAmp(q, 0)
         dt = time.perf_counter() - t0
     p1 = Q.host_tier_stats(q)
-    passes, exchanges = p1[1] - p0[1], p1[2] - p0[2]
-    page_bytes = 16 << out["page_bits"]
-    pages = 1 << (n - out["page_bits"])
-    # sweep passes copy every page in and out (the first writes without
-    # reading); exchange passes do both for every page
-    moved = (2 * passes - 1) * pages * page_bytes + 2 * exchanges * pages * page_bytes
+    passes, exchanges, moved = p1[1] - p0[1], p1[2] - p0[2], p1[3] - p0[3]
     out.update({"ms_per_circuit": dt * 1e3, "page_passes": int(passes), "qubit_exchanges": int(exchanges),
                 "host_device_bytes": int(moved), "host_device_gbs": moved / dt / 1e9,
                 "vs_hbm": dt * 1e3 / out["hbm_ms"]})

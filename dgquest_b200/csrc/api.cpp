@@ -1940,12 +1940,13 @@ void dgq_shutdown(void) { dgq::jitStopBackground(); }
 
 int64_t dgq_setDeviceBudget(int64_t bytes) { return g_deviceBudget.exchange(bytes > 0 ? bytes : 0); }
 
-int dgq_getHostTierStats(Qureg q, int *pageBits, int64_t *passes, int64_t *exchanges) {
+int dgq_getHostTierStats(Qureg q, int *pageBits, int64_t *passes, int64_t *exchanges, int64_t *bytesMoved) {
     if (!vQureg(q, __func__)) return -1;
     const QuregState &s = *stateOf(q);
     if (pageBits) *pageBits = s.hostTier ? s.pageBits : 0;
     if (passes) *passes = s.hostTierPasses;
     if (exchanges) *exchanges = s.hostTierSwaps;
+    if (bytesMoved) *bytesMoved = s.hostTierBytes;
     return s.hostTier ? 1 : 0;
 }
 

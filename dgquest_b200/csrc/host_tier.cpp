@@ -132,15 +132,38 @@ bool pageLocal(const TileProgram &p, int W, int pageBits, int numBits) {
     return true;
 }
 
+// Checks that every planned sweep stays inside its page.
+bool planIsPageLocal(const QuregState &s, const char *func) {
+    for (const TileProgram &p : s.planned)
+        if (!pageLocal(p, s.plannedTileBits, s.pageBits, s.numBits))
+            return raiseExternal(kErrUnsupported, func, "internal: a sweep of the host tier reaches outside its page");
+    return true;
+}
+
+// Launches s.planned on page `page`, held in device buffer b, on stream st.
+bool launchPlanOnPage(QuregState &s, uint64_t page, int b, cudaStream_t st, const char *func) {
+    const int W = s.plannedTileBits;
+    const uint32_t ctas = 1u << (s.pageBits - W);
+    // global index (page << pageBits) | i lands on buffer element i
+    const uintptr_t base =
+        reinterpret_cast<uintptr_t>(s.dPage[b]) - (uintptr_t) ((page << s.pageBits) * ampBytesOf(s));
+    void *rebased = reinterpret_cast<void *>(base);
+    for (size_t i = 0; i < s.planned.size(); i++) {
+        TileProgram p = s.planned[i];
+        p.ctaOffset = (uint32_t) page * ctas;
+        p.ctaCount = ctas;
+        const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+        const cudaError_t e = fn ? launchJitSweep(fn, rebased, W, p, st) : launchTile(rebased, s.single, W, p, st);
+        if (!ok(e, func)) return false;
+    }
+    return true;
+}
+
 // Runs s.planned on every page: copy in (unless the first sweep writes the
 // whole page), the plan's sweeps, copy out.
 bool runPagePass(QuregState &s, const char *func) {
-    const int W = s.plannedTileBits;
-    for (const TileProgram &p : s.planned)
-        if (!pageLocal(p, W, s.pageBits, s.numBits))
-            return raiseExternal(kErrUnsupported, func, "internal: a sweep of the host tier reaches outside its page");
+    if (!planIsPageLocal(s, func)) return false;
     const uint64_t pages = 1ULL << (s.numBits - s.pageBits);
-    const uint32_t ctas = 1u << (s.pageBits - W);
     const size_t pageBytes = ampBytesOf(s) << s.pageBits;
     const bool load = s.planned.empty() || s.planned[0].initKind == INIT_NONE;
     for (uint64_t page = 0; page < pages; page++) {
@@ -148,27 +171,20 @@ bool runPagePass(QuregState &s, const char *func) {
         cudaStream_t st = s.pageStream[b];
         if (load && !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, page), pageBytes, cudaMemcpyHostToDevice, st), func))
             return false;
-        // global index (page << pageBits) | i lands on buffer element i
-        const uintptr_t base = reinterpret_cast<uintptr_t>(s.dPage[b]) - (uintptr_t) ((page << s.pageBits) * ampBytesOf(s));
-        void *rebased = reinterpret_cast<void *>(base);
-        for (size_t i = 0; i < s.planned.size(); i++) {
-            TileProgram p = s.planned[i];
-            p.ctaOffset = (uint32_t) page * ctas;
-            p.ctaCount = ctas;
-            const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
-            const cudaError_t e =
-                fn ? launchJitSweep(fn, rebased, W, p, st) : launchTile(rebased, s.single, W, p, st);
-            if (!ok(e, func)) return false;
-        }
-        if (!ok(cudaMemcpyAsync(hostPage(s, page), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
+        if (!launchPlanOnPage(s, page, b, st, func) ||
+            !ok(cudaMemcpyAsync(hostPage(s, page), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
             return false;
+        s.hostTierBytes += (load ? 2 : 1) * pageBytes;
     }
     s.hostTierPasses++;
     return hostTierSync(s, func);
 }
 
-// Exchanges page-index bit h with page bit l over all page pairs.
-bool runSwapPass(QuregState &s, int h, int l, const char *func) {
+// Exchanges page-index bit h with page bit l over all page pairs; with
+// thenPlan, each pair then runs s.planned (the next segment, planned in the
+// exchanged bits) before it goes back, saving that segment a pass of its own.
+bool runSwapPass(QuregState &s, int h, int l, bool thenPlan, const char *func) {
+    if (thenPlan && !planIsPageLocal(s, func)) return false;
     const uint64_t pages = 1ULL << (s.numBits - s.pageBits);
     const uint64_t hb = 1ULL << (h - s.pageBits);
     const size_t pageBytes = ampBytesOf(s) << s.pageBits;
@@ -180,13 +196,18 @@ bool runSwapPass(QuregState &s, int h, int l, const char *func) {
         cudaStream_t st = s.pageStream[a];
         if (!ok(cudaMemcpyAsync(s.dPage[a], hostPage(s, p0), pageBytes, cudaMemcpyHostToDevice, st), func) ||
             !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, p1), pageBytes, cudaMemcpyHostToDevice, st), func) ||
-            !ok(launchPageSwap(s.dPage[a], s.dPage[b], s.single, s.pageBits, l, st), func) ||
-            !ok(cudaMemcpyAsync(hostPage(s, p0), s.dPage[a], pageBytes, cudaMemcpyDeviceToHost, st), func) ||
+            !ok(launchPageSwap(s.dPage[a], s.dPage[b], s.single, s.pageBits, l, st), func))
+            return false;
+        if (thenPlan && (!launchPlanOnPage(s, p0, a, st, func) || !launchPlanOnPage(s, p1, b, st, func)))
+            return false;
+        if (!ok(cudaMemcpyAsync(hostPage(s, p0), s.dPage[a], pageBytes, cudaMemcpyDeviceToHost, st), func) ||
             !ok(cudaMemcpyAsync(hostPage(s, p1), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
             return false;
+        s.hostTierBytes += 4 * pageBytes;
         pair++;
     }
     if (!hostTierSync(s, func)) return false;
+    if (thenPlan) s.hostTierPasses++;
     // the qubits at virtual bits h and l trade places
     const int qa = s.v2l[h], qb = s.v2l[l];
     s.v2l[h] = qb;
@@ -261,20 +282,32 @@ bool hostTierFlush(QuregState &s, const char *func) {
                                  "a multi-qubit unitary of more than 4 targets on a register in host memory");
     std::vector<Segment> segs = cutSegments(s.pending, s.pageBits);
     const MatrixPool pool = s.pool;
-    const bool denseFusion = s.denseFusion;
+    const int denseFusion = s.denseFusion;
     s.denseFusion = 0;
     bool good = true;
+    bool ranWithExchange = false;  // segment k ran fused with the exchange before it
     for (size_t k = 0; k < segs.size() && good; k++) {
         // the first segment carries the pending initialisation or collapse
         // (a header-only pass when it holds no gates)
         const bool header = k == 0 && (s.initPending || s.restrictActive);
-        if (!segs[k].gates.empty() || header) {
+        if (!ranWithExchange && (!segs[k].gates.empty() || header)) {
             s.pending = segs[k].gates;
             s.pool = pool;
             good = planForPages(s, func) && runPagePass(s, func);
         }
-        for (const auto &sw : segs[k].swapsAfter)
-            if (good) good = runSwapPass(s, sw.first, sw.second, func);
+        ranWithExchange = false;
+        const auto &sw = segs[k].swapsAfter;
+        for (size_t i = 0; i < sw.size() && good; i++) {
+            // the last exchange before a segment runs that segment too
+            const bool fuse = i + 1 == sw.size() && k + 1 < segs.size() && !segs[k + 1].gates.empty();
+            if (fuse) {
+                s.pending = segs[k + 1].gates;
+                s.pool = pool;
+                good = planForPages(s, func);
+            }
+            if (good) good = runSwapPass(s, sw[i].first, sw[i].second, fuse, func);
+            ranWithExchange = fuse;
+        }
     }
     s.denseFusion = denseFusion;
     s.pending.clear();
@@ -327,6 +360,7 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
     }
     if (!hostTierSync(s, func)) return false;
     s.hostTierPasses++;
+    for (uint64_t page = 0; page < pages; page++) s.hostTierBytes += used[page] ? pageBytes : 0;
     p0.assign((size_t) s.numBits, 0.0);
     total = 0.0;
     for (uint64_t page = 0; page < pages; page++) {

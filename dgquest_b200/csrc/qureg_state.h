@@ -79,6 +79,7 @@ struct QuregState {
     size_t pagePartialCap = 0;
     int64_t hostTierSwaps = 0;   // page-pair exchange passes run so far
     int64_t hostTierPasses = 0;  // page passes (sweep segments and read-outs) run so far
+    int64_t hostTierBytes = 0;   // bytes copied between host and device so far
 };
 
 namespace dgq {

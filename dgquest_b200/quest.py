@@ -185,7 +185,7 @@ _SIGS = {
     "dgq_setCostModel": (I, [D, D]),
     "dgq_loadCostModel": (I, [ctypes.c_char_p]),
     "dgq_getCostModel": (I, [P(D), P(D)]),
-    "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64)]),
+    "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
     "dgq_launchPlanned": (I, [Q]),
     "dgq_sync": (I, [Q]),
     "dgq_getStream": (c_void_p, [Q]),
@@ -315,13 +315,14 @@ def plan_stats(q):
 
 
 def host_tier_stats(q):
-    """(page bits, page passes, qubit exchanges) of a host-tier register, or
-    None for a register in HBM."""
+    """(page bits, page passes, qubit exchanges, host<->device bytes) of a
+    host-tier register, or None for a register in HBM."""
     pb = ctypes.c_int(0)
     passes = ctypes.c_int64(0)
     ex = ctypes.c_int64(0)
-    r = dgq_getHostTierStats(q, ctypes.byref(pb), ctypes.byref(passes), ctypes.byref(ex))
-    return (pb.value, passes.value, ex.value) if r == 1 else None
+    moved = ctypes.c_int64(0)
+    r = dgq_getHostTierStats(q, ctypes.byref(pb), ctypes.byref(passes), ctypes.byref(ex), ctypes.byref(moved))
+    return (pb.value, passes.value, ex.value, moved.value) if r == 1 else None
 
 
 def seed(keys):

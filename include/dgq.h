@@ -93,9 +93,10 @@ int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30);
  * products, batches and the plan/launch split report E_UNSUPPORTED for
  * such registers. Returns the previous budget. */
 int64_t dgq_setDeviceBudget(int64_t bytes);
-/* 1 for a host-tier register (with its page width, page passes and qubit
- * exchanges so far), 0 for a register in HBM, -1 on error. */
-int dgq_getHostTierStats(Qureg qureg, int *pageBits, int64_t *passes, int64_t *exchanges);
+/* 1 for a host-tier register (with its page width, page passes, qubit
+ * exchanges and host<->device bytes so far; an exchange that also runs the
+ * next segment counts as a pass too), 0 for a register in HBM, -1 on error. */
+int dgq_getHostTierStats(Qureg qureg, int *pageBits, int64_t *passes, int64_t *exchanges, int64_t *bytesMoved);
 
 /* Dense-block form. qubits = 5, 6 or 7: the register's gates are fused into
  * dense unitaries on that many qubits (dgQuEST's greedy block rule,

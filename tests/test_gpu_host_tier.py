@@ -40,21 +40,21 @@ def test_host_tier_matches_oracle(quest, env, small_budget, kernels, kind):
            "mixed": lambda: C.mixed_ops(n, 400, 91)}[kind]()
     q = quest.createQureg(n, env)
     try:
-        pb, _, _ = quest.host_tier_stats(q)
+        pb, _, _, _ = quest.host_tier_stats(q)
         assert pb == 14
         quest.initZeroState(q)
         C.replay(q, ops)
         amps = quest.state_vector(q)
         p0 = quest.prob_all_zero(q)
         total = quest.calcTotalProb(q)
-        _, passes, exchanges = quest.host_tier_stats(q)
+        _, passes, exchanges, moved = quest.host_tier_stats(q)
     finally:
         quest.destroyQureg(q, env)
     ref, ref_p0, _ = oracle.run(n, ops)
     assert np.abs(amps - ref).max() <= 1e-12
     assert np.abs(p0 - ref_p0).max() <= 1e-12
     assert abs(total - 1.0) <= 1e-12
-    assert passes >= 2
+    assert passes >= 2 and moved > 0
     if kind != "ghzqft":
         assert exchanges >= 1  # gates on the qubits above the page
 
@@ -127,7 +127,7 @@ def test_host_tier_measurement_mid_circuit(quest, env, small_budget):
         out = C.replay(q, ops)
         amps = quest.state_vector(q)
         p0 = quest.prob_all_zero(q)
-        _, _, exchanges = quest.host_tier_stats(q)
+        _, _, exchanges, _ = quest.host_tier_stats(q)
     finally:
         quest.destroyQureg(q, env)
     ref, ref_p0, ref_out = oracle.run(n, ops, seed_keys=[7, 8])
