@@ -81,10 +81,20 @@ struct Segment {
 };
 
 // Cuts the gates into page-local segments; the gates after each exchange
-// are rewritten in the exchanged bits.
+// are rewritten in the exchanged bits. uses[b] lists, in order, the gates
+// whose non-diagonal targets include address bit b (in the rewritten bits),
+// so the next use of a bit is one binary search.
 std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
     std::vector<Segment> segs(1);
     const u64 local = (1ULL << pageBits) - 1;
+    std::vector<std::vector<size_t>> uses(64);
+    for (size_t j = 0; j < g.size(); j++)
+        for (u64 m = nonDiagonal(g[j]); m; m &= m - 1) uses[(size_t) __builtin_ctzll(m)].push_back(j);
+    auto nextUse = [&](int b, size_t from) {
+        const auto &u = uses[(size_t) b];
+        const auto it = std::lower_bound(u.begin(), u.end(), from);
+        return it == u.end() ? g.size() : *it;
+    };
     for (size_t i = 0; i < g.size(); i++) {
         const u64 glob = nonDiagonal(g[i]) & ~local;
         if (glob) {
@@ -95,12 +105,7 @@ std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
                 size_t victimNext = 0;
                 for (int l = pageBits - 1; l >= 0; l--) {
                     if ((taken >> l) & 1ULL) continue;
-                    size_t next = g.size();
-                    for (size_t j = i; j < g.size(); j++)
-                        if ((nonDiagonal(g[j]) >> l) & 1ULL) {
-                            next = j;
-                            break;
-                        }
+                    const size_t next = nextUse(l, i);
                     if (victim < 0 || next > victimNext) {
                         victim = l;
                         victimNext = next;
@@ -109,6 +114,16 @@ std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
                 taken |= 1ULL << victim;
                 segs.back().swapsAfter.emplace_back(h, victim);
                 for (size_t j = i; j < g.size(); j++) swapBitsOf(g[j], h, victim);
+                // from gate i on, bits h and victim trade their uses
+                auto &uh = uses[(size_t) h];
+                auto &ul = uses[(size_t) victim];
+                const auto ih = std::lower_bound(uh.begin(), uh.end(), i) - uh.begin();
+                const auto il = std::lower_bound(ul.begin(), ul.end(), i) - ul.begin();
+                std::vector<size_t> th(uh.begin() + ih, uh.end()), tl(ul.begin() + il, ul.end());
+                uh.resize((size_t) ih);
+                ul.resize((size_t) il);
+                uh.insert(uh.end(), tl.begin(), tl.end());
+                ul.insert(ul.end(), th.begin(), th.end());
             }
             segs.emplace_back();
         }
