@@ -442,6 +442,52 @@ def run_host_tier_form(args, world):
     return out
 
 
+def run_sharded_form(args, world):
+    """Sharded register: the 30-qubit depth-20 random circuit (complex128) in
+    8 shards of 2 GiB, all on this GPU (on several GPUs the exchange kernels
+    reach the partner shard through peer memory instead), against the same
+    circuit in one HBM buffer. Wall time of initZeroState + gates + getAmp;
+    exchange bytes are half of every shard in each direction per exchange."""
+    from dgquest_b200 import circuits as C
+    from dgquest_b200 import quest as Q
+    n, depth, shard_bits = 30, 20, 3
+    ops = C.random_layers(n, depth, C.config_seed(2))
+    env = Q.createQuESTEnv()
+    out = {"workload": f"random circuit n={n} depth={depth}, complex128, {1 << shard_bits} shards on one GPU",
+           "qubits": n, "depth": depth, "shards": 1 << shard_bits}
+    idx = np.random.RandomState(6).randint(0, 1 << n, size=1024)
+
+    def timed(q):
+        for _ in range(2):
+            t0 = time.perf_counter()
+            Q.initZeroState(q)
+            C.replay(q, ops)
+            Q.getAmp(q, 0)
+            dt = time.perf_counter() - t0
+        return dt
+
+    q = Q.createQureg(n, env)
+    out["hbm_ms"] = timed(q) * 1e3
+    ref = [Q.getAmp(q, int(i)) for i in idx]
+    Q.destroyQureg(q, env)
+    q = Q.create_sharded(n, env, shard_bits)
+    p0 = Q.shard_stats(q)
+    dt = timed(q)
+    p1 = Q.shard_stats(q)
+    # the second of the two timed runs
+    passes, exchanges, moved = [(b - a) // 2 for a, b in zip(p0[1:], p1[1:])]
+    out.update({"ms_per_circuit": dt * 1e3, "shard_passes": int(passes), "qubit_exchanges": int(exchanges),
+                "bytes_between_shards": int(moved), "vs_hbm": dt * 1e3 / out["hbm_ms"]})
+    err = 0.0
+    for i, a in zip(idx, ref):
+        b = Q.getAmp(q, int(i))
+        err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
+    out["max_abs_err_vs_hbm_sampled"] = err
+    Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+    return out
+
+
 def run_dense_form(args, world):
     """Dense 6-qubit blocks: multiQubitUnitary with 6 targets on a 30-qubit
     register, complex64 on the tensor cores (tcgen05, 3xTF32) and on the SIMT
@@ -729,6 +775,7 @@ def main():
     ap.add_argument("--serve-policy", type=int, default=1, choices=[1, 2],
                     help="specialisation policy of the serving loop (2: no background compiles)")
     ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
+    ap.add_argument("--no-shards", action="store_true", help="skip the sharded-register run")
     ap.add_argument("--no-tc-blocks", action="store_true", help="skip the dense-block tensor-core run of the grid circuit")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--dense-qubits", type=int, default=30)
@@ -761,6 +808,8 @@ def main():
             line["dense_blocks"] = dense
     if not args.no_host_tier and rank == 0 and world == 1:
         line["host_tier"] = run_host_tier_form(args, world)
+    if not args.no_shards and rank == 0 and world == 1:
+        line["sharded"] = run_sharded_form(args, world)
     if not args.no_grid32:
         grid = run_precision_form(args, world)
         if rank == 0:

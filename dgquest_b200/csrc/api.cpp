@@ -533,9 +533,9 @@ bool launchPlanned(QuregState &s, const char *func, size_t from = 0) {
 void setRenorm(QuregState &s, size_t i, size_t last, int &event) {
     dgq::TileProgram &p = s.planned[i];
     p.isSingle = s.single ? 1 : 0;
-    // (a register in host memory runs each sweep page by page: no sweep sees
-    // the whole output's norm before the next one starts)
-    if (!s.single || s.hostTier) return;
+    // (a register in host memory or in shards runs each sweep page by page:
+    // no sweep sees the whole output's norm before the next one starts)
+    if (!s.single || s.hostTier || s.sharded) return;
     const dgq::TileProgram *prev = i > 0 ? &s.planned[i - 1] : nullptr;
     if (prev && prev->renormOut) {
         p.renormIn = 1;
@@ -746,12 +746,13 @@ void freeOn(void *ptr, cudaStream_t st) {
 
 bool flush(QuregState &s, const char *func) {
     if (s.pending.empty() && !s.initPending) return true;
-    if (s.hostTier) return dgq::hostTierFlush(s, func);
+    if (s.hostTier || s.sharded) return dgq::hostTierFlush(s, func);
     return planPending(s, func, true, true);
 }
 
 // Entry points that need the state in HBM.
 bool vDeviceResident(const QuregState &s, const char *func) {
+    if (s.sharded) return raise(E_UNSUPPORTED, func, "not available for a sharded register");
     if (!s.hostTier) return true;
     return raise(E_UNSUPPORTED, func, "not available for a register held in host memory (larger than the device budget)");
 }
@@ -759,7 +760,7 @@ bool vDeviceResident(const QuregState &s, const char *func) {
 bool ensureProbs(QuregState &s, const char *func) {
     if (s.probsValid) return true;
     if (!flush(s, func)) return false;
-    if (s.hostTier) {
+    if (s.hostTier || s.sharded) {
         std::vector<double> p0;
         double total = 0.0;
         if (!dgq::hostTierProbs(s, p0, total, func)) return false;
@@ -902,7 +903,7 @@ bool normaliseLayout(QuregState &s, const char *func) {
         s.pending.push_back(g);
     }
     if (!flush(s, func)) return false;
-    if (s.hostTier) return true;  // read through the map from host memory
+    if (s.hostTier || s.sharded) return true;  // read through the map, page by page
     for (;;) {
         dgq::SwapArgs a;
         std::memset(&a, 0, sizeof(a));
@@ -1131,7 +1132,8 @@ int getQuEST_PREC(void) { return (int) (sizeof(qreal) / 4); }
 // ---------------------------------------------------------------- registers
 }  // extern "C"
 
-static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const char *func) {
+static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const char *func, int shardBits = 0,
+                             const int *shardDevices = nullptr) {
     Qureg q;
     std::memset(&q, 0, sizeof(q));
     if (numQubits <= 0) {
@@ -1159,8 +1161,19 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
     // device could hold at all; a state that only does not fit next to the
     // registers alive now is an error (E_SYS_TOO_BIG_FOR_DEVICE), as before
     const size_t never = totalB > (1ull << 30) ? totalB - (1ull << 30) : totalB;
-    const bool hostTier = setBudget > 0 ? bytes > std::min<size_t>(avail, (size_t) setBudget) : bytes > never;
-    if (hostTier) {
+    const bool hostTier =
+        shardBits == 0 && (setBudget > 0 ? bytes > std::min<size_t>(avail, (size_t) setBudget) : bytes > never);
+    if (shardBits > 0) {
+        // shards of 2^(n - shardBits) amplitudes on the given devices
+        std::string err;
+        int code = E_UNSUPPORTED;
+        s->pageBits = s->numBits - shardBits;
+        if (!dgq::shardAttach(*s, shardBits, shardDevices, code, err)) {
+            delete s;
+            raise(code, func, err.c_str());
+            return q;
+        }
+    } else if (hostTier) {
         // the host tier: the state in pinned host memory, paged through HBM
         const size_t budget = setBudget > 0 ? std::min<size_t>(avail, (size_t) setBudget) : avail;
         std::string err;
@@ -1176,10 +1189,11 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
     }
     if (!cudaOk(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), func)) {
         dgq::hostTierRelease(*s);
+        dgq::shardRelease(*s);
         delete s;
         return q;
     }
-    if (!registerPool() || (!s->hostTier && !cudaOk(allocOn(&s->dState, bytes, s->stream), func)) ||
+    if (!registerPool() || (!s->hostTier && !s->sharded && !cudaOk(allocOn(&s->dState, bytes, s->stream), func)) ||
         !cudaOk(allocOn((void **) &s->dProbOut, sizeof(double) * (dgq::kMaxStateBits + 1), s->stream), func) ||
         !cudaOk(allocOn((void **) &s->dNorm, sizeof(double) * 2, s->stream), func) ||
         !cudaOk(cudaStreamSynchronize(s->stream), func)) {
@@ -1188,6 +1202,7 @@ static Qureg createQuregWith(int numQubits, QuESTEnv env, bool single, const cha
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
         dgq::hostTierRelease(*s);
+        dgq::shardRelease(*s);
         delete s;
         return q;
     }
@@ -1206,6 +1221,17 @@ extern "C" {
 Qureg createQureg(int numQubits, QuESTEnv env) { return createQuregWith(numQubits, env, false, __func__); }
 
 Qureg dgq_createQuregF32(int numQubits, QuESTEnv env) { return createQuregWith(numQubits, env, true, __func__); }
+
+Qureg dgq_createShardedQureg(int numQubits, QuESTEnv env, int shardBits, const int *devices, int single) {
+    if (shardBits < 1 || shardBits > 4 || numQubits - shardBits < DGQ_MIN_SHARD_QUBITS) {
+        Qureg q;
+        std::memset(&q, 0, sizeof(q));
+        raise(numQubits <= 0 ? E_INVALID_NUM_QUBITS : E_INVALID_ARGUMENT, __func__,
+              "shardBits must be 1..4 with at least 14 qubits in each shard");
+        return q;
+    }
+    return createQuregWith(numQubits, env, single != 0, __func__, shardBits, devices);
+}
 
 int dgq_getPrecision(Qureg qureg) {
     if (!vQureg(qureg, __func__)) return 0;
@@ -1236,6 +1262,7 @@ void destroyQureg(Qureg qureg, QuESTEnv env) {
         cudaStreamDestroy(s->stream);
     }
     dgq::hostTierRelease(*s);
+    dgq::shardRelease(*s);
     delete s;
 }
 
@@ -1290,15 +1317,19 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
     s.probsValid = false;
     const uint64_t n = 1ULL << s.numQubits;
     const uint64_t total = 1ULL << s.numBits;
-    if (s.hostTier) {
-        cudaOk(dgq::hostTierSync(s, __func__) ? cudaSuccess : cudaErrorUnknown, __func__);
+    if (s.hostTier || s.sharded) {
+        if (s.hostTier) cudaOk(dgq::hostTierSync(s, __func__) ? cudaSuccess : cudaErrorUnknown, __func__);
+        // shards: the amplitudes in storage type on the host, then one copy per shard
+        std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
+        void *dst = s.sharded ? (void *) staged.data() : s.hState;
         for (uint64_t i = 0; i < total; i++) {
             const double r = i < n ? reals[i] : 0.0, m = i < n ? imags[i] : 0.0;
             if (s.single)
-                reinterpret_cast<float2 *>(s.hState)[i] = make_float2((float) r, (float) m);
+                reinterpret_cast<float2 *>(dst)[i] = make_float2((float) r, (float) m);
             else
-                reinterpret_cast<double2 *>(s.hState)[i] = make_double2(r, m);
+                reinterpret_cast<double2 *>(dst)[i] = make_double2(r, m);
         }
+        if (s.sharded) dgq::shardWriteVirtual(s, 0, total, staged.data(), __func__);
         return;
     }
     // stage re and im in chunks, interleave on the GPU
@@ -1343,14 +1374,19 @@ void setAmps(Qureg qureg, long long int startInd, qreal *reals, qreal *imags, lo
     }
     if (!normaliseLayout(s, __func__)) return;
     s.probsValid = false;
-    if (s.hostTier) {
+    if (s.hostTier || s.sharded) {
+        // shards: read, change and write back the whole state (virtual order)
+        std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
+        if (s.sharded && !dgq::shardReadVirtual(s, 0, 1ULL << s.numBits, staged.data(), __func__)) return;
+        void *dst = s.sharded ? (void *) staged.data() : s.hState;
         for (long long k = 0; k < numAmps; k++) {
             const uint64_t v = toVirtualIndex(s, (uint64_t) (startInd + k));
             if (s.single)
-                reinterpret_cast<float2 *>(s.hState)[v] = make_float2((float) reals[k], (float) imags[k]);
+                reinterpret_cast<float2 *>(dst)[v] = make_float2((float) reals[k], (float) imags[k]);
             else
-                reinterpret_cast<double2 *>(s.hState)[v] = make_double2(reals[k], imags[k]);
+                reinterpret_cast<double2 *>(dst)[v] = make_double2(reals[k], imags[k]);
         }
+        if (s.sharded) dgq::shardWriteVirtual(s, 0, 1ULL << s.numBits, staged.data(), __func__);
         return;
     }
     const uint64_t chunk = std::min<uint64_t>((uint64_t) std::max<long long>(numAmps, 1), 1ULL << 24);
@@ -1384,7 +1420,9 @@ void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
         raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
         return;
     }
-    if (t.single != c.single || t.hostTier != c.hostTier) {
+    bool sameShards = t.sharded == c.sharded && t.shardBits == c.shardBits;
+    for (int k = 0; sameShards && t.sharded && k < (1 << t.shardBits); k++) sameShards = t.shardDev[k] == c.shardDev[k];
+    if (t.single != c.single || t.hostTier != c.hostTier || !sameShards) {
         raise(E_MISMATCHING_QUREG_TYPES, __func__);
         return;
     }
@@ -1397,6 +1435,8 @@ void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
     if (t.hostTier) {
         if (!dgq::hostTierSync(t, __func__)) return;
         std::memcpy(t.hState, c.hState, ampBytes(t) << t.numBits);
+    } else if (t.sharded) {
+        if (!dgq::shardSync(t, __func__) || !dgq::shardCopy(t, c, __func__)) return;
     } else if (!cudaOk(cudaMemcpyAsync(t.dState, c.dState, ampBytes(t) << t.numBits, cudaMemcpyDeviceToDevice,
                                        t.stream),
                        __func__) ||
@@ -1423,7 +1463,7 @@ void reportQuregParams(Qureg qureg) {
     printf("Number of qubits is %d.\n", s.numQubits);
     printf("Number of amps is %llu.\n", 1ULL << s.numQubits);
     printf("Precision: %s, state in %s.\n", s.single ? "complex64" : "complex128",
-           s.hostTier ? "pinned host memory (host tier)" : "HBM");
+           s.hostTier ? "pinned host memory (host tier)" : s.sharded ? "HBM shards" : "HBM");
 }
 
 // include/QuEST.h:177: every amplitude, for small registers
@@ -1784,7 +1824,16 @@ Complex getAmp(Qureg q, long long int index) {
         return out;
     }
     double2 a;
-    if (s.hostTier) {
+    if (s.sharded) {
+        // one amplitude from the shard that holds it
+        if (s.single) {
+            float2 f;
+            if (!dgq::shardReadVirtual(s, v, 1, &f, __func__)) return out;
+            a = make_double2(f.x, f.y);
+        } else if (!dgq::shardReadVirtual(s, v, 1, &a, __func__)) {
+            return out;
+        }
+    } else if (s.hostTier) {
         // the flushed state is in pinned host memory
         if (s.single) {
             const float2 f = reinterpret_cast<const float2 *>(s.hState)[v];
@@ -1940,6 +1989,16 @@ void dgq_shutdown(void) { dgq::jitStopBackground(); }
 
 int64_t dgq_setDeviceBudget(int64_t bytes) { return g_deviceBudget.exchange(bytes > 0 ? bytes : 0); }
 
+int dgq_getShardStats(Qureg q, int *shardBits, int64_t *passes, int64_t *exchanges, int64_t *bytesExchanged) {
+    if (!vQureg(q, __func__)) return -1;
+    const QuregState &s = *stateOf(q);
+    if (shardBits) *shardBits = s.sharded ? s.shardBits : 0;
+    if (passes) *passes = s.sharded ? s.hostTierPasses : 0;
+    if (exchanges) *exchanges = s.sharded ? s.hostTierSwaps : 0;
+    if (bytesExchanged) *bytesExchanged = s.sharded ? s.hostTierBytes : 0;
+    return s.sharded ? 1 : 0;
+}
+
 int dgq_getHostTierStats(Qureg q, int *pageBits, int64_t *passes, int64_t *exchanges, int64_t *bytesMoved) {
     if (!vQureg(q, __func__)) return -1;
     const QuregState &s = *stateOf(q);
@@ -1989,17 +2048,21 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
     QuregState &s = *stateOf(q);
     if (!flush(s, __func__)) return -1;
     const uint64_t n = 1ULL << s.numQubits;
-    if (s.hostTier) {
-        // logical order through the map, from pinned host memory
+    if (s.hostTier || s.sharded) {
+        // logical order through the map, from pinned host memory (shards:
+        // from a host copy of the shards)
+        std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
+        if (s.sharded && !dgq::shardReadVirtual(s, 0, 1ULL << s.numBits, staged.data(), __func__)) return -1;
+        const void *src = s.sharded ? (const void *) staged.data() : s.hState;
         const double sc = s.restrictActive ? s.rScale : 1.0;
         for (uint64_t i = 0; i < n; i++) {
             const uint64_t v = toVirtualIndex(s, i);
             double2 a;
             if (s.single) {
-                const float2 f = reinterpret_cast<const float2 *>(s.hState)[v];
+                const float2 f = reinterpret_cast<const float2 *>(src)[v];
                 a = make_double2(f.x, f.y);
             } else {
-                a = reinterpret_cast<const double2 *>(s.hState)[v];
+                a = reinterpret_cast<const double2 *>(src)[v];
             }
             const bool keep = !s.restrictActive || (v & s.rMask) == s.rValue;
             re[i] = keep ? a.x * sc : 0.0;

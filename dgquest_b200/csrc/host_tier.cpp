@@ -23,6 +23,17 @@
 //    map records the exchange;
 //  * the passes pipeline over kPageBufs device buffers, one stream each:
 //    copy in, kernels and copy out of different pages overlap.
+//
+// The same segments serve sharded registers, dgQuEST's multi-GPU form (each
+// GPU holds a slice of the state; an MPI page exchange moves qubits between
+// them, QuEST_backend_distributed.cpp:403-601, with the sections of
+// deriveMappings, QuEST_backend.h:532-636): a shard is a page that stays
+// resident in the HBM of its device, a pass launches the segment's plan on
+// every shard in place, and an exchange is one kernel per shard pair that
+// swaps the two half-shards directly, through peer memory (NVLink) when
+// the pair sits on two devices. One host thread drives every device; no
+// kernel waits for another, the passes are ordered by the host and by
+// events between the pair's streams.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -83,8 +94,12 @@ struct Segment {
 // Cuts the gates into page-local segments; the gates after each exchange
 // are rewritten in the exchanged bits. uses[b] lists, in order, the gates
 // whose non-diagonal targets include address bit b (in the rewritten bits),
-// so the next use of a bit is one binary search.
-std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
+// so the next use of a bit is one binary search. With batch (sharded
+// registers, where one pass exchanges several bits for little more than
+// the cost of one), an exchange also brings in every other page-index bit
+// that is needed again before the page bit it would replace, as dgQuEST's
+// section boundaries move several qubits in one reorder.
+std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits, int numBits, bool batch) {
     std::vector<Segment> segs(1);
     const u64 local = (1ULL << pageBits) - 1;
     std::vector<std::vector<size_t>> uses(64);
@@ -99,7 +114,23 @@ std::vector<Segment> cutSegments(std::vector<Gate> g, int pageBits) {
         const u64 glob = nonDiagonal(g[i]) & ~local;
         if (glob) {
             u64 taken = nonDiagonal(g[i]) & local;
-            for (u64 m = glob; m; m &= m - 1) {
+            u64 wanted = glob;
+            if (batch) {
+                // page-index bits by next use, soonest first
+                std::vector<std::pair<size_t, int>> soon;
+                for (int b = pageBits; b < numBits; b++)
+                    if (!((glob >> b) & 1ULL) && nextUse(b, i) < g.size()) soon.emplace_back(nextUse(b, i), b);
+                std::sort(soon.begin(), soon.end());
+                // page bits by next use, latest first (not the gate's own)
+                std::vector<std::pair<size_t, int>> late;
+                for (int l = pageBits - 1; l >= 0; l--)
+                    if (!((taken >> l) & 1ULL)) late.emplace_back(nextUse(l, i), l);
+                std::stable_sort(late.begin(), late.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+                const size_t need = (size_t) __builtin_popcountll(glob);
+                for (size_t t = 0; t < soon.size() && need + t < late.size(); t++)
+                    if (soon[t].first < late[need + t].first) wanted |= 1ULL << soon[t].second;
+            }
+            for (u64 m = wanted; m; m &= m - 1) {
                 const int h = __builtin_ctzll(m);
                 int victim = -1;
                 size_t victimNext = 0;
@@ -155,23 +186,97 @@ bool planIsPageLocal(const QuregState &s, const char *func) {
     return true;
 }
 
-// Launches s.planned on page `page`, held in device buffer b, on stream st.
-bool launchPlanOnPage(QuregState &s, uint64_t page, int b, cudaStream_t st, const char *func) {
+// Launches s.planned on page `page`, held in device buffer buf, on stream
+// st, with the specialised kernels fns (loaded in the context of st's
+// device; null entries run the interpreting kernel).
+bool launchPlanAt(QuregState &s, void *buf, uint64_t page, cudaStream_t st, const std::vector<CUfunction> &fns,
+                  const char *func) {
     const int W = s.plannedTileBits;
     const uint32_t ctas = 1u << (s.pageBits - W);
     // global index (page << pageBits) | i lands on buffer element i
-    const uintptr_t base =
-        reinterpret_cast<uintptr_t>(s.dPage[b]) - (uintptr_t) ((page << s.pageBits) * ampBytesOf(s));
+    const uintptr_t base = reinterpret_cast<uintptr_t>(buf) - (uintptr_t) ((page << s.pageBits) * ampBytesOf(s));
     void *rebased = reinterpret_cast<void *>(base);
     for (size_t i = 0; i < s.planned.size(); i++) {
         TileProgram p = s.planned[i];
         p.ctaOffset = (uint32_t) page * ctas;
         p.ctaCount = ctas;
-        const CUfunction fn = i < s.plannedFns.size() ? s.plannedFns[i] : nullptr;
+        const CUfunction fn = i < fns.size() ? fns[i] : nullptr;
         const cudaError_t e = fn ? launchJitSweep(fn, rebased, W, p, st) : launchTile(rebased, s.single, W, p, st);
         if (!ok(e, func)) return false;
     }
     return true;
+}
+
+bool launchPlanOnPage(QuregState &s, uint64_t page, int b, cudaStream_t st, const char *func) {
+    return launchPlanAt(s, s.dPage[b], page, st, s.plannedFns, func);
+}
+
+// Makes `dev` the calling thread's device; the destructor puts back the
+// device that was current before.
+struct DeviceScope {
+    int prev = -1;
+    bool good = true;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        good = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// The specialised kernels of s.planned for every device that holds a shard
+// (the plan's own functions belong to the home device's context; other
+// devices load the same sources in theirs).
+bool shardFunctions(QuregState &s, std::vector<std::vector<CUfunction>> &perShard, const char *func) {
+    perShard.assign((size_t) 1 << s.shardBits, {});
+    std::vector<std::string> sources;
+    std::vector<size_t> which;
+    for (size_t i = 0; i < s.plannedFns.size(); i++)
+        if (s.plannedFns[i]) {
+            sources.push_back(generateSweepSource(s.planned[i], s.plannedTileBits));
+            which.push_back(i);
+        }
+    std::vector<int> done;
+    std::vector<std::vector<CUfunction>> byDev;
+    for (size_t k = 0; k < perShard.size(); k++) {
+        const int dev = s.shardDev[k];
+        if (dev == s.homeDevice || sources.empty()) {
+            perShard[k] = s.plannedFns;
+            continue;
+        }
+        const auto it = std::find(done.begin(), done.end(), dev);
+        if (it != done.end()) {
+            perShard[k] = byDev[(size_t) (it - done.begin())];
+            continue;
+        }
+        DeviceScope on(dev);
+        if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+        std::vector<CUfunction> got;
+        std::string err;
+        if (!jitGetKernels(sources, got, nullptr, &err)) return raiseExternal(kErrUnsupported, func, err.c_str());
+        std::vector<CUfunction> fns(s.planned.size(), nullptr);
+        for (size_t j = 0; j < which.size(); j++) fns[which[j]] = got[j];
+        done.push_back(dev);
+        byDev.push_back(fns);
+        perShard[k] = fns;
+    }
+    return true;
+}
+
+// Runs s.planned on every shard in place.
+bool runShardPass(QuregState &s, const char *func) {
+    if (!planIsPageLocal(s, func)) return false;
+    std::vector<std::vector<CUfunction>> fns;
+    if (!shardFunctions(s, fns, func)) return false;
+    for (int k = 0; k < (1 << s.shardBits); k++) {
+        DeviceScope on(s.shardDev[k]);
+        if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+        if (!launchPlanAt(s, s.dShard[k], (uint64_t) k, s.shardStream[k], fns[(size_t) k], func)) return false;
+    }
+    s.hostTierPasses++;
+    return shardSync(s, func);
 }
 
 // Runs s.planned on every page: copy in (unless the first sweep writes the
@@ -229,6 +334,68 @@ bool runSwapPass(QuregState &s, int h, int l, bool thenPlan, const char *func) {
     s.v2l[l] = qa;
     if (qa >= 0) s.l2v[qa] = l;
     if (qb >= 0) s.l2v[qb] = h;
+    s.hostTierSwaps++;
+    return true;
+}
+
+// Exchanges the shard-index bits h[t] with the shard bits l[t] (disjoint
+// pairs, one pass): with m pairs, the amplitude at shard c | A(a), offset
+// o | L(b) (a, b: m-bit patterns spread over the h and l positions) moves to
+// shard c | A(b), offset o | L(a). Each pair of blocks with a < b trades
+// places in one kernel on the device of the first shard (peer loads and
+// stores when the second is elsewhere); the blocks are disjoint, so the
+// kernels of one pass run concurrently on the shards' streams.
+bool runShardExchange(QuregState &s, const std::vector<std::pair<int, int>> &swaps, const char *func) {
+    std::vector<std::pair<int, int>> sw = swaps;  // (shard bit l, shard-index bit h), l ascending
+    for (auto &x : sw) x = {x.second, x.first};
+    std::sort(sw.begin(), sw.end());
+    const int m = (int) sw.size();
+    if (m < 1 || m > s.shardBits) return raiseExternal(kErrUnsupported, func, "internal: bad shard exchange");
+    BlockSwapArgs args;
+    std::memset(&args, 0, sizeof(args));
+    args.pageBits = s.pageBits;
+    args.m = m;
+    int hMask = 0;
+    for (int t = 0; t < m; t++) {
+        args.pos[t] = sw[(size_t) t].first;
+        hMask |= 1 << (sw[(size_t) t].second - s.pageBits);
+    }
+    auto spreadH = [&](int a) {
+        int r = 0;
+        for (int t = 0; t < m; t++)
+            if ((a >> t) & 1) r |= 1 << (sw[(size_t) t].second - s.pageBits);
+        return r;
+    };
+    auto spreadL = [&](int b) {
+        uint64_t r = 0;
+        for (int t = 0; t < m; t++)
+            if ((b >> t) & 1) r |= 1ULL << sw[(size_t) t].first;
+        return r;
+    };
+    const size_t blockBytes = ampBytesOf(s) << (s.pageBits - m);
+    for (int c = 0; c < (1 << s.shardBits); c++) {
+        if (c & hMask) continue;
+        for (int a = 0; a < (1 << m); a++)
+            for (int b = a + 1; b < (1 << m); b++) {
+                const int x = c | spreadH(a), y = c | spreadH(b);
+                args.patX = spreadL(b);
+                args.patY = spreadL(a);
+                DeviceScope on(s.shardDev[x]);
+                if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+                if (!ok(launchBlockSwap(s.dShard[x], s.dShard[y], s.single, args, s.shardStream[x]), func))
+                    return false;
+                s.hostTierBytes += 2 * blockBytes;  // one block each way
+            }
+    }
+    if (!shardSync(s, func)) return false;
+    for (const auto &x : sw) {
+        const int l = x.first, h = x.second;
+        const int qa = s.v2l[h], qb = s.v2l[l];
+        s.v2l[h] = qb;
+        s.v2l[l] = qa;
+        if (qa >= 0) s.l2v[qa] = l;
+        if (qb >= 0) s.l2v[qb] = h;
+    }
     s.hostTierSwaps++;
     return true;
 }
@@ -295,7 +462,14 @@ bool hostTierFlush(QuregState &s, const char *func) {
         if (g.type == OP_MULTI_UNITARY && g.numMultiTargets > kRegBits)
             return raiseExternal(kErrUnsupported, func,
                                  "a multi-qubit unitary of more than 4 targets on a register in host memory");
-    std::vector<Segment> segs = cutSegments(s.pending, s.pageBits);
+    std::vector<Segment> segs = cutSegments(s.pending, s.pageBits, s.numBits, s.sharded);
+    if (s.restrictActive && segs[0].gates.empty()) {
+        // a pending collapse is in the address bits before any exchange: an
+        // empty program carries it into the first pass
+        Gate one;
+        one.type = OP_ONE;
+        segs[0].gates.push_back(one);
+    }
     const MatrixPool pool = s.pool;
     const int denseFusion = s.denseFusion;
     s.denseFusion = 0;
@@ -308,10 +482,15 @@ bool hostTierFlush(QuregState &s, const char *func) {
         if (!ranWithExchange && (!segs[k].gates.empty() || header)) {
             s.pending = segs[k].gates;
             s.pool = pool;
-            good = planForPages(s, func) && runPagePass(s, func);
+            good = planForPages(s, func) && (s.sharded ? runShardPass(s, func) : runPagePass(s, func));
         }
         ranWithExchange = false;
         const auto &sw = segs[k].swapsAfter;
+        if (s.sharded) {
+            // all of the boundary's bits in one pass
+            if (!sw.empty() && good) good = runShardExchange(s, sw, func);
+            continue;
+        }
         for (size_t i = 0; i < sw.size() && good; i++) {
             // the last exchange before a segment runs that segment too
             const bool fuse = i + 1 == sw.size() && k + 1 < segs.size() && !segs[k + 1].gates.empty();
@@ -349,7 +528,17 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
     a.kappa = std::min(4, std::max(0, nf - 12));
     a.rValue = rValue & localMask;
     const size_t need = (size_t) probNumCtas(a) * 17;
-    if (need > s.pagePartialCap) {
+    if (s.sharded && need > s.shardPartialCap) {
+        for (int k = 0; k < (1 << s.shardBits); k++) {
+            DeviceScope on(s.shardDev[k]);
+            if (s.dShardPartial[k]) cudaFree(s.dShardPartial[k]);
+            s.dShardPartial[k] = nullptr;
+            if (!ok(on.good ? cudaMalloc((void **) &s.dShardPartial[k], need * sizeof(double)) : cudaErrorInvalidDevice,
+                    func))
+                return false;
+        }
+        s.shardPartialCap = need;
+    } else if (!s.sharded && need > s.pagePartialCap) {
         for (int b = 0; b < QuregState::kPageBufs; b++) {
             if (s.dPagePartial[b]) cudaFree(s.dPagePartial[b]);
             s.dPagePartial[b] = nullptr;
@@ -364,18 +553,29 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
         // pages outside a collapse on page-index bits hold no probability
         if (((page << p) & rMask & ~localMask) != (rValue & ~localMask)) continue;
         used[page] = 1;
+        double *sum = &sums[page * (size_t) (nf + 1)];
+        const size_t sumBytes = sizeof(double) * (size_t) (nf + 1);
+        if (s.sharded) {
+            // a shard is read where it lies
+            DeviceScope on(s.shardDev[page]);
+            if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+            cudaStream_t st = s.shardStream[page];
+            if (!ok(launchProb(s.dShard[page], s.single, a, s.dShardPartial[page], s.dShardOut[page], st), func) ||
+                !ok(cudaMemcpyAsync(sum, s.dShardOut[page], sumBytes, cudaMemcpyDeviceToHost, st), func))
+                return false;
+            continue;
+        }
         const int b = (int) (page % QuregState::kPageBufs);
         cudaStream_t st = s.pageStream[b];
         if (!ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, page), pageBytes, cudaMemcpyHostToDevice, st), func) ||
             !ok(launchProb(s.dPage[b], s.single, a, s.dPagePartial[b], s.dPageOut[b], st), func) ||
-            !ok(cudaMemcpyAsync(&sums[page * (size_t) (nf + 1)], s.dPageOut[b], sizeof(double) * (size_t) (nf + 1),
-                                cudaMemcpyDeviceToHost, st),
-                func))
+            !ok(cudaMemcpyAsync(sum, s.dPageOut[b], sumBytes, cudaMemcpyDeviceToHost, st), func))
             return false;
     }
-    if (!hostTierSync(s, func)) return false;
+    if (!(s.sharded ? shardSync(s, func) : hostTierSync(s, func))) return false;
     s.hostTierPasses++;
-    for (uint64_t page = 0; page < pages; page++) s.hostTierBytes += used[page] ? pageBytes : 0;
+    if (!s.sharded)
+        for (uint64_t page = 0; page < pages; page++) s.hostTierBytes += used[page] ? pageBytes : 0;
     p0.assign((size_t) s.numBits, 0.0);
     total = 0.0;
     for (uint64_t page = 0; page < pages; page++) {
@@ -390,6 +590,150 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
     // collapsed page bits: all the probability on their fixed value
     for (int b = 0; b < p; b++)
         if ((rMask >> b) & 1ULL) p0[(size_t) b] = ((rValue >> b) & 1ULL) ? 0.0 : total;
+    return true;
+}
+
+bool shardSync(QuregState &s, const char *func) {
+    for (int k = 0; k < (1 << s.shardBits); k++)
+        if (s.shardStream[k] && !ok(cudaStreamSynchronize(s.shardStream[k]), func)) return false;
+    return true;
+}
+
+bool shardAttach(QuregState &s, int shardBits, const int *devices, int &code, std::string &err) {
+    constexpr int kErrTooBig = 101;  // E_SYS_TOO_BIG_FOR_DEVICE
+    code = kErrUnsupported;
+    const int shards = 1 << shardBits;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        err = "no CUDA device";
+        return false;
+    }
+    if (cudaGetDevice(&s.homeDevice) != cudaSuccess) {
+        err = "no current CUDA device";
+        return false;
+    }
+    for (int k = 0; k < shards; k++) {
+        s.shardDev[k] = devices ? devices[k] : s.homeDevice;
+        if (s.shardDev[k] < 0 || s.shardDev[k] >= count) {
+            err = "a shard's device does not exist";
+            return false;
+        }
+    }
+    // every pair of distinct devices exchanges through peer memory
+    for (int i = 0; i < shards; i++)
+        for (int j = 0; j < shards; j++) {
+            const int a = s.shardDev[i], b = s.shardDev[j];
+            if (a == b) continue;
+            int can = 0;
+            if (cudaDeviceCanAccessPeer(&can, a, b) != cudaSuccess || !can) {
+                err = "two shard devices have no peer access to each other";
+                return false;
+            }
+            DeviceScope on(a);
+            const cudaError_t e = on.good ? cudaDeviceEnablePeerAccess(b, 0) : cudaErrorInvalidDevice;
+            if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) {
+                cudaGetLastError();
+                err = "enabling peer access between shard devices failed";
+                return false;
+            }
+            cudaGetLastError();  // an already-enabled pair leaves its error recorded
+        }
+    const size_t bytes = ampBytesOf(s) << s.pageBits;
+    s.sharded = true;
+    s.shardBits = shardBits;
+    for (int k = 0; k < shards; k++) {
+        DeviceScope on(s.shardDev[k]);
+        if (!on.good || cudaStreamCreateWithFlags(&s.shardStream[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaMalloc((void **) &s.dShardOut[k], sizeof(double) * (kMaxStateBits + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            shardRelease(s);
+            err = "shard streams or buffers are not available";
+            return false;
+        }
+        if (cudaMalloc(&s.dShard[k], bytes) != cudaSuccess) {
+            s.dShard[k] = nullptr;
+            cudaGetLastError();  // the failed allocation must not surface at a later launch
+            shardRelease(s);
+            code = kErrTooBig;
+            err = "a shard does not fit in its device's memory";
+            return false;
+        }
+    }
+    return true;
+}
+
+void shardRelease(QuregState &s) {
+    for (int k = 0; k < QuregState::kMaxShards; k++) {
+        if (!s.shardStream[k] && !s.dShard[k] && !s.dShardOut[k] && !s.dShardPartial[k]) continue;
+        DeviceScope on(s.shardDev[k]);
+        if (s.shardStream[k]) cudaStreamSynchronize(s.shardStream[k]);
+        if (s.dShard[k]) cudaFree(s.dShard[k]);
+        if (s.dShardPartial[k]) cudaFree(s.dShardPartial[k]);
+        if (s.dShardOut[k]) cudaFree(s.dShardOut[k]);
+        if (s.shardStream[k]) cudaStreamDestroy(s.shardStream[k]);
+        s.dShard[k] = nullptr;
+        s.dShardPartial[k] = nullptr;
+        s.dShardOut[k] = nullptr;
+        s.shardStream[k] = nullptr;
+    }
+    s.shardPartialCap = 0;
+    s.sharded = false;
+}
+
+namespace {
+
+// Calls fn(shard, offset in the shard, offset in [begin, begin + count),
+// amplitudes) for the runs of [begin, begin + count) that lie in one shard.
+template <class F>
+bool forShardRuns(const QuregState &s, uint64_t begin, uint64_t count, F fn) {
+    const uint64_t mask = (1ULL << s.pageBits) - 1;
+    for (uint64_t i = begin; i < begin + count;) {
+        const int k = (int) (i >> s.pageBits);
+        const uint64_t off = i & mask;
+        const uint64_t run = std::min<uint64_t>(begin + count - i, (mask + 1) - off);
+        if (!fn(k, off, i - begin, run)) return false;
+        i += run;
+    }
+    return true;
+}
+
+}  // namespace
+
+bool shardReadVirtual(QuregState &s, uint64_t begin, uint64_t count, void *host, const char *func) {
+    const size_t ab = ampBytesOf(s);
+    return forShardRuns(s, begin, count, [&](int k, uint64_t off, uint64_t at, uint64_t run) {
+        DeviceScope on(s.shardDev[k]);
+        if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+        return ok(cudaMemcpyAsync(static_cast<char *>(host) + at * ab, static_cast<const char *>(s.dShard[k]) + off * ab,
+                                  run * ab, cudaMemcpyDeviceToHost, s.shardStream[k]),
+                  func) &&
+               ok(cudaStreamSynchronize(s.shardStream[k]), func);
+    });
+}
+
+bool shardWriteVirtual(QuregState &s, uint64_t begin, uint64_t count, const void *host, const char *func) {
+    const size_t ab = ampBytesOf(s);
+    return forShardRuns(s, begin, count, [&](int k, uint64_t off, uint64_t at, uint64_t run) {
+        DeviceScope on(s.shardDev[k]);
+        if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+        return ok(cudaMemcpyAsync(static_cast<char *>(s.dShard[k]) + off * ab,
+                                  static_cast<const char *>(host) + at * ab, run * ab, cudaMemcpyHostToDevice,
+                                  s.shardStream[k]),
+                  func) &&
+               ok(cudaStreamSynchronize(s.shardStream[k]), func);
+    });
+}
+
+bool shardCopy(QuregState &t, const QuregState &c, const char *func) {
+    const size_t bytes = ampBytesOf(t) << t.pageBits;
+    for (int k = 0; k < (1 << t.shardBits); k++) {
+        DeviceScope on(t.shardDev[k]);
+        if (!on.good) return raiseExternal(kErrCuda, func, "cannot select a shard's device");
+        if (!ok(cudaMemcpyPeerAsync(t.dShard[k], t.shardDev[k], c.dShard[k], c.shardDev[k], bytes, t.shardStream[k]),
+                func) ||
+            !ok(cudaStreamSynchronize(t.shardStream[k]), func))
+            return false;
+    }
     return true;
 }
 

@@ -686,21 +686,32 @@ bool ensureContext() {
     return true;
 }
 
+// Loaded kernels, per source and device: a function belongs to the context
+// of the device it was loaded on (a sharded register on several devices
+// loads each source once per device).
 struct CacheEntry {
     std::string source;
+    int device;
     CUmodule module;
     CUfunction fn;
 };
+
+int currentDevice() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    return dev;
+}
 
 std::mutex g_cacheMutex;
 std::unordered_map<size_t, std::vector<CacheEntry>> g_cache;
 
 CUfunction cacheFind(const std::string &src) {
     std::lock_guard<std::mutex> lk(g_cacheMutex);
+    const int dev = currentDevice();
     auto it = g_cache.find(std::hash<std::string>()(src));
     if (it == g_cache.end()) return nullptr;
     for (const auto &e : it->second)
-        if (e.source == src) return e.fn;
+        if (e.device == dev && e.source == src) return e.fn;
     return nullptr;
 }
 
@@ -941,7 +952,7 @@ bool jitGetKernels(const std::vector<std::string> &sources, std::vector<CUfuncti
         }
         out[i] = fn;
         std::lock_guard<std::mutex> lk(g_cacheMutex);
-        g_cache[std::hash<std::string>()(sources[i])].push_back({sources[i], mod, fn});
+        g_cache[std::hash<std::string>()(sources[i])].push_back({sources[i], currentDevice(), mod, fn});
     }
     for (size_t i = 0; i < sources.size(); i++)
         if (dupOf[i] != (size_t) -1) out[i] = out[dupOf[i]];

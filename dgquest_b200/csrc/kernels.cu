@@ -360,6 +360,47 @@ cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit,
     return cudaGetLastError();
 }
 
+// Block exchange between two shards (sharded registers, several qubits at
+// once): for every offset o whose bits at the m positions pos[] are 0,
+// x[o | patX] trades places with y[o | patY] (patX, patY: patterns over those
+// positions). k enumerates the offsets; inserting a 0 at each position in
+// ascending order turns k into o, so consecutive threads touch consecutive
+// amplitudes except across the inserted bits.
+template <class V>
+__global__ void blockSwapKernel(V *__restrict__ x, V *__restrict__ y, const __grid_constant__ BlockSwapArgs args) {
+    const uint64_t count = 1ULL << (args.pageBits - args.m);
+    for (uint64_t k = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; k < count;
+         k += (uint64_t) gridDim.x * blockDim.x) {
+        uint64_t o = k;
+        for (int t = 0; t < args.m; t++) {
+            const int b = args.pos[t];
+            o = ((o >> b) << (b + 1)) | (o & ((1ULL << b) - 1));
+        }
+        const V v = x[o | args.patX];
+        x[o | args.patX] = y[o | args.patY];
+        y[o | args.patY] = v;
+    }
+}
+
+cudaError_t launchBlockSwap(void *x, void *y, bool single, const BlockSwapArgs &args, cudaStream_t s) {
+    // positions ascending, inside the shard, patterns on them only
+    if (args.m < 1 || args.m > 4 || args.pageBits <= args.m || args.pageBits > 40) return cudaErrorInvalidValue;
+    uint64_t mask = 0;
+    for (int t = 0; t < args.m; t++) {
+        if (args.pos[t] < 0 || args.pos[t] >= args.pageBits || (t > 0 && args.pos[t] <= args.pos[t - 1]))
+            return cudaErrorInvalidValue;
+        mask |= 1ULL << args.pos[t];
+    }
+    if ((args.patX & ~mask) || (args.patY & ~mask)) return cudaErrorInvalidValue;
+    const uint64_t count = 1ULL << (args.pageBits - args.m);
+    const unsigned grid = (unsigned) std::min<uint64_t>((count + 255) / 256, 148u * 16u);
+    if (single)
+        blockSwapKernel<float2><<<grid, 256, 0, s>>>((float2 *) x, (float2 *) y, args);
+    else
+        blockSwapKernel<double2><<<grid, 256, 0, s>>>((double2 *) x, (double2 *) y, args);
+    return cudaGetLastError();
+}
+
 cudaError_t launchSwapBits(void *st, bool single, const SwapArgs &args, cudaStream_t s) {
     const uint64_t numAmps = 1ULL << args.numBits;
     uint64_t blocks = (numAmps + 255) / 256;

@@ -99,6 +99,16 @@ cudaError_t launchSwapBits(void *st, bool single, const SwapArgs &args, cudaStre
 // Host tier: exchanges local bit `bit` with the page-index bit in which the
 // pages a and b (2^pageBits amplitudes each) differ.
 cudaError_t launchPageSwap(void *a, void *b, bool single, int pageBits, int bit, cudaStream_t s);
+// Sharded registers: x[o | patX] <-> y[o | patY] for every offset o of a
+// 2^pageBits-amplitude shard whose bits at pos[0..m) (ascending) are 0.
+struct BlockSwapArgs {
+    int pageBits;
+    int m;
+    int pos[4];
+    uint64_t patX;
+    uint64_t patY;
+};
+cudaError_t launchBlockSwap(void *x, void *y, bool single, const BlockSwapArgs &args, cudaStream_t s);
 cudaError_t launchGather(const void *st, bool single, const GatherArgs &args, double2 *out, cudaStream_t s);
 cudaError_t launchFp64Peak(double *out, int blocks, int iters, cudaStream_t s);
 cudaError_t launchInterleave(const double *re, const double *im, uint64_t count, uint64_t total, void *out,

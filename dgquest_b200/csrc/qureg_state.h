@@ -77,9 +77,27 @@ struct QuregState {
     double *dPagePartial[kPageBufs] = {};
     double *dPageOut[kPageBufs] = {};
     size_t pagePartialCap = 0;
-    int64_t hostTierSwaps = 0;   // page-pair exchange passes run so far
-    int64_t hostTierPasses = 0;  // page passes (sweep segments and read-outs) run so far
-    int64_t hostTierBytes = 0;   // bytes copied between host and device so far
+    // sharded register: 2^shardBits shards of 2^pageBits amplitudes, shard
+    // k holding global indices [k << pageBits, (k + 1) << pageBits) in HBM of
+    // device shardDev[k] (shards may share a device); a gate on a
+    // shard-index bit first exchanges it (with any other shard-index bits
+    // needed soon) for shard bits, in one pass over blocks of shard pairs
+    bool sharded = false;
+    int shardBits = 0;
+    int homeDevice = 0;  // the device of `stream` and of the read-out buffers
+    static constexpr int kMaxShards = 16;
+    void *dShard[kMaxShards] = {};
+    int shardDev[kMaxShards] = {};
+    cudaStream_t shardStream[kMaxShards] = {};
+    double *dShardPartial[kMaxShards] = {};
+    double *dShardOut[kMaxShards] = {};
+    size_t shardPartialCap = 0;
+
+    // counters of the host tier and of sharded registers
+    int64_t hostTierSwaps = 0;   // page-pair (shard-pair) exchange passes run so far
+    int64_t hostTierPasses = 0;  // page (shard) passes: sweep segments and read-outs
+    int64_t hostTierBytes = 0;   // host tier: bytes copied between host and device;
+                                 // shards: bytes that crossed between shards
 };
 
 namespace dgq {
@@ -113,5 +131,18 @@ void hostTierRelease(QuregState &s);
 bool hostTierFlush(QuregState &s, const char *func);
 bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const char *func);
 bool hostTierSync(QuregState &s, const char *func);
+
+// sharded registers (host_tier.cpp). attach: 2^shardBits shards on the
+// given devices (nullptr: all on the current device), peer access enabled
+// between the devices used; flush (hostTierFlush) runs the pending work
+// shard by shard; probs as for the host tier; readVirtual/writeVirtual copy
+// amplitudes [begin, begin + count) in virtual order (storage type) between
+// the shards and host memory.
+bool shardAttach(QuregState &s, int shardBits, const int *devices, int &code, std::string &err);
+void shardRelease(QuregState &s);
+bool shardSync(QuregState &s, const char *func);
+bool shardReadVirtual(QuregState &s, uint64_t begin, uint64_t count, void *host, const char *func);
+bool shardWriteVirtual(QuregState &s, uint64_t begin, uint64_t count, const void *host, const char *func);
+bool shardCopy(QuregState &t, const QuregState &c, const char *func);
 
 }  // namespace dgq

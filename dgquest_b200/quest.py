@@ -186,6 +186,8 @@ _SIGS = {
     "dgq_loadCostModel": (I, [ctypes.c_char_p]),
     "dgq_getCostModel": (I, [P(D), P(D)]),
     "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
+    "dgq_createShardedQureg": (Qureg, [I, E, I, P(I), I]),
+    "dgq_getShardStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
     "dgq_launchPlanned": (I, [Q]),
     "dgq_sync": (I, [Q]),
     "dgq_getStream": (c_void_p, [Q]),
@@ -323,6 +325,27 @@ def host_tier_stats(q):
     moved = ctypes.c_int64(0)
     r = dgq_getHostTierStats(q, ctypes.byref(pb), ctypes.byref(passes), ctypes.byref(ex), ctypes.byref(moved))
     return (pb.value, passes.value, ex.value, moved.value) if r == 1 else None
+
+
+def create_sharded(n, env, shard_bits, devices=None, single=False):
+    """A register of n qubits in 2^shard_bits shards; devices[k] is the CUDA
+    device of shard k (None: all on the current device)."""
+    arr = None
+    if devices is not None:
+        assert len(devices) == 1 << shard_bits
+        arr = (I * len(devices))(*[int(d) for d in devices])
+    return dgq_createShardedQureg(n, env, shard_bits, arr, 1 if single else 0)
+
+
+def shard_stats(q):
+    """(shard bits, shard passes, qubit exchanges, bytes moved between
+    shards) of a sharded register, or None for any other register."""
+    sb = ctypes.c_int(0)
+    passes = ctypes.c_int64(0)
+    ex = ctypes.c_int64(0)
+    moved = ctypes.c_int64(0)
+    r = dgq_getShardStats(q, ctypes.byref(sb), ctypes.byref(passes), ctypes.byref(ex), ctypes.byref(moved))
+    return (sb.value, passes.value, ex.value, moved.value) if r == 1 else None
 
 
 def seed(keys):

@@ -98,6 +98,30 @@ int64_t dgq_setDeviceBudget(int64_t bytes);
  * next segment counts as a pass too), 0 for a register in HBM, -1 on error. */
 int dgq_getHostTierStats(Qureg qureg, int *pageBits, int64_t *passes, int64_t *exchanges, int64_t *bytesMoved);
 
+/* Sharded registers: dgQuEST's multi-GPU state (each GPU holds a slice and an
+ * MPI page exchange moves qubits between slices,
+ * src/cpp/QuEST_backend_distributed.cpp:403-601) in one process. The state is
+ * split into 2^shardBits shards of 2^(numQubits - shardBits) amplitudes, shard
+ * k holding amplitudes [k << (numQubits - shardBits), (k + 1) << ...) in the
+ * HBM of device devices[k] (NULL: every shard on the current device; several
+ * shards may share a device; distinct devices need peer access, which is
+ * enabled here). Pending gates run segment by segment, each segment's
+ * sweeps on every shard in place; a gate on a shard-index qubit first
+ * exchanges it with a qubit inside the shards, one kernel per shard pair
+ * swapping half-shards through peer memory (NVLink) when the pair spans two
+ * devices. Gates (multi-qubit unitaries of at most 4 targets), read-outs,
+ * measurement, setAmps, initStateFromAmps and cloneQureg (between registers
+ * of the same shard layout) work as in HBM; dense sweeps, sampling, inner
+ * products, batches, dgq_getDeviceState and the plan/launch split report
+ * E_UNSUPPORTED. single != 0 makes a complex64 register. shardBits is 1..4
+ * and every shard holds at least DGQ_MIN_SHARD_QUBITS qubits. */
+#define DGQ_MIN_SHARD_QUBITS 14
+Qureg dgq_createShardedQureg(int numQubits, QuESTEnv env, int shardBits, const int *devices, int single);
+/* 1 for a sharded register (with its shard-index bits, shard passes, qubit
+ * exchanges and bytes moved between shards so far), 0 otherwise, -1 on
+ * error. */
+int dgq_getShardStats(Qureg qureg, int *shardBits, int64_t *passes, int64_t *exchanges, int64_t *bytesExchanged);
+
 /* Dense-block form. qubits = 5, 6 or 7: the register's gates are fused into
  * dense unitaries on that many qubits (dgQuEST's greedy block rule,
  * DAG.cpp:219-259, with every qubit a gate touches counted), composed in

@@ -135,3 +135,29 @@ def test_host_tier_measurement_mid_circuit(quest, env, small_budget):
     assert np.abs(amps - ref).max() <= 1e-12
     assert np.abs(p0 - ref_p0).max() <= 1e-12
     assert exchanges >= 1
+
+
+def test_host_tier_collapse_before_exchange(quest, env, small_budget):
+    """A measurement followed at once by a gate on a page-index qubit: the
+    pending collapse is applied before the page exchange moves its bit."""
+    n = 17
+    page = 14  # qubits below this one are in the page; the highest of them is the first to leave
+    b = C.OpList()
+    for k in range(page):
+        b.add(C.H, k)
+    b.add(C.RY, page - 1, p=[0.7]).add(C.CNOT, page - 1, 2)
+    # the measurement runs the gates above without an exchange; the next gate
+    # then exchanges qubit n - 1 with the measured qubit's bit
+    b.add(C.MEASURE, page - 1).add(C.H, n - 1).add(C.RX, n - 2, p=[0.4]).add(C.MEASURE, n - 1).add(C.H, n - 1)
+    ops = b.array()
+    quest.seed([3, 4])
+    q = quest.createQureg(n, env)
+    try:
+        assert quest.host_tier_stats(q) is not None
+        out = C.replay(q, ops)
+        amps = quest.state_vector(q)
+    finally:
+        quest.destroyQureg(q, env)
+    ref, _, ref_out = oracle.run(n, ops, seed_keys=[3, 4])
+    assert out == ref_out
+    assert np.abs(amps - ref).max() <= 1e-12
