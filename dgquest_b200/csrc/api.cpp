@@ -2217,6 +2217,31 @@ int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, 
     return 0;
 }
 
+int dgq_planExchanges(int numQubits, int localQubits, int batch, int count, const int32_t *types,
+                      const uint64_t *targetMasks, int32_t *segments, int32_t *exchanges, int32_t *qubitsMoved) {
+    if (numQubits < 1 || numQubits > dgq::kMaxStateBits - 2 || localQubits < 1 || localQubits > numQubits ||
+        count < 0 || (count > 0 && (!types || !targetMasks))) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
+    }
+    std::vector<Gate> gates((size_t) count);
+    const uint64_t all = numQubits >= 64 ? ~0ULL : (1ULL << numQubits) - 1;
+    for (int i = 0; i < count; i++) {
+        if (types[i] < 0 || types[i] > dgq::OP_MULTI_UNITARY || (targetMasks[i] & ~all)) {
+            raise(E_INVALID_ARGUMENT, __func__, "a gate type or target outside the register");
+            return -1;
+        }
+        gates[(size_t) i].type = (dgq::GateType) types[i];
+        gates[(size_t) i].targetMask = targetMasks[i];
+    }
+    int seg = 0, ex = 0, moved = 0;
+    dgq::planExchanges(gates, localQubits, numQubits, batch != 0, seg, ex, moved);
+    if (segments) *segments = seg;
+    if (exchanges) *exchanges = ex;
+    if (qubitsMoved) *qubitsMoved = moved;
+    return 0;
+}
+
 int dgq_setSpecialisationMinBits(int minBits) {
     const int prev = jitMinBits();
     g_jitMinBits.store(minBits < 0 ? 22 : minBits);

@@ -593,6 +593,19 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
     return true;
 }
 
+void planExchanges(const std::vector<Gate> &gates, int localBits, int numBits, bool batch, int &segments,
+                   int &exchanges, int &qubitsMoved) {
+    const std::vector<Segment> segs = cutSegments(gates, localBits, numBits, batch);
+    segments = (int) segs.size();
+    exchanges = qubitsMoved = 0;
+    for (const Segment &sg : segs)
+        if (!sg.swapsAfter.empty()) {
+            // the host tier runs one pass per qubit, sharded registers one per boundary
+            exchanges += batch ? 1 : (int) sg.swapsAfter.size();
+            qubitsMoved += (int) sg.swapsAfter.size();
+        }
+}
+
 bool shardSync(QuregState &s, const char *func) {
     for (int k = 0; k < (1 << s.shardBits); k++)
         if (s.shardStream[k] && !ok(cudaStreamSynchronize(s.shardStream[k]), func)) return false;

@@ -144,5 +144,10 @@ bool shardSync(QuregState &s, const char *func);
 bool shardReadVirtual(QuregState &s, uint64_t begin, uint64_t count, void *host, const char *func);
 bool shardWriteVirtual(QuregState &s, uint64_t begin, uint64_t count, const void *host, const char *func);
 bool shardCopy(QuregState &t, const QuregState &c, const char *func);
+// How the host tier (batch = false) or a sharded register (batch = true)
+// with 2^localBits amplitudes per page cuts `gates`: segments, exchange
+// passes and qubits moved (host only).
+void planExchanges(const std::vector<Gate> &gates, int localBits, int numBits, bool batch, int &segments,
+                   int &exchanges, int &qubitsMoved);
 
 }  // namespace dgq

@@ -83,6 +83,21 @@ def fuse_apply_host(n, k, types, tm, cm, opnd, amps):
     return re + 1j * im, nb
 
 
+def plan_exchanges(ops, n, local_qubits, batch):
+    """Host-only: (segments, exchange passes, qubits moved) of an op list on
+    a register whose pages (batch=False, host tier) or shards (batch=True)
+    hold 2^local_qubits amplitudes (no GPU needed)."""
+    from .quest import _check, _library
+    fn = _library().dgq_planExchanges
+    P = ctypes.POINTER
+    t, tm, _, _ = ops_to_ir(ops, n)
+    seg, ex, moved = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+    fn(n, local_qubits, 1 if batch else 0, len(t), t.ctypes.data_as(P(ctypes.c_int32)),
+       tm.ctypes.data_as(P(ctypes.c_uint64)), ctypes.byref(seg), ctypes.byref(ex), ctypes.byref(moved))
+    _check()
+    return seg.value, ex.value, moved.value
+
+
 def plan(ops, n, tile_bits=0, want_merged=False):
     """Host-only plan statistics of an op list (no GPU needed)."""
     from .quest import PlanStats, _check, _library

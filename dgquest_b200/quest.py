@@ -207,6 +207,8 @@ _SIGS = {
     "dgq_getDeviceErrors": (I, []),
     "dgq_calcProbOfAllZeroNoAlloc": (I, [c_void_p, I, c_void_p, c_void_p]),
     "dgq_fuseApplyHost": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(D), P(D)]),
+    "dgq_planExchanges": (I, [I, I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_int32),
+                              P(ctypes.c_int32), P(ctypes.c_int32)]),
     "dgq_planGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), P(PlanStats),
                           P(ctypes.c_int32), P(ctypes.c_int32)]),
     "dgq_applyCircuit": (I, [Q, c_void_p, I, P(I)]),

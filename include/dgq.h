@@ -193,6 +193,16 @@ int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, 
                   const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
                   int32_t *numMerged);
 
+/* Host-only view of the qubit exchanges (no GPU call): how the gates
+ * (dgq_planGates encoding; only types and target masks matter) are cut into
+ * segments whose non-diagonal targets lie below localQubits, by the host tier
+ * (batch = 0: pages of 2^localQubits amplitudes, one exchange pass per qubit)
+ * or by a sharded register (batch = 1: shards of 2^localQubits amplitudes,
+ * every qubit of a boundary in one pass). Reports the segments, the exchange
+ * passes and the qubits moved; returns 0, or -1 on a bad argument. */
+int dgq_planExchanges(int numQubits, int localQubits, int batch, int count, const int32_t *types,
+                      const uint64_t *targetMasks, int32_t *segments, int32_t *exchanges, int32_t *qubitsMoved);
+
 /* Host-only view of the dense-block form (no GPU call): fuses the gates
  * (dgq_planGates encoding) into dense blocks of K = 1..7 qubits as
  * dgq_setDenseFusion does and applies the fused gates in FP64 on the host
