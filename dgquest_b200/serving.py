@@ -125,7 +125,7 @@ class Server:
     register would not fit in the budget beside them."""
 
     def __init__(self, env, hbm_budget=None, workers=6, max_bypass=8, runner=None, cached_kernels_only=True,
-                 keep_resident=False, spec_policy=1):
+                 keep_resident=False, spec_policy=1, register_ops=None):
         self.env = env
         # one-off circuit structures run the interpreting kernel instead of
         # waiting for a kernel compile; their kernels compile in the background
@@ -133,8 +133,14 @@ class Server:
         # 1: kernels of new structures compile in the background for later
         # requests; 2: nothing is compiled (structures that never repeat)
         self.spec_policy = spec_policy
-        self.custom_runner = runner
+        # register_ops = (create(r) -> register, destroy(register)): the
+        # register path with a caller's runner(r, register) (host-only tests)
+        self.custom_runner = runner if register_ops is None else None
         self.runner = runner or (lambda r, q=None: run_request(r, env, q=q))
+        if register_ops is None:
+            register_ops = (lambda r: Q.dgq_createQuregF32(r.n, env) if r.single else Q.createQureg(r.n, env),
+                            lambda q: Q.destroyQureg(q, env))
+        self._create_reg, self._destroy_reg = register_ops
         self.idle = collections.defaultdict(list)  # (n, single) -> registers
         self.idle_bytes = 0
         self.reused = 0
@@ -144,8 +150,9 @@ class Server:
         self.peak_in_flight = 0
         if hbm_budget is None:
             # free HBM (with the register pool's spare memory), less a margin
-            # for the per-request scratch and the specialised kernels
-            hbm_budget = int(Q.dgq_getAvailableMemory() * 0.9)
+            # for the per-request scratch, the specialised kernels and the
+            # pool's fragmentation
+            hbm_budget = int(Q.dgq_getAvailableMemory() * 0.85)
         self.budget = int(hbm_budget)
         self.workers = int(workers)
         self.max_bypass = int(max_bypass)
@@ -193,9 +200,40 @@ class Server:
         """Destroys the idle registers."""
         for regs in self.idle.values():
             for q in regs:
-                Q.destroyQureg(q, self.env)
+                self._destroy_reg(q)
         self.idle.clear()
         self.idle_bytes = 0
+
+    def _create(self, r, cond, state):
+        """A new register for admitted request r. The byte count admitted r,
+        but device memory can still be short where the pool's free memory
+        is split among blocks of other sizes: on an out-of-memory error the
+        idle registers are destroyed and the creation retried; on a second
+        one, no further request is admitted until the others in flight have
+        finished, and the creation is retried then (with the lock held)."""
+        def short(exc):
+            return isinstance(exc, Q.QuESTError) and exc.code in (101, 103)
+
+        for attempt in range(2):
+            try:
+                return self._create_reg(r)
+            except Exception as exc:  # noqa: BLE001
+                if not short(exc):
+                    raise
+            with cond:
+                if attempt == 0:
+                    self.close()
+                    continue
+                state["draining"] += 1
+                try:
+                    # (requests whose creation waits here too count as finished)
+                    while state["in_flight"] > state["draining"] and state["error"] is None:
+                        cond.wait(0.05)
+                    self.close()
+                    return self._create_reg(r)
+                finally:
+                    state["draining"] -= 1
+                    cond.notify_all()
 
     def serve(self, requests, realtime=True):
         """Runs the stream; returns results in request order. With realtime,
@@ -207,7 +245,7 @@ class Server:
         cond = threading.Condition()
         waiting = collections.deque()
         bypassed = collections.Counter()
-        state = {"in_use": 0, "in_flight": 0, "arrived": 0, "finished": 0, "error": None}
+        state = {"in_use": 0, "in_flight": 0, "arrived": 0, "finished": 0, "error": None, "draining": 0}
         results = {}
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
@@ -225,6 +263,8 @@ class Server:
 
         def pick():
             # called with the lock held: first fit, head reserved once bypassed enough
+            if state["draining"]:
+                return None
             for i, r in enumerate(waiting):
                 if state["in_use"] + state_bytes(r) <= self.budget:
                     for j in range(i):
@@ -258,17 +298,17 @@ class Server:
                         # destroyed before the lock is released, so that no
                         # other worker counts on memory that is not free yet
                         for e in evict:
-                            Q.destroyQureg(e, self.env)
+                            self._destroy_reg(e)
                 try:
                     if self.custom_runner is not None:
                         samples, expz = self.runner(r)
                     else:
                         if q is None:
-                            q = Q.dgq_createQuregF32(r.n, self.env) if r.single else Q.createQureg(r.n, self.env)
+                            q = self._create(r, cond, state)
                         samples, expz = self.runner(r, q)
                 except Exception as exc:  # noqa: BLE001
                     if q is not None:
-                        Q.destroyQureg(q, self.env)
+                        self._destroy_reg(q)
                     with cond:
                         state["error"] = exc
                         cond.notify_all()

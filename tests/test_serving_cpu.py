@@ -4,6 +4,7 @@ import threading
 import time
 
 import numpy as np
+import pytest
 
 from dgquest_b200 import serving as S
 
@@ -88,3 +89,50 @@ def test_idle_registers_reused_and_evicted_largest_first():
     q, ev = srv._take(mk(19, False), in_use=(16 << 18) + (16 << 19))
     assert q is None and ev == ["reg20"]
     assert srv.idle_bytes == 8 << 18
+
+
+def test_register_creation_retried_when_memory_is_short():
+    """Device memory short although the byte count admitted the request
+    (the pool's free memory split among blocks of other sizes; here a fake
+    device that holds less than the admission budget): the idle registers
+    are destroyed and the creation retried; after a second failure the
+    server drains the requests in flight and retries once more (host logic
+    only, with fake register operations)."""
+    from dgquest_b200 import quest as Q
+    lock = threading.Lock()
+    live, destroyed, failures = {}, [], [0]
+    capacity = 40 << 20  # the admission budget below is 64 MiB
+
+    def create(r):
+        with lock:
+            if sum(live.values()) + S.state_bytes(r) > capacity:
+                failures[0] += 1
+                raise Q.QuESTError(103, "QuEST Error in function createQureg: CUDA runtime error. (out of memory)")
+            q = ("reg", r.rid)
+            live[q] = S.state_bytes(r)
+            return q
+
+    def destroy(q):
+        with lock:
+            destroyed.append(q)
+            del live[q]
+
+    def runner(r, q):
+        time.sleep(0.002)
+        return [r.rid], None
+
+    reqs = [S.Request(i, "bv", 16 + (i % 5), 0, 1, 0.001 * i, (0,), 2, bool(i % 2)) for i in range(80)]
+    srv = S.Server(env=None, hbm_budget=64 << 20, workers=4, runner=runner, register_ops=(create, destroy))
+    res = srv.serve(reqs, realtime=False)
+    assert [x.rid for x in res] == list(range(80))
+    assert all(x.samples == [x.rid] for x in res)
+    assert failures[0] > 0 and destroyed  # memory ran short, idle registers were handed back
+    srv.close()
+    assert not live
+
+    def broken(r):
+        raise Q.QuESTError(104, "Invalid argument.")
+
+    srv = S.Server(env=None, hbm_budget=64 << 20, workers=2, runner=runner, register_ops=(broken, destroy))
+    with pytest.raises(Q.QuESTError):
+        srv.serve(reqs[:4], realtime=False)
