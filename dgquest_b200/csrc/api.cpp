@@ -102,7 +102,7 @@ const char *errorMessage(int code) {
         case E_MISMATCHING_QUREG_DIMENSIONS: return "Dimensions of the qubit registers don't match.";
         case E_INVALID_NUM_TARGETS: return "Invalid number of target qubits. Must be >0 and <=numQubits, and unique.";
         case E_SYS_TOO_BIG_FOR_DEVICE: return "The state-vector does not fit in free GPU memory.";
-        case E_UNSUPPORTED: return "Operation not supported by this build.";
+        case E_UNSUPPORTED: return "Operation not supported by this library.";
         case E_CUDA: return "CUDA runtime error.";
         case E_INVALID_ARGUMENT: return "Invalid argument.";
         default: return "Unknown error.";
