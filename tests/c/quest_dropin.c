@@ -9,6 +9,9 @@
  *   quest_dropin mixed N    rotations, compactUnitary, controlled gates, a
  *                           multiQubitUnitary and measure() under a fixed
  *                           seed; prints outcomes, then P(q=0) and amplitudes
+ *   quest_dropin sharded N  GHZ + QFT as above on a register split into 4
+ *                           shards (dgq_createShardedQureg from dgq.h, all on
+ *                           the current device); the calls are unchanged
  *
  * Output: lines "p0 q value", "amp i re im", "outcome q value". */
 #include <math.h>
@@ -17,6 +20,7 @@
 #include <string.h>
 
 #include "QuEST.h"
+#include "dgq.h"
 
 static const double kPi = 3.14159265358979323846;
 
@@ -65,9 +69,10 @@ int main(int argc, char **argv) {
     QuESTEnv env = createQuESTEnv();
     unsigned long seeds[2] = {12345, 67890};
     seedQuEST(seeds, 2);
-    Qureg q = createQureg(n, env);
+    const int sharded = !strcmp(argv[1], "sharded");
+    Qureg q = sharded ? dgq_createShardedQureg(n, env, 2, NULL, 0) : createQureg(n, env);
     initZeroState(q);
-    if (!strcmp(argv[1], "ghzqft")) {
+    if (!strcmp(argv[1], "ghzqft") || sharded) {
         ghz_qft(q, n);
     } else {
         mixed(q, n);

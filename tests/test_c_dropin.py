@@ -1,8 +1,8 @@
 """A plain C program written against include/QuEST.h (tests/c/quest_dropin.c)
 builds and links with libdgq.so alone (CPU), and on the GPU prints the
 oracle's amplitudes (1e-12), P(q=0) (1e-12) and measurement outcomes
-(bit-exact, seeded) for GHZ+QFT and for a mixed circuit with a
-multi-qubit unitary."""
+(bit-exact, seeded) for GHZ+QFT (also on a sharded register) and for a
+mixed circuit with a multi-qubit unitary."""
 import math
 import os
 import subprocess
@@ -77,6 +77,17 @@ def mixed_ops(n):
 def test_c_program_ghz_qft_matches_oracle(quest, dropin):
     n = 16
     p0, amps, _ = run(dropin, "ghzqft", n)
+    ref, ref_p0, _ = oracle.run(n, C.ghz_qft(n))
+    assert np.abs(amps - ref).max() <= 1e-12
+    assert np.abs(p0 - ref_p0).max() <= 1e-12
+
+
+@pytest.mark.gpu
+def test_c_program_sharded_register_matches_oracle(quest, dropin):
+    """The same calls on a register in 4 shards (2 qubits above each shard,
+    so the QFT's gates on them go through qubit exchanges)."""
+    n = 16
+    p0, amps, _ = run(dropin, "sharded", n)
     ref, ref_p0, _ = oracle.run(n, C.ghz_qft(n))
     assert np.abs(amps - ref).max() <= 1e-12
     assert np.abs(p0 - ref_p0).max() <= 1e-12
