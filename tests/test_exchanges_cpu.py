@@ -72,3 +72,28 @@ def test_bad_arguments():
         ir.plan_exchanges(ops, 4, 5, True)
     with pytest.raises(Q.QuESTError):
         ir.plan_exchanges(ops, 4, 0, True)
+
+
+def test_two_qubits_above_the_page_needed_one_after_the_other():
+    """A controlled rotation whose target is above the page, then a rotation
+    of its control (also above the page): the host tier moves each qubit in
+    a pass of its own, a sharded register moves both in one."""
+    n, local = 18, 16
+    b = C.OpList()
+    for q in range(local):
+        b.add(C.H, q)
+    b.add(C.CRX, n - 2, n - 1, p=(0.3,)).add(C.SWAP, 0, 1)  # only the target must be inside the page
+    b.add(C.RX, n - 2, p=(0.2,))
+    ops = b.array()
+    seg0, ex0, moved0 = ir.plan_exchanges(ops, n, local, False)
+    seg1, ex1, moved1 = ir.plan_exchanges(ops, n, local, True)
+    assert (ex0, moved0) == (2, 2)
+    assert (ex1, moved1) == (1, 2)
+
+
+def test_sharded_register_arguments_checked_before_any_device_call():
+    from dgquest_b200 import quest as Q
+    env = Q.QuESTEnv()  # never used: the checks come first
+    for n, sb in [(16, 0), (16, 5), (15, 2), (0, 1)]:
+        with pytest.raises(Q.QuESTError):
+            Q.create_sharded(n, env, sb)
