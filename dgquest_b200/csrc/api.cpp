@@ -13,6 +13,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -99,7 +100,20 @@ const char *errorMessage(int code) {
         case E_COLLAPSE_STATE_ZERO_PROB: return "Can't collapse to state with zero probability.";
         case E_INVALID_QUBIT_OUTCOME: return "Invalid measurement outcome -- must be either 0 or 1.";
         case E_DEFINED_ONLY_FOR_STATEVECS: return "Operation valid only for state-vectors.";
+        case E_DEFINED_ONLY_FOR_DENSMATRS: return "Operation valid only for density matrices.";
+        case E_INVALID_PROB: return "Probabilities must be in [0, 1].";
+        case E_INVALID_ONE_QUBIT_DEPHASE_PROB:
+            return "The probability of a single qubit dephase error cannot exceed 1/2, which maximally mixes.";
+        case E_INVALID_TWO_QUBIT_DEPHASE_PROB:
+            return "The probability of a two-qubit qubit dephase error cannot exceed 3/4, which maximally mixes.";
+        case E_INVALID_ONE_QUBIT_DEPOL_PROB:
+            return "The probability of a single qubit depolarising error cannot exceed 3/4, which maximally mixes.";
+        case E_INVALID_TWO_QUBIT_DEPOL_PROB:
+            return "The probability of a two-qubit depolarising error cannot exceed 15/16, which maximally mixes.";
         case E_MISMATCHING_QUREG_DIMENSIONS: return "Dimensions of the qubit registers don't match.";
+        case E_MISMATCHING_QUREG_TYPES:
+            return "Registers must both be state-vectors or both be density matrices.";
+        case E_SECOND_ARG_MUST_BE_STATEVEC: return "Second argument must be a state-vector.";
         case E_INVALID_NUM_TARGETS: return "Invalid number of target qubits. Must be >0 and <=numQubits, and unique.";
         case E_SYS_TOO_BIG_FOR_DEVICE: return "The state-vector does not fit in free GPU memory.";
         case E_UNSUPPORTED: return "Operation not supported by this library.";
@@ -757,9 +771,34 @@ bool vDeviceResident(const QuregState &s, const char *func) {
     return raise(E_UNSUPPORTED, func, "not available for a register held in host memory (larger than the device budget)");
 }
 
+bool readLogicalFor(QuregState &s, double *re, double *im, const char *func);
+
+// Density registers: P(row qubit t = 0) and the trace from the diagonal,
+// read on the host (the whole vectorisation: 16 x 4^n bytes).
+bool densityProbs(QuregState &s, const char *func) {
+    const int n = s.densityQubits;
+    const uint64_t dim = 1ULL << n;
+    std::vector<double> re(dim * dim), im(dim * dim);
+    if (!readLogicalFor(s, re.data(), im.data(), func)) return false;
+    std::vector<double> p0((size_t) n, 0.0);
+    double total = 0.0;
+    for (uint64_t i = 0; i < dim; i++) {
+        const double d = re[i + (i << n)];
+        total += d;
+        for (int t = 0; t < n; t++)
+            if (!((i >> t) & 1ULL)) p0[(size_t) t] += d;
+    }
+    s.p0.assign((size_t) s.numBits, 0.0);
+    for (int t = 0; t < n; t++) s.p0[(size_t) s.l2v[t]] = p0[(size_t) t];
+    s.totalProb = total;
+    s.probsValid = true;
+    return true;
+}
+
 bool ensureProbs(QuregState &s, const char *func) {
     if (s.probsValid) return true;
     if (!flush(s, func)) return false;
+    if (s.densityQubits) return densityProbs(s, func);
     if (s.hostTier || s.sharded) {
         std::vector<double> p0;
         double total = 0.0;
@@ -846,6 +885,16 @@ bool vStateIndex(const Qureg &q, long long idx, const char *func) {
     if (idx < 0 || idx >= maxIdx) return raise(E_INVALID_STATE_INDEX, func);
     return true;
 }
+bool vStateVec(const Qureg &q, const char *func) {
+    if (!vQureg(q, func)) return false;
+    if (q.isDensityMatrix) return raise(E_DEFINED_ONLY_FOR_STATEVECS, func);
+    return true;
+}
+bool vDensity(const Qureg &q, const char *func) {
+    if (!vQureg(q, func)) return false;
+    if (!q.isDensityMatrix) return raise(E_DEFINED_ONLY_FOR_DENSMATRS, func);
+    return true;
+}
 bool vOutcome(int o, const char *func) {
     if (o != 0 && o != 1) return raise(E_INVALID_QUBIT_OUTCOME, func);
     return true;
@@ -871,8 +920,7 @@ bool isMatrix2Unitary(const ComplexMatrix2 &u) {
 }
 
 // ---------------------------------------------------------------- recording
-void record(const Qureg &q, dgq::GateType type, u64 logicalTargets, u64 logicalControls, const double *op, int nop) {
-    QuregState &s = *stateOf(q);
+void push(QuregState &s, dgq::GateType type, u64 logicalTargets, u64 logicalControls, const double *op, int nop) {
     Gate g;
     g.type = type;
     g.targetMask = toVirtualMask(s, logicalTargets);
@@ -880,6 +928,44 @@ void record(const Qureg &q, dgq::GateType type, u64 logicalTargets, u64 logicalC
     for (int i = 0; i < nop; i++) g.op[i] = op[i];
     s.pending.push_back(g);
     s.probsValid = false;
+}
+
+// The complex conjugate of a gate in the same encoding: phase powers
+// e^{i pi k/4} become k -> 8 - k, angles change sign (phase shift, Rz and Rx
+// store -angle; Ry is real), Y and its conjugate trade types, and the
+// imaginary parts of compact pairs and 2x2 matrices change sign.
+dgq::GateType conjugateGate(dgq::GateType type, const double *op, int nop, double *out) {
+    for (int i = 0; i < nop; i++) out[i] = op[i];
+    if (type <= dgq::OP_T_GATE_CONJ) return (dgq::GateType) ((8 - (int) type) % 8);
+    switch (type) {
+        case dgq::OP_PHASE_SHIFT:
+        case dgq::OP_ROTATE_Z:
+        case dgq::OP_ROTATE_X: out[0] = -op[0]; break;
+        case dgq::OP_PAULI_Y: return dgq::OP_PAULI_Y_CONJ;
+        case dgq::OP_PAULI_Y_CONJ: return dgq::OP_PAULI_Y;
+        case dgq::OP_COMPACT_UNITARY:
+            out[1] = -op[1];
+            out[3] = -op[3];
+            break;
+        case dgq::OP_UNITARY:
+            for (int i = 1; i < 8; i += 2) out[i] = -op[i];
+            break;
+        default: break;  // X, H, Ry: real
+    }
+    return type;
+}
+
+// Density registers apply rho -> U rho U^dagger as U on the row qubits
+// 0..n-1 and conj(U) on the column qubits n..2n-1 of the vectorisation
+// (upstream QuEST's representation of createDensityQureg, QuEST.h:139).
+void record(const Qureg &q, dgq::GateType type, u64 logicalTargets, u64 logicalControls, const double *op, int nop) {
+    QuregState &s = *stateOf(q);
+    push(s, type, logicalTargets, logicalControls, op, nop);
+    if (const int n = s.densityQubits) {
+        double c[8];
+        const dgq::GateType ct = conjugateGate(type, op, nop, c);
+        push(s, ct, logicalTargets << n, logicalControls << n, c, nop);
+    }
 }
 
 void recordMatrix(const Qureg &q, u64 targets, u64 controls, const ComplexMatrix2 &u) {
@@ -1018,7 +1104,7 @@ int dgq_applyCircuit(Qureg q, const dgq_gate_record *r, int count, int *outcomes
 }
 
 int dgq_sampleOutcomes(Qureg q, int numSamples, uint32_t seed, uint64_t *outcomes) {
-    if (!vQureg(q, __func__)) return -1;
+    if (!vStateVec(q, __func__)) return -1;
     if (numSamples < 0 || (numSamples > 0 && !outcomes))
         return raise(E_INVALID_ARGUMENT, __func__, "numSamples < 0 or null output") ? 0 : -1;
     QuregState &s = *stateOf(q);
@@ -1222,6 +1308,28 @@ Qureg createQureg(int numQubits, QuESTEnv env) { return createQuregWith(numQubit
 
 Qureg dgq_createQuregF32(int numQubits, QuESTEnv env) { return createQuregWith(numQubits, env, true, __func__); }
 
+// include/QuEST.h:139 (declared only in dgQuEST): an n-qubit density matrix
+// in |0><0|, held as the 2n-qubit vectorisation (row qubits 0..n-1, column
+// qubits n..2n-1), complex128
+Qureg createDensityQureg(int numQubits, QuESTEnv env) {
+    Qureg q;
+    std::memset(&q, 0, sizeof(q));
+    if (numQubits <= 0) {
+        raise(E_INVALID_NUM_QUBITS, __func__);
+        return q;
+    }
+    if (2 * numQubits > dgq::kMaxStateBits - 2) {
+        raise(E_SYS_TOO_BIG_FOR_DEVICE, __func__);
+        return q;
+    }
+    q = createQuregWith(2 * numQubits, env, false, __func__);
+    if (!q.state) return q;
+    q.state->densityQubits = numQubits;
+    q.isDensityMatrix = 1;
+    q.numQubitsRepresented = (u64) numQubits;
+    return q;
+}
+
 Qureg dgq_createShardedQureg(int numQubits, QuESTEnv env, int shardBits, const int *devices, int single) {
     if (shardBits < 1 || shardBits > 4 || numQubits - shardBits < DGQ_MIN_SHARD_QUBITS) {
         Qureg q;
@@ -1292,21 +1400,21 @@ void initZeroState(Qureg qureg) {
 
 void initPlusState(Qureg qureg) {
     if (!vQureg(qureg, __func__)) return;
-    setInit(qureg, dgq::INIT_PLUS, 0, 1.0 / std::sqrt((double) (1LL << qureg.numQubitsRepresented)));
+    // density registers: |+><+| has every element 1/2^n
+    const double dim = (double) (1LL << qureg.numQubitsRepresented);
+    setInit(qureg, dgq::INIT_PLUS, 0, qureg.isDensityMatrix ? 1.0 / dim : 1.0 / std::sqrt(dim));
 }
 
 void initClassicalState(Qureg qureg, long long int stateInd) {
     if (!vStateIndex(qureg, stateInd, __func__)) return;
-    setInit(qureg, dgq::INIT_CLASSICAL, (uint64_t) stateInd, 0.0);
+    // density registers: |k><k| is element (k, k)
+    const uint64_t k = (uint64_t) stateInd;
+    setInit(qureg, dgq::INIT_CLASSICAL, qureg.isDensityMatrix ? k + (k << qureg.numQubitsRepresented) : k, 0.0);
 }
 
-void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
-    if (!vQureg(qureg, __func__)) return;
-    if (!reals || !imags) {
-        raise(E_INVALID_ARGUMENT, __func__, "null amplitude array");
-        return;
-    }
-    QuregState &s = *stateOf(qureg);
+// Replaces the register's vector by (reals, imags), 2^numQubits entries in
+// logical order (a density register's vectorisation).
+static void loadAmps(QuregState &s, const double *reals, const double *imags, const char *func) {
     s.pending.clear();
     s.pool.mats.clear();
     s.initPending = false;
@@ -1318,7 +1426,7 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
     const uint64_t n = 1ULL << s.numQubits;
     const uint64_t total = 1ULL << s.numBits;
     if (s.hostTier || s.sharded) {
-        if (s.hostTier) cudaOk(dgq::hostTierSync(s, __func__) ? cudaSuccess : cudaErrorUnknown, __func__);
+        if (s.hostTier) cudaOk(dgq::hostTierSync(s, func) ? cudaSuccess : cudaErrorUnknown, func);
         // shards: the amplitudes in storage type on the host, then one copy per shard
         std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
         void *dst = s.sharded ? (void *) staged.data() : s.hState;
@@ -1329,36 +1437,45 @@ void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
             else
                 reinterpret_cast<double2 *>(dst)[i] = make_double2(r, m);
         }
-        if (s.sharded) dgq::shardWriteVirtual(s, 0, total, staged.data(), __func__);
+        if (s.sharded) dgq::shardWriteVirtual(s, 0, total, staged.data(), func);
         return;
     }
     // stage re and im in chunks, interleave on the GPU
     const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 24);
     double *dRe = nullptr, *dIm = nullptr;
-    if (!cudaOk(cudaMalloc(&dRe, chunk * sizeof(double)), __func__)) return;
-    if (!cudaOk(cudaMalloc(&dIm, chunk * sizeof(double)), __func__)) {
+    if (!cudaOk(cudaMalloc(&dRe, chunk * sizeof(double)), func)) return;
+    if (!cudaOk(cudaMalloc(&dIm, chunk * sizeof(double)), func)) {
         cudaFree(dRe);
         return;
     }
     if (total > n) {
-        cudaOk(cudaMemsetAsync((char *) s.dState + n * ampBytes(s), 0, (total - n) * ampBytes(s), s.stream), __func__);
+        cudaOk(cudaMemsetAsync((char *) s.dState + n * ampBytes(s), 0, (total - n) * ampBytes(s), s.stream), func);
     }
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint64_t c = std::min(chunk, n - off);
-        cudaOk(cudaMemcpyAsync(dRe, reals + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
-        cudaOk(cudaMemcpyAsync(dIm, imags + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), __func__);
-        cudaOk(dgq::launchInterleave(dRe, dIm, c, c, (char *) s.dState + off * ampBytes(s), s.single, s.stream), __func__);
+        cudaOk(cudaMemcpyAsync(dRe, reals + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), func);
+        cudaOk(cudaMemcpyAsync(dIm, imags + off, c * sizeof(double), cudaMemcpyHostToDevice, s.stream), func);
+        cudaOk(dgq::launchInterleave(dRe, dIm, c, c, (char *) s.dState + off * ampBytes(s), s.single, s.stream), func);
         g_launches++;
     }
-    cudaOk(cudaStreamSynchronize(s.stream), __func__);
+    cudaOk(cudaStreamSynchronize(s.stream), func);
     cudaFree(dRe);
     cudaFree(dIm);
+}
+
+void initStateFromAmps(Qureg qureg, qreal *reals, qreal *imags) {
+    if (!vStateVec(qureg, __func__)) return;
+    if (!reals || !imags) {
+        raise(E_INVALID_ARGUMENT, __func__, "null amplitude array");
+        return;
+    }
+    loadAmps(*stateOf(qureg), reals, imags, __func__);
 }
 
 // include/QuEST.h:257 (declared only in dgQuEST): amplitudes [startInd,
 // startInd + numAmps) in logical order, the others kept
 void setAmps(Qureg qureg, long long int startInd, qreal *reals, qreal *imags, long long int numAmps) {
-    if (!vQureg(qureg, __func__) || !vStateIndex(qureg, startInd, __func__)) return;
+    if (!vStateVec(qureg, __func__) || !vStateIndex(qureg, startInd, __func__)) return;
     QuregState &s = *stateOf(qureg);
     if (numAmps < 0 || numAmps > (1LL << s.numQubits)) {
         raise(E_INVALID_NUM_AMPS, __func__);
@@ -1422,7 +1539,7 @@ void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
     }
     bool sameShards = t.sharded == c.sharded && t.shardBits == c.shardBits;
     for (int k = 0; sameShards && t.sharded && k < (1 << t.shardBits); k++) sameShards = t.shardDev[k] == c.shardDev[k];
-    if (t.single != c.single || t.hostTier != c.hostTier || !sameShards) {
+    if (t.single != c.single || t.hostTier != c.hostTier || !sameShards || t.densityQubits != c.densityQubits) {
         raise(E_MISMATCHING_QUREG_TYPES, __func__);
         return;
     }
@@ -1453,7 +1570,33 @@ void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
 }
 
 // include/QuEST.h:229: for state-vectors, the pure state's amplitudes
-void initPureState(Qureg qureg, Qureg pure) { cloneQureg(qureg, pure); }
+void initPureState(Qureg qureg, Qureg pure) {
+    if (!vQureg(qureg, __func__) || !vQureg(pure, __func__)) return;
+    if (!qureg.isDensityMatrix) {
+        cloneQureg(qureg, pure);
+        return;
+    }
+    // density register: rho = |psi><psi|, built on the host
+    if (pure.isDensityMatrix) {
+        raise(E_SECOND_ARG_MUST_BE_STATEVEC, __func__);
+        return;
+    }
+    if (pure.numQubitsRepresented != qureg.numQubitsRepresented) {
+        raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
+        return;
+    }
+    QuregState &s = *stateOf(qureg);
+    const int n = s.densityQubits;
+    const uint64_t dim = 1ULL << n;
+    std::vector<double> pr(dim), pi(dim), re(dim * dim), im(dim * dim);
+    if (!readLogicalFor(*stateOf(pure), pr.data(), pi.data(), __func__)) return;
+    for (uint64_t c = 0; c < dim; c++)
+        for (uint64_t r = 0; r < dim; r++) {
+            re[r + (c << n)] = pr[r] * pr[c] + pi[r] * pi[c];
+            im[r + (c << n)] = pi[r] * pr[c] - pr[r] * pi[c];
+        }
+    loadAmps(s, re.data(), im.data(), __func__);
+}
 
 // include/QuEST.h:183
 void reportQuregParams(Qureg qureg) {
@@ -1670,9 +1813,13 @@ void swapGate(Qureg q, int a, int b) {
     // relabel logical qubits instead of moving amplitudes: later gates and
     // read-outs translate through l2v
     QuregState &s = *stateOf(q);
-    std::swap(s.l2v[a], s.l2v[b]);
-    s.v2l[s.l2v[a]] = a;
-    s.v2l[s.l2v[b]] = b;
+    for (int k = 0; k < (s.densityQubits ? 2 : 1); k++) {
+        // density registers: the row qubits and the column qubits
+        const int x = a + k * s.densityQubits, y = b + k * s.densityQubits;
+        std::swap(s.l2v[x], s.l2v[y]);
+        s.v2l[s.l2v[x]] = x;
+        s.v2l[s.l2v[y]] = y;
+    }
 }
 // src/QuEST.c:320-416 (u1/u2/u3 and the square-root gates are 2x2 unitaries)
 void u1Gate(Qureg q, int t, qreal lambda) {
@@ -1800,27 +1947,196 @@ void multiQubitUnitary(Qureg q, int *targs, int numTargs, ComplexMatrixN u) {
             m[(size_t) 2 * (r * d + c)] = u.real[r][c];
             m[(size_t) 2 * (r * d + c) + 1] = u.imag[r][c];
         }
+    for (int k = 0; k < (s.densityQubits ? 2 : 1); k++) {
+        // density registers: conj(U) on the column qubits as well
+        const int shift = k * s.densityQubits;
+        Gate g;
+        g.type = dgq::OP_MULTI_UNITARY;
+        g.targetMask = toVirtualMask(s, tm << shift);
+        g.controlMask = 0;
+        g.numMultiTargets = numTargs;
+        for (int i = 0; i < numTargs; i++) g.multiTargets[i] = s.l2v[targs[i] + shift];
+        g.multiIndex = (int32_t) s.pool.mats.size();
+        std::vector<double> mk = m;
+        if (k == 1)
+            for (size_t i = 1; i < mk.size(); i += 2) mk[i] = -mk[i];
+        s.pool.mats.push_back(std::move(mk));
+        s.pending.push_back(g);
+    }
+    s.probsValid = false;
+}
+
+// ---------------------------------------------------------------- noise
+// Density registers: a channel rho -> sum_K K rho K^dagger on k = 1 or 2
+// qubits is one dense op on the row qubits and the column qubits together
+// (targets qs[0..k), qs[0..k) + n; matrix index bits in that order), the
+// superoperator S[(r', c')][(r, c)] = sum_K K[r'][r] conj(K[c'][c]).
+using Kraus = std::vector<std::complex<double>>;  // d x d, row-major
+
+static void recordChannel(Qureg q, const int *qs, int k, const std::vector<Kraus> &kraus) {
+    QuregState &s = *stateOf(q);
+    const int n = s.densityQubits, d = 1 << k, D = d * d;
+    std::vector<double> m((size_t) 2 * D * D, 0.0);
+    for (const Kraus &K : kraus)
+        for (int rp = 0; rp < d; rp++)
+            for (int cp = 0; cp < d; cp++)
+                for (int r = 0; r < d; r++)
+                    for (int c = 0; c < d; c++) {
+                        const std::complex<double> v = K[(size_t) (rp * d + r)] * std::conj(K[(size_t) (cp * d + c)]);
+                        const size_t at = (size_t) 2 * ((rp + cp * d) * D + (r + c * d));
+                        m[at] += v.real();
+                        m[at + 1] += v.imag();
+                    }
     Gate g;
     g.type = dgq::OP_MULTI_UNITARY;
+    u64 tm = 0;
+    for (int i = 0; i < k; i++) tm |= bit(qs[i]) | bit(qs[i] + n);
     g.targetMask = toVirtualMask(s, tm);
     g.controlMask = 0;
-    g.numMultiTargets = numTargs;
-    for (int i = 0; i < numTargs; i++) g.multiTargets[i] = s.l2v[targs[i]];
+    g.numMultiTargets = 2 * k;
+    for (int i = 0; i < k; i++) {
+        g.multiTargets[i] = s.l2v[qs[i]];
+        g.multiTargets[k + i] = s.l2v[qs[i] + n];
+    }
     g.multiIndex = (int32_t) s.pool.mats.size();
     s.pool.mats.push_back(std::move(m));
     s.pending.push_back(g);
     s.probsValid = false;
 }
 
-// ---------------------------------------------------------------- read-outs
-Complex getAmp(Qureg q, long long int index) {
-    Complex out{0.0, 0.0};
-    if (!vStateIndex(q, index, __func__)) return out;
+static const std::complex<double> kI(0.0, 1.0);
+
+static Kraus pauli(int p) {  // 0 I, 1 X, 2 Y, 3 Z
+    switch (p) {
+        case 1: return {0.0, 1.0, 1.0, 0.0};
+        case 2: return {0.0, -kI, kI, 0.0};
+        case 3: return {1.0, 0.0, 0.0, -1.0};
+        default: return {1.0, 0.0, 0.0, 1.0};
+    }
+}
+
+// P_a (x) P_b on two qubits, a the low bit of the 4 x 4 index
+static Kraus pauli2(int pa, int pb, double w) {
+    const Kraus A = pauli(pa), B = pauli(pb);
+    Kraus K(16);
+    for (int rb = 0; rb < 2; rb++)
+        for (int ra = 0; ra < 2; ra++)
+            for (int cb = 0; cb < 2; cb++)
+                for (int ca = 0; ca < 2; ca++)
+                    K[(size_t) ((ra + 2 * rb) * 4 + (ca + 2 * cb))] = w * A[(size_t) (ra * 2 + ca)] * B[(size_t) (rb * 2 + cb)];
+    return K;
+}
+
+static bool vNoise(Qureg q, int t, double prob, double maxProb, int code, const char *func) {
+    if (!vDensity(q, func) || !vTarget(q, t, func)) return false;
+    if (!(prob >= 0.0 && prob <= 1.0)) return raise(E_INVALID_PROB, func);
+    if (prob > maxProb) return raise(code, func);
+    return true;
+}
+
+// include/QuEST.h:1373: (1 - p) rho + p Z rho Z
+void applyOneQubitDephaseError(Qureg q, const int targetQubit, qreal prob) {
+    if (!vNoise(q, targetQubit, prob, 0.5, E_INVALID_ONE_QUBIT_DEPHASE_PROB, __func__)) return;
+    const double a = std::sqrt(1.0 - prob), b = std::sqrt(prob);
+    Kraus K0 = pauli(0), K1 = pauli(3);
+    for (auto &x : K0) x *= a;
+    for (auto &x : K1) x *= b;
+    recordChannel(q, &targetQubit, 1, {K0, K1});
+}
+
+// include/QuEST.h:1399: (1 - p) rho + p/3 (Za rho Za + Zb rho Zb + ZaZb rho ZaZb)
+void applyTwoQubitDephaseError(Qureg q, const int qubit1, const int qubit2, qreal prob) {
+    if (!vNoise(q, qubit1, prob, 0.75, E_INVALID_TWO_QUBIT_DEPHASE_PROB, __func__) ||
+        !vUniqueTargets(q, qubit1, qubit2, __func__))
+        return;
+    const int qs[2] = {qubit1, qubit2};
+    const double w = std::sqrt(prob / 3.0);
+    recordChannel(q, qs, 2,
+                  {pauli2(0, 0, std::sqrt(1.0 - prob)), pauli2(3, 0, w), pauli2(0, 3, w), pauli2(3, 3, w)});
+}
+
+// include/QuEST.h:1423: (1 - p) rho + p/3 (X rho X + Y rho Y + Z rho Z)
+void applyOneQubitDepolariseError(Qureg q, const int targetQubit, qreal prob) {
+    if (!vNoise(q, targetQubit, prob, 0.75, E_INVALID_ONE_QUBIT_DEPOL_PROB, __func__)) return;
+    std::vector<Kraus> ks;
+    for (int p = 0; p < 4; p++) {
+        Kraus K = pauli(p);
+        const double w = p == 0 ? std::sqrt(1.0 - prob) : std::sqrt(prob / 3.0);
+        for (auto &x : K) x *= w;
+        ks.push_back(K);
+    }
+    recordChannel(q, &targetQubit, 1, ks);
+}
+
+// include/QuEST.h:1445: amplitude damping (decay to |0>) with probability p:
+// Kraus operators [[1, 0], [0, sqrt(1 - p)]] and [[0, sqrt(p)], [0, 0]]
+void applyOneQubitDampingError(Qureg q, const int targetQubit, qreal prob) {
+    if (!vNoise(q, targetQubit, prob, 1.0, E_INVALID_ONE_QUBIT_DEPOL_PROB, __func__)) return;
+    const Kraus K0 = {1.0, 0.0, 0.0, std::sqrt(1.0 - prob)};
+    const Kraus K1 = {0.0, std::sqrt(prob), 0.0, 0.0};
+    recordChannel(q, &targetQubit, 1, {K0, K1});
+}
+
+// include/QuEST.h:1494: (1 - p) rho + p/15 (sum of the 15 non-identity
+// two-qubit Paulis P rho P)
+void applyTwoQubitDepolariseError(Qureg q, const int qubit1, const int qubit2, qreal prob) {
+    if (!vNoise(q, qubit1, prob, 15.0 / 16.0, E_INVALID_TWO_QUBIT_DEPOL_PROB, __func__) ||
+        !vUniqueTargets(q, qubit1, qubit2, __func__))
+        return;
+    const int qs[2] = {qubit1, qubit2};
+    std::vector<Kraus> ks;
+    for (int pa = 0; pa < 4; pa++)
+        for (int pb = 0; pb < 4; pb++)
+            ks.push_back(pauli2(pa, pb, pa == 0 && pb == 0 ? std::sqrt(1.0 - prob) : std::sqrt(prob / 15.0)));
+    recordChannel(q, qs, 2, ks);
+}
+
+// include/QuEST.h:1507: combineQureg := (1 - prob) combineQureg + prob
+// otherQureg (equal-size density matrices; on the host)
+void addDensityMatrix(Qureg combineQureg, qreal prob, Qureg otherQureg) {
+    if (!vDensity(combineQureg, __func__) || !vDensity(otherQureg, __func__)) return;
+    if (combineQureg.numQubitsRepresented != otherQureg.numQubitsRepresented) {
+        raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__);
+        return;
+    }
+    if (!(prob >= 0.0 && prob <= 1.0)) {
+        raise(E_INVALID_PROB, __func__);
+        return;
+    }
+    QuregState &a = *stateOf(combineQureg);
+    QuregState &b = *stateOf(otherQureg);
+    const size_t len = (size_t) 1 << a.numQubits;
+    std::vector<double> ar(len), ai(len), br(len), bi(len);
+    if (!readLogicalFor(a, ar.data(), ai.data(), __func__) || !readLogicalFor(b, br.data(), bi.data(), __func__))
+        return;
+    for (size_t i = 0; i < len; i++) {
+        ar[i] = (1.0 - prob) * ar[i] + prob * br[i];
+        ai[i] = (1.0 - prob) * ai[i] + prob * bi[i];
+    }
+    loadAmps(a, ar.data(), ai.data(), __func__);
+}
+
+// include/QuEST.h:1524: Tr(rho^2) = the sum of |rho_rc|^2 over all elements
+qreal calcPurity(Qureg q) {
+    if (!vDensity(q, __func__)) return 0.0;
     QuregState &s = *stateOf(q);
-    if (!flush(s, __func__)) return out;
-    const uint64_t v = toVirtualIndex(s, (uint64_t) index);
+    const size_t len = (size_t) 1 << s.numQubits;
+    std::vector<double> re(len), im(len);
+    if (!readLogicalFor(s, re.data(), im.data(), __func__)) return 0.0;
+    double t = 0.0;
+    for (size_t i = 0; i < len; i++) t += re[i] * re[i] + im[i] * im[i];
+    return t;
+}
+
+// ---------------------------------------------------------------- read-outs
+// Amplitude `index` of the register's vector (logical order; a density
+// register's vectorisation).
+static Complex ampAt(QuregState &s, uint64_t index, const char *func) {
+    Complex out{0.0, 0.0};
+    if (!flush(s, func)) return out;
+    const uint64_t v = toVirtualIndex(s, index);
     if (s.restrictActive && (v & s.rMask) != s.rValue) {
-        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+        if (!cudaOk(cudaStreamSynchronize(s.stream), func)) return out;
         return out;
     }
     double2 a;
@@ -1828,9 +2144,9 @@ Complex getAmp(Qureg q, long long int index) {
         // one amplitude from the shard that holds it
         if (s.single) {
             float2 f;
-            if (!dgq::shardReadVirtual(s, v, 1, &f, __func__)) return out;
+            if (!dgq::shardReadVirtual(s, v, 1, &f, func)) return out;
             a = make_double2(f.x, f.y);
-        } else if (!dgq::shardReadVirtual(s, v, 1, &a, __func__)) {
+        } else if (!dgq::shardReadVirtual(s, v, 1, &a, func)) {
             return out;
         }
     } else if (s.hostTier) {
@@ -1844,20 +2160,34 @@ Complex getAmp(Qureg q, long long int index) {
     } else if (s.single) {
         float2 f;
         if (!cudaOk(cudaMemcpyAsync(&f, (const float2 *) s.dState + v, sizeof(f), cudaMemcpyDeviceToHost, s.stream),
-                    __func__))
+                    func))
             return out;
-        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+        if (!cudaOk(cudaStreamSynchronize(s.stream), func)) return out;
         a = make_double2(f.x, f.y);
     } else {
         if (!cudaOk(cudaMemcpyAsync(&a, (const double2 *) s.dState + v, sizeof(a), cudaMemcpyDeviceToHost, s.stream),
-                    __func__))
+                    func))
             return out;
-        if (!cudaOk(cudaStreamSynchronize(s.stream), __func__)) return out;
+        if (!cudaOk(cudaStreamSynchronize(s.stream), func)) return out;
     }
     const double sc = s.restrictActive ? s.rScale : 1.0;
     out.real = a.x * sc;
     out.imag = a.y * sc;
     return out;
+}
+
+Complex getAmp(Qureg q, long long int index) {
+    if (!vStateVec(q, __func__) || !vStateIndex(q, index, __func__)) return Complex{0.0, 0.0};
+    return ampAt(*stateOf(q), (uint64_t) index, __func__);
+}
+
+// include/QuEST.h:591 (declared only in dgQuEST): element (row, col) of a
+// density matrix
+Complex getDensityAmp(Qureg q, long long int row, long long int col) {
+    if (!vDensity(q, __func__) || !vStateIndex(q, row, __func__) || !vStateIndex(q, col, __func__))
+        return Complex{0.0, 0.0};
+    QuregState &s = *stateOf(q);
+    return ampAt(s, (uint64_t) row + ((uint64_t) col << s.densityQubits), __func__);
 }
 qreal getRealAmp(Qureg q, long long int index) { return getAmp(q, index).real; }
 qreal getImagAmp(Qureg q, long long int index) { return getAmp(q, index).imag; }
@@ -1902,6 +2232,8 @@ qreal collapseToOutcome(Qureg q, const int measureQubit, int outcome) {
         return 0.0;
     }
     applyCollapse(s, v, outcome, prob);
+    // density registers: the column qubit too (P rho P / prob)
+    if (s.densityQubits) applyCollapse(s, s.l2v[measureQubit + s.densityQubits], outcome, prob);
     return prob;
 }
 
@@ -1924,6 +2256,7 @@ int measureWithStats(Qureg q, int measureQubit, qreal *outcomeProb) {
     const double prob = outcome == 0 ? zeroProb : 1 - zeroProb;
     if (outcomeProb) *outcomeProb = prob;
     applyCollapse(s, v, outcome, prob);
+    if (s.densityQubits) applyCollapse(s, s.l2v[measureQubit + s.densityQubits], outcome, prob);
     return outcome;
 }
 
@@ -2043,16 +2376,16 @@ void *dgq_getDeviceState(Qureg q, int *numBits) {
     return (void *) stateOf(q)->dState;
 }
 
-int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
-    if (!vQureg(q, __func__) || !re || !im) return -1;
-    QuregState &s = *stateOf(q);
-    if (!flush(s, __func__)) return -1;
+// The register's vector in logical order (collapse applied) into re/im
+// (2^numQubits entries; a density register's vectorisation).
+static bool readLogical(QuregState &s, double *re, double *im, const char *func) {
+    if (!flush(s, func)) return false;
     const uint64_t n = 1ULL << s.numQubits;
     if (s.hostTier || s.sharded) {
         // logical order through the map, from pinned host memory (shards:
         // from a host copy of the shards)
         std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
-        if (s.sharded && !dgq::shardReadVirtual(s, 0, 1ULL << s.numBits, staged.data(), __func__)) return -1;
+        if (s.sharded && !dgq::shardReadVirtual(s, 0, 1ULL << s.numBits, staged.data(), func)) return false;
         const void *src = s.sharded ? (const void *) staged.data() : s.hState;
         const double sc = s.restrictActive ? s.rScale : 1.0;
         for (uint64_t i = 0; i < n; i++) {
@@ -2068,11 +2401,11 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
             re[i] = keep ? a.x * sc : 0.0;
             im[i] = keep ? a.y * sc : 0.0;
         }
-        return 0;
+        return true;
     }
     const uint64_t chunk = std::min<uint64_t>(n, 1ULL << 22);
     double2 *dOut = nullptr;
-    if (!cudaOk(cudaMalloc(&dOut, chunk * sizeof(double2)), __func__)) return -1;
+    if (!cudaOk(cudaMalloc(&dOut, chunk * sizeof(double2)), func)) return false;
     std::vector<double2> host((size_t) chunk);
     dgq::GatherArgs ga;
     std::memset(&ga, 0, sizeof(ga));
@@ -2086,10 +2419,10 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
     for (uint64_t off = 0; off < n && ok; off += chunk) {
         ga.begin = off;
         ga.count = std::min(chunk, n - off);
-        ok = cudaOk(dgq::launchGather(s.dState, s.single, ga, dOut, s.stream), __func__) &&
+        ok = cudaOk(dgq::launchGather(s.dState, s.single, ga, dOut, s.stream), func) &&
              cudaOk(cudaMemcpyAsync(host.data(), dOut, ga.count * sizeof(double2), cudaMemcpyDeviceToHost, s.stream),
-                    __func__) &&
-             cudaOk(cudaStreamSynchronize(s.stream), __func__);
+                    func) &&
+             cudaOk(cudaStreamSynchronize(s.stream), func);
         g_launches++;
         for (uint64_t i = 0; ok && i < ga.count; i++) {
             re[off + i] = host[(size_t) i].x;
@@ -2097,14 +2430,30 @@ int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
         }
     }
     cudaFree(dOut);
-    return ok ? 0 : -1;
+    return ok;
 }
+
+int dgq_getStateVector(Qureg q, qreal *re, qreal *im) {
+    if (!vQureg(q, __func__) || !re || !im) return -1;
+    return readLogical(*stateOf(q), re, im, __func__) ? 0 : -1;
+}
+
+}  // extern "C"
+
+namespace {
+bool readLogicalFor(QuregState &s, double *re, double *im, const char *func) { return readLogical(s, re, im, func); }
+}  // namespace
+
+extern "C" {
+
 
 int dgq_calcProbOfAllZero(Qureg q, qreal *probs) {
     if (!vQureg(q, __func__) || !probs) return -1;
     QuregState &s = *stateOf(q);
     if (!ensureProbs(s, __func__)) return -1;
-    for (int i = 0; i < s.numQubits; i++) probs[i] = s.p0[(size_t) s.l2v[i]];
+    // density registers: the represented qubits (the row qubits)
+    const int count = s.densityQubits ? s.densityQubits : s.numQubits;
+    for (int i = 0; i < count; i++) probs[i] = s.p0[(size_t) s.l2v[i]];
     return 0;
 }
 
@@ -2297,7 +2646,7 @@ int dgq_compileSweepSource(const char *source, char *log, int len) {
 // src/QuEST.h:1306 (declared, no body in dgQuEST): <bra|ket> for state-vectors
 Complex calcInnerProduct(Qureg bra, Qureg ket) {
     Complex out{0.0, 0.0};
-    if (!vQureg(bra, __func__) || !vQureg(ket, __func__)) return out;
+    if (!vStateVec(bra, __func__) || !vStateVec(ket, __func__)) return out;
     QuregState &b = *stateOf(bra);
     QuregState &k = *stateOf(ket);
     if (b.numQubits != k.numQubits) {
@@ -2342,6 +2691,29 @@ Complex calcInnerProduct(Qureg bra, Qureg ket) {
 
 // src/QuEST.h:1539 (declared, no body in dgQuEST): |<pure|qureg>|^2 for state-vectors
 qreal calcFidelity(Qureg qureg, Qureg pureState) {
+    if (!vQureg(qureg, __func__) || !vQureg(pureState, __func__)) return 0.0;
+    if (qureg.isDensityMatrix) {
+        // <psi| rho |psi> on the host (include/QuEST.h:1539)
+        if (pureState.isDensityMatrix) return raise(E_SECOND_ARG_MUST_BE_STATEVEC, __func__), 0.0;
+        if (pureState.numQubitsRepresented != qureg.numQubitsRepresented)
+            return raise(E_MISMATCHING_QUREG_DIMENSIONS, __func__), 0.0;
+        QuregState &s = *stateOf(qureg);
+        const int n = s.densityQubits;
+        const uint64_t dim = 1ULL << n;
+        std::vector<double> re(dim * dim), im(dim * dim), pr(dim), pi(dim);
+        if (!readLogicalFor(s, re.data(), im.data(), __func__) ||
+            !readLogicalFor(*stateOf(pureState), pr.data(), pi.data(), __func__))
+            return 0.0;
+        std::complex<double> f = 0.0;
+        for (uint64_t c = 0; c < dim; c++) {
+            std::complex<double> row = 0.0;  // (rho psi)_r summed against conj(psi_r) below
+            for (uint64_t r = 0; r < dim; r++)
+                row += std::conj(std::complex<double>(pr[r], pi[r])) *
+                       std::complex<double>(re[r + (c << n)], im[r + (c << n)]);
+            f += row * std::complex<double>(pr[c], pi[c]);
+        }
+        return f.real();
+    }
     const Complex ip = calcInnerProduct(qureg, pureState);
     return ip.real * ip.real + ip.imag * ip.imag;
 }

@@ -400,6 +400,7 @@ dgq_batch dgq_batchCreate(const Qureg *quregs, int count, const dgq_batch_config
         if (!s) return abandon(E_INVALID_ARGUMENT, "a register handle is not initialised");
         if (s->hostTier) return abandon(E_UNSUPPORTED, "a register held in host memory");
         if (s->sharded) return abandon(E_UNSUPPORTED, "a sharded register");
+        if (s->densityQubits) return abandon(E_UNSUPPORTED, "a density matrix");
         b->regs[i] = s;
         if (i == 0) b->single = s->single;
         if (s->single != b->single) return abandon(E_UNSUPPORTED, "a batch holds registers of one precision");

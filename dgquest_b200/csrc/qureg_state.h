@@ -18,7 +18,11 @@
 #include "tile_program.h"
 
 struct QuregState {
-    int numQubits = 0;  // user-visible qubits
+    int numQubits = 0;  // user-visible qubits (density registers: 2 x densityQubits)
+    // density matrix of densityQubits qubits (0: a state vector), held as the
+    // state vector of its 2 x densityQubits-qubit vectorisation: element
+    // (row r, column c) at index r + (c << densityQubits)
+    int densityQubits = 0;
     int numBits = 0;    // address bits of the buffer (>= numQubits, >= kMinTileBits)
     bool single = false;  // complex64 amplitudes (float2) instead of complex128
     void *dState = nullptr;

@@ -197,6 +197,15 @@ _SIGS = {
     "dgq_calcProbOfAllZero": (I, [Q, P(D)]),
     "dgq_measureFp64Peak": (I, [P(D)]),
     "dgq_createQuregF32": (Qureg, [I, E]),
+    "createDensityQureg": (Qureg, [I, E]),
+    "getDensityAmp": (Complex, [Q, ctypes.c_longlong, ctypes.c_longlong]),
+    "calcPurity": (D, [Q]),
+    "applyOneQubitDephaseError": (None, [Q, I, D]),
+    "applyTwoQubitDephaseError": (None, [Q, I, I, D]),
+    "applyOneQubitDepolariseError": (None, [Q, I, D]),
+    "applyOneQubitDampingError": (None, [Q, I, D]),
+    "applyTwoQubitDepolariseError": (None, [Q, I, I, D]),
+    "addDensityMatrix": (None, [Q, D, Q]),
     "dgq_getPrecision": (I, [Q]),
     "dgq_sweepSource": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I, I,
                             ctypes.c_char_p, I]),
@@ -297,12 +306,19 @@ def matrixN(u):
 
 
 def state_vector(q):
-    """All amplitudes of q in logical order, as a complex128 numpy array."""
-    n = int(q.numQubitsRepresented)
+    """All amplitudes of q in logical order, as a complex128 numpy array (a
+    density register: its 4^n elements, element (r, c) at r + c * 2^n)."""
+    n = int(q.numQubitsInStateVec)
     re = np.empty(1 << n, dtype=np.float64)
     im = np.empty(1 << n, dtype=np.float64)
     dgq_getStateVector(q, re.ctypes.data_as(POINTER(c_double)), im.ctypes.data_as(POINTER(c_double)))
     return re + 1j * im
+
+
+def density_matrix(q):
+    """The density matrix of a density register as a 2^n x 2^n array."""
+    dim = 1 << int(q.numQubitsRepresented)
+    return state_vector(q).reshape(dim, dim).T
 
 
 def prob_all_zero(q):

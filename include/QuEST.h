@@ -81,6 +81,10 @@ int getQuEST_PREC(void);                              /* src/QuEST.c:456-458 */
 
 /* ---- registers -------------------------------------------------------- */
 Qureg createQureg(int numQubits, QuESTEnv env);       /* include/QuEST.h:125 */
+/* declared only in dgQuEST; upstream QuEST's representation: an n-qubit
+ * density matrix held as the 2n-qubit vector of its elements, element
+ * (row r, column c) at index r + (c << n); gates act as U rho U^dagger */
+Qureg createDensityQureg(int numQubits, QuESTEnv env); /* include/QuEST.h:139 */
 void searchQuregTaskPartitions(Qureg qureg, QuESTEnv env); /* include/QuEST.h:127 */
 void destroyQureg(Qureg qureg, QuESTEnv env);         /* include/QuEST.h:148 */
 int getNumQubits(Qureg qureg);                        /* include/QuEST.h:187 */
@@ -153,6 +157,16 @@ int measure(Qureg qureg, int measureQubit);                   /* include/QuEST.h
 int measureWithStats(Qureg qureg, int measureQubit, qreal *outcomeProb); /* include/QuEST.h:1303 */
 Complex calcInnerProduct(Qureg bra, Qureg ket);                 /* include/QuEST.h:1306 (declared only in dgQuEST) */
 qreal calcFidelity(Qureg qureg, Qureg pureState);               /* include/QuEST.h:1539 (declared only in dgQuEST) */
+
+/* ---- density matrices (declared only in dgQuEST) ------------------------ */
+Complex getDensityAmp(Qureg qureg, long long int row, long long int col); /* include/QuEST.h:591 */
+qreal calcPurity(Qureg qureg);                                  /* include/QuEST.h:1524 */
+void applyOneQubitDephaseError(Qureg qureg, const int targetQubit, qreal prob); /* include/QuEST.h:1373 */
+void applyTwoQubitDephaseError(Qureg qureg, const int qubit1, const int qubit2, qreal prob); /* :1399 */
+void applyOneQubitDepolariseError(Qureg qureg, const int targetQubit, qreal prob); /* include/QuEST.h:1423 */
+void applyOneQubitDampingError(Qureg qureg, const int targetQubit, qreal prob); /* include/QuEST.h:1445 */
+void applyTwoQubitDepolariseError(Qureg qureg, const int qubit1, const int qubit2, qreal prob); /* :1494 */
+void addDensityMatrix(Qureg combineQureg, qreal prob, Qureg otherQureg); /* include/QuEST.h:1507 */
 
 #ifdef __cplusplus
 }
