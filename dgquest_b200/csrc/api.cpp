@@ -773,17 +773,56 @@ bool vDeviceResident(const QuregState &s, const char *func) {
 
 bool readLogicalFor(QuregState &s, double *re, double *im, const char *func);
 
-// Density registers: P(row qubit t = 0) and the trace from the diagonal,
-// read on the host (the whole vectorisation: 16 x 4^n bytes).
+// The diagonal of a device-resident density register, rho(i, i) = entry
+// i (2^n + 1) of the vectorisation, gathered on the device: 2^n complex
+// values cross to the host instead of 4^n.
+bool densityDiagonal(QuregState &s, std::vector<double> &diag, const char *func) {
+    const int n = s.densityQubits;
+    const uint64_t dim = 1ULL << n;
+    double2 *dOut = nullptr;
+    if (!cudaOk(cudaMallocAsync((void **) &dOut, dim * sizeof(double2), s.stream), func)) return false;
+    dgq::GatherArgs ga;
+    std::memset(&ga, 0, sizeof(ga));
+    ga.begin = 0;
+    ga.count = dim;
+    ga.stride = dim + 1;
+    ga.numReal = s.numQubits;
+    ga.hasRestrict = s.restrictActive ? 1 : 0;
+    ga.restrictMask = s.rMask;
+    ga.restrictValue = s.rValue;
+    ga.restrictScale = s.rScale;
+    for (int b = 0; b < s.numQubits; b++) ga.l2v[b] = (uint8_t) s.l2v[b];
+    std::vector<double2> host((size_t) dim);
+    const bool ok = cudaOk(dgq::launchGather(s.dState, s.single, ga, dOut, s.stream), func) &&
+                    cudaOk(cudaMemcpyAsync(host.data(), dOut, dim * sizeof(double2), cudaMemcpyDeviceToHost, s.stream),
+                           func);
+    g_launches++;
+    cudaFreeAsync(dOut, s.stream);
+    if (!ok || !cudaOk(cudaStreamSynchronize(s.stream), func)) return false;
+    diag.resize((size_t) dim);
+    for (uint64_t i = 0; i < dim; i++) diag[(size_t) i] = host[(size_t) i].x;
+    return true;
+}
+
+// Density registers: P(row qubit t = 0) and the trace from the diagonal
+// (gathered on the device; a register in host memory reads its whole
+// vectorisation, 16 x 4^n bytes).
 bool densityProbs(QuregState &s, const char *func) {
     const int n = s.densityQubits;
     const uint64_t dim = 1ULL << n;
-    std::vector<double> re(dim * dim), im(dim * dim);
-    if (!readLogicalFor(s, re.data(), im.data(), func)) return false;
+    std::vector<double> diag;
+    if (s.hostTier || s.sharded) {
+        std::vector<double> re(dim * dim), im(dim * dim);
+        if (!readLogicalFor(s, re.data(), im.data(), func)) return false;
+        diag.resize((size_t) dim);
+        for (uint64_t i = 0; i < dim; i++) diag[(size_t) i] = re[i + (i << n)];
+    } else if (!densityDiagonal(s, diag, func)) {
+        return false;
+    }
     std::vector<double> p0((size_t) n, 0.0);
     double total = 0.0;
     for (uint64_t i = 0; i < dim; i++) {
-        const double d = re[i + (i << n)];
+        const double d = diag[(size_t) i];
         total += d;
         for (int t = 0; t < n; t++)
             if (!((i >> t) & 1ULL)) p0[(size_t) t] += d;
@@ -2071,7 +2110,8 @@ void applyOneQubitDepolariseError(Qureg q, const int targetQubit, qreal prob) {
 // include/QuEST.h:1445: amplitude damping (decay to |0>) with probability p:
 // Kraus operators [[1, 0], [0, sqrt(1 - p)]] and [[0, sqrt(p)], [0, 0]]
 void applyOneQubitDampingError(Qureg q, const int targetQubit, qreal prob) {
-    if (!vNoise(q, targetQubit, prob, 1.0, E_INVALID_ONE_QUBIT_DEPOL_PROB, __func__)) return;
+    // any probability in [0, 1] is valid; vNoise reports the rest as E_INVALID_PROB
+    if (!vNoise(q, targetQubit, prob, 1.0, E_INVALID_PROB, __func__)) return;
     const Kraus K0 = {1.0, 0.0, 0.0, std::sqrt(1.0 - prob)};
     const Kraus K1 = {0.0, std::sqrt(prob), 0.0, 0.0};
     recordChannel(q, &targetQubit, 1, {K0, K1});
@@ -2530,6 +2570,41 @@ int dgq_fuseApplyHost(int numQubits, int K, int count, const int32_t *types, con
     return blocks;
 }
 
+// Gates given in dgQuEST's IR encoding through the host-only entry points
+// (dgq_planGates, dgq_sweepSource), checked before the planner sees them:
+// types 0..18 except the unused 9 (the multi-qubit unitary needs a matrix
+// pool these calls do not take), masks inside the register, disjoint target
+// and control masks, one target bit for Rz and the non-diagonal types, and
+// no target but at least one qubit for the diagonal phase types.
+static bool gatesFromArrays(int numQubits, int count, const int32_t *types, const uint64_t *targetMasks,
+                            const uint64_t *controlMasks, const double *operands, std::vector<Gate> &out,
+                            const char *func) {
+    const u64 all = numQubits >= 64 ? ~0ULL : (1ULL << numQubits) - 1;
+    out.clear();
+    out.reserve((size_t) count);
+    for (int i = 0; i < count; i++) {
+        const int t = types[i];
+        const u64 tm = targetMasks[i], cm = controlMasks[i];
+        bool ok = t >= 0 && t <= dgq::OP_UNITARY && t != dgq::OP_RESERVED_9 && !((tm | cm) & ~all) && !(tm & cm);
+        if (ok && t >= dgq::OP_ROTATE_Z) ok = tm != 0 && (tm & (tm - 1)) == 0;
+        if (ok && t < dgq::OP_ROTATE_Z) ok = tm == 0 && cm != 0;
+        if (!ok) {
+            char msg[160];
+            snprintf(msg, sizeof msg, "gate %d: type %d, target mask 0x%llx, control mask 0x%llx is not a valid gate", i,
+                     t, (unsigned long long) tm, (unsigned long long) cm);
+            raise(E_INVALID_ARGUMENT, func, msg);
+            return false;
+        }
+        Gate g;
+        g.type = (dgq::GateType) t;
+        g.targetMask = tm;
+        g.controlMask = cm;
+        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
+        out.push_back(g);
+    }
+    return true;
+}
+
 int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, const uint64_t *targetMasks,
                   const uint64_t *controlMasks, const double *operands, dgq_plan_stats *out, int32_t *mergedTypes,
                   int32_t *numMerged) {
@@ -2543,14 +2618,7 @@ int dgq_planGates(int numQubits, int tileBits, int count, const int32_t *types, 
     s.numBits = std::max(numQubits, dgq::kMinTileBits);
     resetMapping(s);
     s.tileBitsSetting = tileBits;
-    for (int i = 0; i < count; i++) {
-        Gate g;
-        g.type = (dgq::GateType) types[i];
-        g.targetMask = targetMasks[i];
-        g.controlMask = controlMasks[i];
-        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
-        s.pending.push_back(g);
-    }
+    if (!gatesFromArrays(numQubits, count, types, targetMasks, controlMasks, operands, s.pending, __func__)) return -1;
     if (mergedTypes || numMerged) {
         dgq::GateDag dag(s.numBits, true);
         for (const Gate &g : s.pending) dag.add(g);
@@ -2611,14 +2679,11 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
     s.allowPaired = precision == 1;
     resetMapping(s);
     s.tileBitsSetting = tileBits;
-    for (int i = 0; i < count; i++) {
-        Gate g;
-        g.type = (dgq::GateType) types[i];
-        g.targetMask = targetMasks[i];
-        g.controlMask = controlMasks[i];
-        for (int k = 0; k < 8; k++) g.op[k] = operands[8 * i + k];
-        s.pending.push_back(g);
+    if (count > 0 && (!types || !targetMasks || !controlMasks || !operands)) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
     }
+    if (!gatesFromArrays(numQubits, count, types, targetMasks, controlMasks, operands, s.pending, __func__)) return -1;
     s.initPending = true;
     s.initKind = dgq::INIT_CLASSICAL;
     const bool ok = planPending(s, __func__, false);

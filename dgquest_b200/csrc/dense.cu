@@ -161,13 +161,10 @@ __global__ void __launch_bounds__(256, 2) denseKernel(V *__restrict__ st, const 
 template <class V, int K>
 cudaError_t launchDenseVK(V *st, const DenseArgs &a, const double *U, cudaStream_t s) {
     const size_t smem = (sizeof(V) << a.tileBits) + sizeof(V) * kDenseChunk * (1u << K);
-    static bool attrSet = false;
-    if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(denseKernel<V, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int) ((sizeof(V) << kDenseTileBits) + sizeof(V) * kDenseChunk * (1u << 7)));
-        if (e != cudaSuccess) return e;
-        attrSet = true;
-    }
+    static std::atomic<uint64_t> optIn{0};
+    cudaError_t e = ensureSmemOptIn((const void *) denseKernel<V, K>,
+                                    (int) ((sizeof(V) << kDenseTileBits) + sizeof(V) * kDenseChunk * (1u << 7)), optIn);
+    if (e != cudaSuccess) return e;
     const unsigned grid = 1u << (a.numBits - a.tileBits);
     denseKernel<V, K><<<grid, 256, smem, s>>>(st, a, U);
     return cudaGetLastError();

@@ -137,14 +137,10 @@ __global__ void __launch_bounds__(1 << (W - kRegBits), 65536 / (128 << (W - kReg
 
 template <int W, class V, bool LEAN>
 static cudaError_t launchTileWL(V *st, const TileProgram &prog, cudaStream_t s) {
-    static bool attrSet = false;
+    static std::atomic<uint64_t> optIn{0};
     const size_t smem = sizeof(V) << W;
-    if (!attrSet) {
-        cudaError_t e =
-            cudaFuncSetAttribute(tileKernel<W, V, LEAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        if (e != cudaSuccess) return e;
-        attrSet = true;
-    }
+    cudaError_t e = ensureSmemOptIn((const void *) tileKernel<W, V, LEAN>, (int) smem, optIn);
+    if (e != cudaSuccess) return e;
     const unsigned grid = prog.ctaCount ? prog.ctaCount : 1u << (prog.numBits - W);
     tileKernel<W, V, LEAN><<<grid, 1 << (W - kRegBits), smem, s>>>(st, prog);
     return cudaGetLastError();
@@ -419,7 +415,7 @@ template <class V>
 __global__ void gatherKernel(const V *__restrict__ st, const __grid_constant__ GatherArgs args, double2 *__restrict__ out) {
     for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < args.count;
          i += (uint64_t) gridDim.x * blockDim.x) {
-        const uint64_t l = args.begin + i;
+        const uint64_t l = args.begin + i * (args.stride ? args.stride : 1ULL);
         uint64_t v = 0;
         for (int b = 0; b < args.numReal; b++) v |= ((l >> b) & 1ULL) << args.l2v[b];
         double2 x = make_double2((double) st[v].x, (double) st[v].y);

@@ -7,6 +7,28 @@
 
 #include "tile_program.h"
 
+#include <atomic>
+
+namespace dgq {
+
+// Dynamic shared memory above 48 KiB must be opted into per kernel and per
+// device (cudaFuncSetAttribute applies to the current device). `done` holds
+// one bit per device ordinal (< 64) for which the opt-in has been made;
+// concurrent callers may both set the attribute, which is harmless.
+inline cudaError_t ensureSmemOptIn(const void *func, int bytes, std::atomic<uint64_t> &done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev < 64 ? (1ULL << dev) : 0ULL;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    if (bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return cudaSuccess;
+}
+
+}  // namespace dgq
+
 namespace dgq {
 
 struct ProbArgs {
@@ -25,6 +47,7 @@ struct SwapArgs {
 
 struct GatherArgs {
     uint64_t begin, count;
+    uint64_t stride;  // logical index of entry i: begin + i * stride (0 means 1)
     int32_t numReal;
     int32_t hasRestrict;
     uint64_t restrictMask, restrictValue;

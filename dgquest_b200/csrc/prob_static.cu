@@ -5,14 +5,15 @@
 // per-CTA partial sums) lives in the file-scope device array below instead
 // of a buffer from cudaMalloc. It is meant for callers that must not
 // allocate GPU memory while they call us:
-//   * code being recorded into a CUDA graph (cudaMalloc/cudaFree are not
-//     allowed while a stream is capturing),
 //   * hosts that reserve all device memory up front and hand out pieces
 //     themselves (a framework's caching allocator, a serving process with a
 //     fixed HBM budget), where an allocation behind their back can fail or
 //     fragment their pool,
 //   * latency-sensitive loops, where cudaMalloc/cudaFree would synchronise
 //     the device.
+// The state and the output must live on the device that is current when
+// the call is made (checked with cudaPointerGetAttributes, a host query);
+// the scratch is that device's copy of the array.
 // The array holds kStaticProbCtas x 17 doubles (2,228,224 bytes = 2.125 MiB)
 // and stays resident on every GPU that loads libdgq until the process exits.
 // That bounds the state to 2^30 amplitudes (numBits <= 30). All calls share
@@ -63,6 +64,22 @@ extern "C" int dgq_calcProbOfAllZeroNoAlloc(const void *deviceState, int numBits
     if (e != cudaSuccess || dev < 0 || dev >= 64) {
         raiseExternal(103, __func__, e != cudaSuccess ? cudaGetErrorString(e) : "device ordinal >= 64");
         return -2;
+    }
+    // both buffers on the current device: the scratch is this device's array,
+    // and a pointer into another GPU would make the kernels read peer memory
+    for (const void *p : {deviceState, (const void *) deviceProbs}) {
+        cudaPointerAttributes at;
+        e = cudaPointerGetAttributes(&at, p);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            raiseExternal(104, __func__, "state or output pointer is not CUDA memory");
+            return -1;
+        }
+        if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) ||
+            (at.type == cudaMemoryTypeDevice && at.device != dev)) {
+            raiseExternal(104, __func__, "state and output must be device memory of the current device");
+            return -1;
+        }
     }
     double *scratch = nullptr;
     {

@@ -246,7 +246,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         parity ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         __syncthreads();
-        if (abort) break;
+        if (abort) {
+            // the committed MMAs may still be writing tensor memory: before it
+            // is released below, wait once more (bounded) for their commit
+            // (the phase just waited on), and skip this tile's epilogue
+            waitParity(mbarAddr, parity ^ 1u, 1u << 24);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            break;
+        }
         // D row (lane) 32 w + t: Re Y[row] for rows < 64, Im Y[row - 64] above
         const uint32_t m = warp * 32 + lane;
         float *ysf = reinterpret_cast<float *>(xs);
@@ -342,12 +349,9 @@ uint32_t *tcDenseErrorWord() {
 
 cudaError_t launchTcDense(float2 *st, const DenseArgs &a, const float *Apacked, uint32_t *error, cudaStream_t s) {
     if (a.tileBits != 12 || !error) return cudaErrorInvalidValue;
-    static bool attrSet = false;
-    if (!attrSet) {
-        cudaError_t e = cudaFuncSetAttribute(tcDenseKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kTcSmem);
-        if (e != cudaSuccess) return e;
-        attrSet = true;
-    }
+    static std::atomic<uint64_t> optIn{0};
+    cudaError_t e = ensureSmemOptIn((const void *) tcDenseKernel, (int) kTcSmem, optIn);
+    if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

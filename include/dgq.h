@@ -167,20 +167,24 @@ int dgq_measureFp64Peak(double *tflops);
 
 /* P(address bit = 0) for every bit of a state the caller owns, computed
  * without allocating any GPU memory. No counterpart in dgQuEST: it serves
- * callers that cannot call cudaMalloc while they call this library (a
- * stream being captured into a CUDA graph, hosts that manage all device
- * memory themselves, latency-bound loops where an allocation would
- * synchronise the device). deviceState: 2^numBits interleaved complex128
- * amplitudes in device memory; deviceProbs: numBits + 1 doubles in device
- * memory, receiving P(bit b = 0) for b < numBits and the total probability
- * last; stream: a cudaStream_t (NULL = default stream); results are ready
- * when the stream reaches them. The partial sums go to a static device
- * array of 16384 x 17 doubles (2.125 MiB, resident on every GPU that loads
- * the library), so numBits is limited to 1..30; larger states are rejected.
- * The first call on each device looks up that array's address (make it
- * before any stream capture). Calls share the array: calls that overlap on
- * the GPU race. Returns 0, or -1 (invalid argument / too large) or -2 (CUDA
- * error), reported like every other error of this library. */
+ * callers that cannot call cudaMalloc while they call this library (hosts
+ * that manage all device memory themselves, such as a framework's caching
+ * allocator or a server with a fixed HBM budget, where an allocation behind
+ * their back can fail or fragment their pool; latency-bound loops where an
+ * allocation would synchronise the device). deviceState: 2^numBits
+ * interleaved complex128 amplitudes in device memory; deviceProbs:
+ * numBits + 1 doubles in device memory, receiving P(bit b = 0) for
+ * b < numBits and the total probability last. Both must be memory of the
+ * device that is current at the call (checked; another GPU's memory is
+ * rejected). stream: a cudaStream_t (NULL = default stream); results are
+ * ready when the stream reaches them. The partial sums go to a static
+ * device array of 16384 x 17 doubles (2.125 MiB, resident on every GPU that
+ * loads the library until the process exits), so numBits is limited to
+ * 1..30; larger states are rejected. The first call on each device looks up
+ * that array's device address (make that first call before any stream
+ * capture). Calls share the array: calls that overlap on the GPU race.
+ * Returns 0, or -1 (invalid argument / too large) or -2 (CUDA error),
+ * reported like every other error of this library. */
 int dgq_calcProbOfAllZeroNoAlloc(const void *deviceState, int numBits, double *deviceProbs, void *stream);
 
 /* Host-only planning (no GPU call): plans `count` gates given in dgQuEST's

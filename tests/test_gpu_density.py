@@ -203,3 +203,31 @@ def test_density_only_and_state_vector_only_calls(quest, env):
     finally:
         quest.destroyQureg(q, env)
         quest.destroyQureg(v, env)
+
+
+def test_noise_channel_probability_errors(quest, env):
+    # each channel's own limit raises its own QuEST message; a probability
+    # outside [0, 1] raises the generic one (QuEST_validation.c messages)
+    q = quest.createDensityQureg(3, env)
+    generic = "Probabilities must be in [0, 1]."
+    cases = [
+        (lambda p: quest.applyOneQubitDephaseError(q, 0, p), 0.6, "single qubit dephase"),
+        (lambda p: quest.applyTwoQubitDephaseError(q, 0, 1, p), 0.8, "two-qubit qubit dephase"),
+        (lambda p: quest.applyOneQubitDepolariseError(q, 0, p), 0.8, "single qubit depolarising"),
+        (lambda p: quest.applyTwoQubitDepolariseError(q, 0, 1, p), 0.95, "two-qubit depolarising"),
+        (lambda p: quest.applyOneQubitDampingError(q, 0, p), None, None),
+    ]
+    try:
+        for call, above, words in cases:
+            if above is not None:
+                with pytest.raises(quest.QuESTError) as ei:
+                    call(above)
+                assert words in ei.value.message, ei.value.message
+            for bad in (-0.1, 1.5):
+                with pytest.raises(quest.QuESTError) as ei:
+                    call(bad)
+                assert ei.value.message == generic, ei.value.message
+        quest.applyOneQubitDampingError(q, 0, 1.0)  # full decay is a valid channel
+        assert abs(quest.calcTotalProb(q) - 1.0) <= TOL
+    finally:
+        quest.destroyQureg(q, env)

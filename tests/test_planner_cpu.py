@@ -63,3 +63,34 @@ def test_generated_sweeps_compile(w, precision):
         assert size > 0, log.value.decode()
     # precision 1 selects the paired complex64 form (float4 slots)
     assert all((b"float4 sm[]" in s) == (precision == 1) for s in srcs)
+
+
+@pytest.mark.parametrize("bad", ["multi_unitary_type", "type_out_of_range", "mask_beyond_register",
+                                 "empty_target", "target_is_control"])
+def test_plan_gates_rejects_invalid_gates(bad):
+    # the host-only planner takes raw IR arrays: a gate it cannot encode is an
+    # E_INVALID_ARGUMENT error, not undefined behaviour in the planner
+    n = 12
+    t, tm, cm, o = ir.ops_to_ir(C.random_layers(n, 2, 3), n)
+    i = 5
+    assert t[i] in (ir.OP_RX, ir.OP_RY, ir.OP_RZ)
+    if bad == "multi_unitary_type":
+        t[i] = 19
+    elif bad == "type_out_of_range":
+        t[i] = 27
+    elif bad == "mask_beyond_register":
+        tm[i] = np.uint64(1 << n)
+    elif bad == "empty_target":
+        tm[i] = np.uint64(0)
+    else:
+        cm[i] = tm[i]
+    st = Q.PlanStats()
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_planGates(n, 0, len(t), t.ctypes.data_as(P(ctypes.c_int32)), tm.ctypes.data_as(P(ctypes.c_uint64)),
+                        cm.ctypes.data_as(P(ctypes.c_uint64)), o.ctypes.data_as(P(ctypes.c_double)),
+                        ctypes.byref(st), None, None)
+    buf = ctypes.create_string_buffer(1 << 16)
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_sweepSource(n, 0, len(t), t.ctypes.data_as(P(ctypes.c_int32)), tm.ctypes.data_as(P(ctypes.c_uint64)),
+                          cm.ctypes.data_as(P(ctypes.c_uint64)), o.ctypes.data_as(P(ctypes.c_double)), 0, 2, buf,
+                          len(buf))

@@ -1,13 +1,16 @@
 """The allocation-free probability entry point.
 
 dgq_calcProbOfAllZeroNoAlloc serves callers that cannot allocate GPU memory
-while they call the library (graph capture, hosts that own all device
-memory, latency-bound loops): its scratch is a static device array. This
-file is collected last so a failure here comes after every other test.
-It checks, through the C ABI, that the entry point agrees with the regular
-read-out (dgq_calcProbOfAllZero) on two calls in a row (two different
-states, so stale scratch from the first call would show in the second),
-and that it rejects states larger than its scratch holds.
+while they call the library (hosts that own all device memory, such as a
+caching allocator or a server with a fixed HBM budget; latency-bound loops
+where cudaMalloc would synchronise the device): its scratch is a static
+device array. This file is collected last so a failure here comes after
+every other test. It checks, through the C ABI, that the entry point agrees
+with the regular read-out (dgq_calcProbOfAllZero) on two calls in a row
+(two different states, so stale scratch from the first call would show in
+the second), that it rejects states larger than its scratch holds, and that
+it rejects buffers that are not memory of the current device (a host query,
+before any launch).
 """
 import ctypes
 
@@ -56,4 +59,15 @@ def test_no_alloc_rejects_oversized_state(quest, env):
     with pytest.raises(quest.QuESTError) as ei:
         quest.dgq_calcProbOfAllZeroNoAlloc(dstate, 31, dstate, None)
     assert "1..30" in ei.value.message
+    quest.destroyQureg(q, env)
+
+
+def test_no_alloc_rejects_host_memory(quest, env):
+    q = quest.createQureg(10, env)
+    nb = ctypes.c_int(0)
+    dstate = quest.dgq_getDeviceState(q, ctypes.byref(nb))
+    host = np.zeros(nb.value + 1, dtype=np.float64)
+    with pytest.raises(quest.QuESTError) as ei:
+        quest.dgq_calcProbOfAllZeroNoAlloc(dstate, nb.value, host.ctypes.data, None)
+    assert "current device" in ei.value.message or "not CUDA memory" in ei.value.message
     quest.destroyQureg(q, env)
