@@ -19,7 +19,11 @@ Inputs are larger than L2 (16 GiB state vs 126 MB L2), so no flush is needed.
 With --gpus N (torchrun), each rank runs an independent replica (the path
 does not shard on one GPU); the time is the max over ranks.
 `--impl reference` times the reference's algorithm on the host cores instead
-(the CPU oracle, OpenMP on all cores, on a bounded sample of the circuit).
+(the CPU oracle, OpenMP on all cores, one complete layer of the circuit per
+step; the circuit time is the mean layer time x 20). The default run also
+times dgQuEST's own GPU path on the same circuit (`reference_gpu`: the
+reference built from its sources, oracle/_ref/ref_harness) and the CPU
+oracle on one layer with all cores and one (`cpu_baseline`).
 """
 import argparse
 import ctypes
@@ -134,42 +138,78 @@ def max_over_ranks(x, world):
 
 
 # ---------------------------------------------------------------- CPU legs
-def cpu_sample(ops, n, gates, threads=None):
-    """Times the oracle on the first `gates` calls of the circuit (state of n qubits)."""
+def layer_of(ops, n, layer):
+    """The ops of one layer of the random circuit: n rotations, then n/2 CZ."""
+    per = n + n // 2
+    return ops[layer * per:(layer + 1) * per]
+
+
+def cpu_time_ops(n, samples, threads):
+    """Times the oracle (OpenMP, `threads` threads) applying each op list of
+    `samples` in turn to one n-qubit state; returns the seconds of each."""
     import oracle
-    if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
+    oracle.set_threads(threads)
     o = oracle.Oracle(n)
-    sample = ops[:gates]
-    t0 = time.perf_counter()
-    o.apply(sample)
-    dt = time.perf_counter() - t0
+    out = []
+    for sample in samples:
+        t0 = time.perf_counter()
+        o.apply(sample)
+        out.append(time.perf_counter() - t0)
     o.close()
-    return dt, oracle.max_threads()
+    return out
+
+
+def cpu_one_core_layer(ops, n):
+    """One-core estimate of a layer's time: one op of each kind the layer
+    holds (Rx, Ry, Rz, CZ; qubits from the middle of the register) timed on
+    one thread, weighted by the kind counts of layer 0. Returns (seconds per
+    layer, description)."""
+    from dgquest_b200 import circuits as C
+    layer = layer_of(ops, n, 0)
+    kinds = [int(k) for k in layer["kind"]]
+    counts = {k: kinds.count(k) for k in set(kinds)}
+    reps = []
+    for k in sorted(counts):
+        idx = [i for i, kk in enumerate(kinds) if kk == k]
+        reps.append(layer[idx[len(idx) // 2]:idx[len(idx) // 2] + 1])
+    times = cpu_time_ops(n, reps, 1)
+    per_kind = dict(zip(sorted(counts), times))
+    t_layer = sum(counts[k] * per_kind[k] for k in counts)
+    names = {C.RX: "Rx", C.RY: "Ry", C.RZ: "Rz", C.CZ: "CZ"}
+    desc = ("1 thread: one op of each kind of layer 0 timed (" +
+            ", ".join(f"{names.get(k, k)} {per_kind[k]:.2f} s x {counts[k]}" for k in sorted(counts)) +
+            f"), weighted by the layer's kind counts; x {len(ops) // len(layer)} layers")
+    return t_layer, desc
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's algorithm on the host cores: dgQuEST has no CPU
+    executor for this path, so the oracle port (plain C + OpenMP, all host
+    threads) applies the circuit gate by gate. Each step applies one
+    complete layer of the 30-qubit circuit (30 rotations + 15 CZ, layers in
+    turn); circuits/s = 1 / (mean layer time x 20 layers)."""
     from dgquest_b200 import circuits as C
     if rank != 0:
         return
+    import oracle
     ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))
-    gates = args.ref_gates
-    for _ in range(args.warmup):
-        cpu_sample(ops, N_QUBITS, max(1, gates // 4))
-    times = []
-    cores = 1
-    for _ in range(args.steps):
-        dt, cores = cpu_sample(ops, N_QUBITS, gates)
-        times.append(dt)
-    t = float(np.mean(times))
-    circuits_per_s = (gates / len(ops)) / t
-    sample = f"first {gates} of {len(ops)} gate calls of the 30-qubit circuit per step, scaled by {len(ops)}/{gates}"
+    cores = oracle.max_threads()
+    warm = [ops[:2]] * max(0, args.warmup)  # warm-up: two gates each (pages the state in)
+    samples = warm + [layer_of(ops, N_QUBITS, i % DEPTH) for i in range(args.steps)]
+    times = cpu_time_ops(N_QUBITS, samples, cores)[len(warm):]
+    t_layer = float(np.mean(times))
+    circuit_s = t_layer * DEPTH
+    circuits_per_s = 1.0 / circuit_s
+    sample = (f"{args.steps} complete layers (30 rotations + 15 CZ each) of the 30-qubit circuit, one per step; "
+              f"circuit time = mean layer time x {DEPTH}")
     line = {"metric": METRIC, "value": circuits_per_s, "unit": "circuits/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * len(ops) / gates * 1000.0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_layer * 1000.0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded MT19937 random circuit)", "impl": "reference",
             "config": {"workload": "random circuit n=30 depth=20 (Rx/Ry/Rz + CZ matching), complex128",
                        "qubits": N_QUBITS, "depth": DEPTH, "parallelism": "host cores"},
+            "extrapolated": True, "fraction_of_circuit_timed": args.steps / DEPTH,
+            "layer_seconds": times,
             "cpu_baseline": {"value": circuits_per_s, "unit": "circuits/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": circuits_per_s, "unit": "circuits/s", "h2d_bytes_per_step": 0,
@@ -177,8 +217,50 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args):
+    """dgQuEST's own GPU path, built from the reference's sources for sm_100a
+    (oracle/_ref/ref_harness, `make -C oracle ref`), on the same circuit and
+    GPU: its QuEST calls, searchQuregTaskPartitions and getAmp(q, 0) with
+    K = 5 (QuEST.conf "5 5 5"), timed by the harness around getAmp. Also
+    reads 64 sampled amplitudes for a comparison with this library's."""
+    import tempfile
+    from dgquest_b200 import circuits as C
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"unavailable": "oracle/_ref/ref_harness not built (make -C oracle ref needs the reference sources)"}
+    n = N_QUBITS
+    ops = C.random_layers(n, DEPTH, C.config_seed(2))
+    idx = np.unique(np.random.RandomState(11).randint(0, 1 << n, size=64).astype(np.int64))
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "QuEST.conf"), "w") as f:
+            f.write("5 5 5\n")
+        open(os.path.join(d, "predict_data.txt"), "w").close()
+        np.ascontiguousarray(ops).tofile(os.path.join(d, "ops.bin"))
+        idx.tofile(os.path.join(d, "idx.bin"))
+        clocks = ClockSampler(0)
+        clocks.start()
+        t0 = time.perf_counter()
+        r = subprocess.run([harness, "ops.bin", str(n), "out.bin", "sample", "idx.bin"], cwd=d,
+                           capture_output=True, text=True, timeout=600)
+        wall = time.perf_counter() - t0
+        clk = clocks.stop()
+        if r.returncode != 0:
+            return {"unavailable": f"ref_harness exited {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+        with open(os.path.join(d, "out.bin"), "rb") as f:
+            data = f.read()
+    num = int(np.frombuffer(data[12:20], dtype="<i8")[0])
+    t_get, t_prob = np.frombuffer(data[20:36], dtype="<f8")
+    off = 36 + 8 * n + 8 * num
+    ri = np.frombuffer(data[off:off + 16 * num], dtype="<f8")
+    return {"impl": "dgQuEST built from its sources for sm_100a (ref_harness), K = 5",
+            "getamp_s": float(t_get), "probs_s": float(t_prob), "wall_s": wall,
+            "circuits_per_s": 1.0 / float(t_get), "clocks": clk,
+            "sample_indices": idx.tolist(), "sample_amps": (ri[0::2] + 1j * ri[1::2]),
+            "note": "getamp_s is the reference's own timing of getAmp(q, 0), which runs the whole circuit"}
+
+
 # ---------------------------------------------------------------- GPU leg
-def run_gpu(args, world, rank, local):
+def run_gpu(args, world, rank, local, ref_gpu=None):
     import torch
 
     from dgquest_b200 import circuits as C
@@ -242,6 +324,12 @@ def run_gpu(args, world, rank, local):
             e2e_times.append(dt)
             record_times.append(t1 - t0)
     e2e_t = max_over_ranks(float(np.mean(e2e_times)), world)
+    if ref_gpu and "sample_amps" in ref_gpu:
+        # the register holds the circuit's final state (last e2e run)
+        amps = [Q.getAmp(q, int(i)) for i in ref_gpu.pop("sample_indices")]
+        ours = np.array([complex(a.real, a.imag) for a in amps])
+        ref_gpu["max_abs_err_vs_this_library"] = float(np.abs(ours - ref_gpu.pop("sample_amps")).max())
+        ref_gpu["amplitudes_compared"] = len(ours)
     st2 = Q.plan_stats(q)
     h2d = int(st2.launchBytes)  # one sweep program per kernel parameter block
     d2h = 16 + (n + 1) * 8
@@ -324,6 +412,10 @@ def run_gpu(args, world, rank, local):
                                 "compiled once (cold_specialisation_ms, first planning) and reused; sweeps "
                                 "launch while the rest of the circuit is planned (streamed_sweeps)"},
                 "gpu_launches": int(launches), "clocks": clk, "fp32_form": fp32}
+        if ref_gpu is not None:
+            if "getamp_s" in ref_gpu:
+                ref_gpu["e2e_speedup_of_this_library"] = ref_gpu["getamp_s"] / e2e_t
+            line["reference_gpu"] = ref_gpu
     return line
 
 
@@ -762,8 +854,8 @@ def main():
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--tile-bits", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-gates", type=int, default=8)
-    ap.add_argument("--cpu-gates", type=int, default=8)
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the run of dgQuEST's own GPU path (oracle/_ref/ref_harness)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
@@ -801,7 +893,11 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    line = run_gpu(args, world, rank, local)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu and args.qubits == N_QUBITS and args.depth == DEPTH:
+        # first, while this process holds no device memory of its own
+        ref_gpu = run_reference_gpu(args)
+    line = run_gpu(args, world, rank, local, ref_gpu)
     if not args.no_dense:
         dense = run_dense_form(args, world)
         if rank == 0:
@@ -821,13 +917,19 @@ def main():
     if not args.no_serve and rank == 0:
         line["serving"] = run_serving_form(args, world)
     if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
         from dgquest_b200 import circuits as C
         ops = C.random_layers(N_QUBITS, DEPTH, C.config_seed(2))
-        dt, cores = cpu_sample(ops, N_QUBITS, args.cpu_gates)
-        line["cpu_baseline"] = {"value": (args.cpu_gates / len(ops)) / dt, "unit": "circuits/s", "cores": cores,
-                                "kind": "port",
-                                "sample": f"oracle (OpenMP) on the first {args.cpu_gates} of {len(ops)} gate "
-                                          f"calls, 30 qubits, scaled by {len(ops)}/{args.cpu_gates}"}
+        cores = oracle.max_threads()
+        t_all = cpu_time_ops(N_QUBITS, [ops[:2], layer_of(ops, N_QUBITS, 0)], cores)[1]
+        t_one, one_desc = cpu_one_core_layer(ops, N_QUBITS)
+        oracle.set_threads(cores)
+        line["cpu_baseline"] = {"value": 1.0 / (t_all * DEPTH), "unit": "circuits/s", "cores": cores,
+                                "kind": "port", "extrapolated": True,
+                                "sample": f"oracle (OpenMP, {cores} threads) on layer 0 of the 30-qubit circuit "
+                                          f"(30 rotations + 15 CZ, {t_all:.2f} s), x {DEPTH} layers",
+                                "one_core": {"value": 1.0 / (t_one * DEPTH), "unit": "circuits/s", "cores": 1,
+                                             "sample": one_desc}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

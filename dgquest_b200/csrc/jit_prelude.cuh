@@ -1,5 +1,5 @@
 // jit_prelude.cuh -- device code shared by the runtime-specialised sweep
-// kernels (codegen.cpp writes one kernel per sweep program and NVRTC
+// kernels (jit.cpp writes one kernel per sweep program and NVRTC
 // compiles it for sm_100a together with this header and tile_program.h).
 //
 // The generated kernel is the tile kernel of kernels.cu with everything

@@ -59,6 +59,7 @@ def lib():
         L.orc_mt_first_outputs.argtypes = [POINTER(c_ulong), c_int, POINTER(c_uint32), c_int]
         L.orc_mt_first_outputs_seed.argtypes = [c_uint32, POINTER(c_uint32), c_int]
         L.orc_max_threads.restype = c_int
+        L.orc_set_threads.argtypes = [c_int]
         _lib = L
     return _lib
 
@@ -167,3 +168,8 @@ def run(n, ops, seed_keys=None):
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+def set_threads(n):
+    """Threads of the oracle's OpenMP loops from now on."""
+    lib().orc_set_threads(int(n))

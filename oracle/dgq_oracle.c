@@ -520,6 +520,17 @@ void orc_mt_first_outputs_seed(uint32_t seed, uint32_t *out, int count) {
     for (int i = 0; i < count; i++) out[i] = mt_next(&g);
 }
 
+/* Threads the OpenMP loops use from now on (the CPU baseline times the
+ * oracle on all host cores and on one). */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    extern void omp_set_num_threads(int);
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void) n;
+#endif
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
     extern int omp_get_max_threads(void);

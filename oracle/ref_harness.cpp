@@ -2,7 +2,7 @@
  * ref_harness.cpp -- drives the reference (dgQuEST) built from its own
  * sources, to produce golden outputs for the oracle and the tests.
  *
- * TEST INFRASTRUCTURE ONLY. Built by oracle/ref_build.mk into oracle/_ref/
+ * TEST INFRASTRUCTURE ONLY. Built by `make -C oracle ref` (oracle/Makefile) into oracle/_ref/
  * and run on a GPU host; its outputs are committed as fixtures under
  * tests/golden/ by tests/golden/make_golden.py.
  *
