@@ -226,7 +226,7 @@ def test_noise_channel_probability_errors(quest, env):
             for bad in (-0.1, 1.5):
                 with pytest.raises(quest.QuESTError) as ei:
                     call(bad)
-                assert ei.value.message == generic, ei.value.message
+                assert ei.value.message.endswith(generic), ei.value.message
         quest.applyOneQubitDampingError(q, 0, 1.0)  # full decay is a valid channel
         assert abs(quest.calcTotalProb(q) - 1.0) <= TOL
     finally:
