@@ -287,8 +287,9 @@ int chooseTileBits(QuregState &s) {
     // complex64 tiles could reach 2^13 amplitudes in 64 KiB, but at 16
     // amplitudes a thread that is one 512-thread CTA per SM, which hides no
     // latency; 2^12 keeps three CTAs per SM (override: dgq_setTileBits(13))
-    const int hi = std::min(s.single && s.tileBitsSetting >= dgq::kMaxTileBitsC64 ? dgq::kMaxTileBitsC64
-                                                                                    : dgq::kMaxTileBitsF64,
+    // a set width of 13 is honoured in either precision (complex128: 128 KiB
+    // of shared memory, one 512-thread CTA per SM, specialised kernels only)
+    const int hi = std::min(s.tileBitsSetting >= dgq::kMaxTileBitsC64 ? dgq::kMaxTileBitsC64 : dgq::kMaxTileBitsF64,
                             s.numBits);
     const int lo = dgq::kMinTileBits;
     s.planLookahead = -1;
