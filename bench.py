@@ -260,6 +260,47 @@ def run_reference_gpu(args):
 
 
 # ---------------------------------------------------------------- GPU leg
+def form_report(st, measured):
+    """The predictor's form choice of a plan (plan statistics) beside the
+    measured times (ms) of the forms that were run."""
+    pred = {"tiles": round(st.predictedTileMs, 2)}
+    for i, k in enumerate((5, 6, 7)):
+        v = round(st.predictedDenseMs[i], 2)
+        pred[f"dense_k{k}"] = f">{v}" if (st.denseBound >> i) & 1 else v
+    chosen = f"tiles W={st.tileBits}" if st.formK == 0 else f"dense K={st.formK}"
+    return {"chosen": chosen, "by_predictor": bool(st.formAuto), "predicted_ms": pred,
+            "measured_ms": {k: round(v, 2) for k, v in measured.items()},
+            "note": "'>x': the estimate stopped counting blocks once they cost more than the tile form"}
+
+
+def time_dense_form(n, ops, single, K, runs=1):
+    """One warm-up and `runs` timed launches (ms, CUDA events) of the circuit
+    fused into dense K-qubit blocks (dgq_setDenseFusion(q, K))."""
+    import torch
+
+    from dgquest_b200 import quest as Q
+    env = Q.createQuESTEnv()
+    q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+    Q.dgq_setDenseFusion(q, K)
+    Q.initZeroState(q)
+    Q.apply_circuit(q, ops)
+    Q.dgq_planPending(q)
+    blocks = Q.plan_stats(q).denseBlocks
+    stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+    Q.dgq_launchPlanned(q)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(runs):
+        Q.dgq_launchPlanned(q)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    Q.destroyQureg(q, env)
+    Q.destroyQuESTEnv(env)
+    return e0.elapsed_time(e1) / runs, int(blocks)
+
+
 def run_gpu(args, world, rank, local, ref_gpu=None):
     import torch
 
@@ -371,13 +412,21 @@ def run_gpu(args, world, rank, local, ref_gpu=None):
         Q.initZeroState(q)
         C.replay(q, ops)
         fid = Q.calcFidelity(q, q32)
+        form32 = {"tiles": ms32}
+        if not args.no_dense:
+            form32["dense_k6_tensor_cores"], _ = time_dense_form(n, ops, True, 6)
         fp32 = {"ms_per_step": ms32, "circuits_per_s": world * 1000.0 / ms32, "speedup_vs_fp64": ms_step / ms32,
+                "form_choice": form_report(st32, form32),
                 "fidelity_vs_fp64": fid, "dtype": "complex64 amplitudes, FP32 arithmetic (SIMT)",
                 "tile_bits": st32.tileBits, "sweeps": st32.sweeps,
                 "hbm_gbs": 2.0 * (1 << n) * 8 * st32.sweeps / (ms32 / 1000.0) / 1e9}
         Q.destroyQureg(q32, env)
     Q.destroyQureg(q, env)
     Q.destroyQuESTEnv(env)
+    form64 = {"tiles": ms_step}
+    if not args.no_dense:
+        form64["dense_k6_simt"], _ = time_dense_form(n, ops, False, 6)
+    form64 = form_report(st, form64)
 
     line = None
     if rank == 0:
@@ -411,7 +460,7 @@ def run_gpu(args, world, rank, local, ref_gpu=None):
                         "note": "steady state: the sweep kernels specialised for this circuit's structure are "
                                 "compiled once (cold_specialisation_ms, first planning) and reused; sweeps "
                                 "launch while the rest of the circuit is planned (streamed_sweeps)"},
-                "gpu_launches": int(launches), "clocks": clk, "fp32_form": fp32}
+                "gpu_launches": int(launches), "clocks": clk, "fp32_form": fp32, "form_choice": form64}
         if ref_gpu is not None:
             if "getamp_s" in ref_gpu:
                 ref_gpu["e2e_speedup_of_this_library"] = ref_gpu["getamp_s"] / e2e_t
@@ -676,7 +725,7 @@ def run_precision_form(args, world):
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
         amp = 8 if single else 16
-        out[name] = {"ms_per_circuit": ms, "sweeps": st.sweeps, "tile_bits": st.tileBits,
+        out[name] = {"ms_per_circuit": ms, "sweeps": st.sweeps, "tile_bits": st.tileBits, "plan_stats": st,
                      "hbm_gbs": 2.0 * (1 << n) * amp * st.sweeps / (ms / 1e3) / 1e9,
                      "gate_layers_per_s": depth / (ms / 1e3)}
         regs[name] = q
@@ -692,6 +741,9 @@ def run_precision_form(args, world):
     out["amplitudes_sampled"] = len(idx)
     out["speedup_complex64"] = out["complex128"]["ms_per_circuit"] / out["complex64"]["ms_per_circuit"]
     out["arithmetic"] = "complex64 paired form (packed FP32 SIMT register phases)"
+    for name in ("complex128", "complex64"):
+        st_ = out[name].pop("plan_stats")
+        out[name]["form_choice"] = form_report(st_, {"tiles": out[name]["ms_per_circuit"]})
     Q.destroyQureg(q32, env)
     if not args.no_tc_blocks:
         # the same circuit fused into dense 6-qubit blocks, each a 3xTF32 GEMM
@@ -717,6 +769,7 @@ def run_precision_form(args, world):
             a = Q.getAmp(q64, int(i))
             b = Q.getAmp(q, int(i))
             err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
+        out["complex64"]["form_choice"]["measured_ms"]["dense_k6_tensor_cores"] = round(ms, 2)
         out["complex64_tensor_core_blocks"] = {
             "ms_per_circuit": ms, "dense_blocks": int(st.denseBlocks), "sweeps": st.sweeps,
             "tensor_tflops_algorithmic": st.denseBlocks * (1 << n) * 1536.0 / (ms / 1e3) / 1e12,

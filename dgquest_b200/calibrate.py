@@ -3,7 +3,9 @@
 predictor, time_predictor.cpp:397-476).
 
 The tile-width choice predicts a plan's time as
-    sweeps x sweep_ms + phases x phase_ms        (per 2^30 amplitudes).
+    sweeps x sweep_ms + phases x phase_ms        (per 2^30 amplitudes),
+and the form choice a dense-block plan's as blocks x dense_ms (per variant
+and block width K; --dense measures those too).
 This module plans a set of seeded circuits at several tile widths, times
 every plan with CUDA events on the register's stream, fits the two rates by
 least squares (non-negative), writes them to a cost file and installs them:
@@ -73,6 +75,53 @@ def measure(n=26, widths=(10, 11, 12), repeats=3, names=None):
     return rows
 
 
+DENSE_VARIANTS = (("f64", False, 0), ("c64", True, 0), ("c64tc", True, 1))
+
+
+def measure_dense(n=26, Ks=(5, 6, 7), repeats=3):
+    """ms per dense block per 2^30 amplitudes, {(variant, K): ms}, for the
+    form choice: two random K-qubit unitaries (multiQubitUnitary) on an
+    n-qubit register, the plan timed with CUDA events (the init pass
+    included, so the figure is a slight over-estimate per block)."""
+    import torch
+    gen = np.random.default_rng(11)
+    env = Q.createQuESTEnv()
+    out = {}
+    try:
+        for name, single, tc in DENSE_VARIANTS:
+            for K in Ks:
+                if name == "c64tc" and K != 6:
+                    continue
+                prev = Q.dgq_setTensorCores(tc)
+                q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+                try:
+                    Q.initPlusState(q)
+                    for t in (list(range(K)), list(range(n - K, n))):
+                        m = Q.matrixN(C.random_unitary(gen, 1 << K))
+                        Q.multiQubitUnitary(q, Q.int_array(t), K, m)
+                        Q.destroyComplexMatrixN(m)
+                    Q.dgq_planPending(q)
+                    stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+                    Q.dgq_launchPlanned(q)
+                    torch.cuda.synchronize()
+                    ts = []
+                    for _ in range(repeats):
+                        e0 = torch.cuda.Event(enable_timing=True)
+                        e1 = torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        Q.dgq_launchPlanned(q)
+                        e1.record(stream)
+                        torch.cuda.synchronize()
+                        ts.append(e0.elapsed_time(e1))
+                    out[(name, K)] = float(np.median(ts)) / 2 * 2.0 ** (30 - n)
+                finally:
+                    Q.destroyQureg(q, env)
+                    Q.dgq_setTensorCores(prev)
+    finally:
+        Q.destroyQuESTEnv(env)
+    return out
+
+
 def fit(rows, n):
     """Non-negative least squares for (sweep_ms, phase_ms) per 2^30 amplitudes."""
     scale = 2.0 ** (30 - n)
@@ -86,23 +135,36 @@ def fit(rows, n):
     return float(x[0]), float(x[1])
 
 
-def write(path, sweep_ms, phase_ms, note=""):
+def write(path, sweep_ms, phase_ms, note="", dense=None):
     with open(path, "w") as f:
         f.write(f"{HEADER}\n")
         if note:
             f.write(f"# {note}\n")
         f.write(f"sweep_ms_per_2p30 {sweep_ms:.6f}\n")
         f.write(f"phase_ms_per_2p30 {phase_ms:.6f}\n")
+        for (name, K), ms in sorted((dense or {}).items()):
+            f.write(f"dense_ms_per_2p30_{name}_k{K} {ms:.6f}\n")
 
 
-def calibrate(n=26, out=None, widths=(10, 11, 12), repeats=3, names=None):
-    """Measures, fits, installs (dgq_setCostModel) and optionally writes the
-    rates; returns (sweep_ms, phase_ms, rows)."""
+def install_dense(dense):
+    """Installs measured dense rates (dgq_setDenseCost)."""
+    index = {name: i for i, (name, _, _) in enumerate(DENSE_VARIANTS)}
+    for (name, K), ms in dense.items():
+        Q.dgq_setDenseCost(index[name], K, ms)
+
+
+def calibrate(n=26, out=None, widths=(10, 11, 12), repeats=3, names=None, dense=False):
+    """Measures, fits, installs (dgq_setCostModel, and with dense=True the
+    dense-block rates, dgq_setDenseCost) and optionally writes the rates;
+    returns (sweep_ms, phase_ms, rows)."""
     rows = measure(n, widths, repeats, names)
     sweep_ms, phase_ms = fit(rows, n)
     Q.dgq_setCostModel(sweep_ms, phase_ms)
+    drates = measure_dense(n, repeats=repeats) if dense else None
+    if drates:
+        install_dense(drates)
     if out:
-        write(out, sweep_ms, phase_ms, note=f"fitted on {len(rows)} plans at n={n}")
+        write(out, sweep_ms, phase_ms, note=f"fitted on {len(rows)} plans at n={n}", dense=drates)
     return sweep_ms, phase_ms, rows
 
 
@@ -117,8 +179,9 @@ def main():
     ap.add_argument("--qubits", type=int, default=26)
     ap.add_argument("--out", default="dgq_cost.txt")
     ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--dense", action="store_true", help="also measure the dense-block rates of the form choice")
     args = ap.parse_args()
-    sweep_ms, phase_ms, rows = calibrate(args.qubits, args.out, repeats=args.repeats)
+    sweep_ms, phase_ms, rows = calibrate(args.qubits, args.out, repeats=args.repeats, dense=args.dense)
     print(json.dumps({"sweep_ms_per_2p30": sweep_ms, "phase_ms_per_2p30": phase_ms, "plans": len(rows),
                       "file": args.out}))
 

@@ -216,15 +216,56 @@ uint64_t toVirtualIndex(const QuregState &s, uint64_t logical) {
 // The rates can be replaced by a calibration of this GPU
 // (dgquest_b200/calibrate.py measures them; dgq_setCostModel installs them,
 // dgq_loadCostModel or DGQ_COST_FILE reads the file it writes).
+// The predictor also chooses the form of a plan (dgq_setDenseFusion(q, -1),
+// the default): register-phase tiles, or the gates fused into dense blocks of
+// K = 5, 6 or 7 qubits, each block one dense sweep. A dense sweep costs a
+// fixed time per block per amplitude (denseMs, ms per block per 2^30
+// amplitudes) for three variants: complex128 SIMT, complex64 SIMT and
+// complex64 on the tensor cores (K = 6 only). Built-in: the K = 6 figures
+// measured on B200 at 30 qubits (58.1, 37.4 and 14.8 ms), K = 5 and 7 scaled
+// by 2^K (the SIMT dense kernel is compute-bound, 8 x 2^K flops per
+// amplitude). Tiles on a complex64 register (the paired form) cost
+// c64TileFactor times the complex128 prediction (measured: 77 of 140 ms on
+// the 30-qubit circuit). A dense form is taken when its prediction is below
+// denseMargin times the tile form's.
+enum DenseVariant { DV_F64 = 0, DV_C64 = 1, DV_C64_TC = 2 };
+// complex64 dense 6-qubit sweeps on the tensor cores (dgq_setTensorCores)
+std::atomic<int> g_tensorCores{1};
 struct CostModel {
     double sweepSecondsPerAmp = 2.6e-3 / 1073741824.0;
     double phaseSecondsPerAmp = 1.8e-3 / 1073741824.0;
     double launchSeconds = 3e-6;
+    double denseMs[3][3] = {{29.05, 58.1, 116.2}, {18.7, 37.4, 74.8}, {0.0, 14.8, 0.0}};  // [variant][K - 5]
+    double c64TileFactor = 0.55;
+    double denseMargin = 0.8;
 };
 
 std::mutex g_costMutex;
 CostModel g_cost;
 bool g_costFileTried = false;
+
+const char *kDenseVariantName[3] = {"f64", "c64", "c64tc"};
+
+// Optional lines of a cost file: "dense_ms_per_2p30_<f64|c64|c64tc>_k<K> <ms>"
+// and "c64_tile_factor <x>"; applied to `cm` (other keys are ignored).
+void readCostFileExtras(const char *path, CostModel &cm) {
+    FILE *f = fopen(path, "r");
+    if (!f) return;
+    char line[256];
+    while (fgets(line, sizeof(line), f)) {
+        char key[64];
+        double v = 0.0;
+        if (line[0] == '#' || sscanf(line, "%63s %lf", key, &v) != 2 || !std::isfinite(v) || v < 0.0) continue;
+        if (!strcmp(key, "c64_tile_factor") && v > 0.0) cm.c64TileFactor = v;
+        for (int var = 0; var < 3; var++)
+            for (int K = 5; K <= 7; K++) {
+                char name[64];
+                snprintf(name, sizeof name, "dense_ms_per_2p30_%s_k%d", kDenseVariantName[var], K);
+                if (!strcmp(key, name)) cm.denseMs[var][K - 5] = v;
+            }
+    }
+    fclose(f);
+}
 
 // "dgq_cost 1" then "sweep_ms_per_2p30 <x>" and "phase_ms_per_2p30 <y>"
 // lines (any order, '#' comments); returns false on a malformed file.
@@ -262,6 +303,7 @@ CostModel costModel() {
         if (path && readCostFile(path, sw, ph)) {
             g_cost.sweepSecondsPerAmp = sw * 1e-3 / 1073741824.0;
             g_cost.phaseSecondsPerAmp = ph * 1e-3 / 1073741824.0;
+            readCostFileExtras(path, g_cost);
         }
     }
     return g_cost;
@@ -327,6 +369,75 @@ int chooseTileBits(QuregState &s) {
             bestT = c.t;
             best = c.W;
             s.planLookahead = c.lookahead;
+        }
+    }
+    s.predictedTileSeconds = bestT;
+    return best;
+}
+
+// Predicted time of the dense-block form with K-qubit blocks: the blocks'
+// dense sweeps plus the tile sweeps of the gates that touch more than K
+// qubits and pass through. *blocksOut: the number of blocks.
+// bound > 0: stop counting blocks once they cost more than bound seconds
+// (*stopped is set and the result is the cost of the blocks counted).
+double predictDenseSeconds(const QuregState &s, int K, int *blocksOut, double bound, bool *stopped) {
+    const CostModel cm = costModel();
+    const int var = !s.single ? DV_F64 : (K == 6 && g_tensorCores.load() ? DV_C64_TC : DV_C64);
+    const double rate = cm.denseMs[var][K - 5] > 0.0 ? cm.denseMs[var][K - 5] : cm.denseMs[DV_C64][K - 5];
+    const double amps = std::ldexp(1.0, s.numBits);
+    const double perBlock = rate * 1e-3 * amps / 1073741824.0 + cm.launchSeconds;
+    const int maxBlocks = bound > 0.0 ? (int) std::min(1e6, std::floor(bound / perBlock)) + 1 : 0;
+    dgq::MatrixPool pool = s.pool;
+    int blocks = 0;
+    bool cut = false;
+    const std::vector<Gate> fused = dgq::fuseDenseBlocks(s.pending, s.numBits, K, pool, &blocks, maxBlocks, &cut);
+    if (blocksOut) *blocksOut = blocks;
+    if (stopped) *stopped = cut;
+    double t = blocks * perBlock;
+    if (cut) return t;
+    std::vector<Gate> rest;
+    for (const Gate &g : fused)
+        if (!(g.type == dgq::OP_MULTI_UNITARY && g.numMultiTargets > dgq::kRegBits)) rest.push_back(g);
+    if (!rest.empty()) {
+        const double tt = predictPlanSeconds(rest, s.numBits, std::min(12, s.numBits), pool, -1);
+        t += s.single ? tt * cm.c64TileFactor : tt;
+    }
+    return t;
+}
+
+// The predictor's choice of form for the pending gates (dgq_setDenseFusion
+// -1): 0 for register-phase tiles, else the dense block width K. Fills the
+// plan statistics' predictions (ms) for every candidate.
+int chooseForm(QuregState &s) {
+    const CostModel cm = costModel();
+    // the tile form first: its prediction bounds the dense estimates, whose
+    // block counting stops as soon as they cannot win
+    s.formTileBits = chooseTileBits(s);
+    s.formLookahead = s.planLookahead;
+    double tile = s.predictedTileSeconds;
+    if (s.single) tile *= cm.c64TileFactor;
+    s.stats.predictedTileMs = tile * 1e3;
+    double dense[3] = {0.0, 0.0, 0.0};
+    int blocks[3] = {0, 0, 0};
+    bool cut[3] = {false, false, false};
+    {
+        std::vector<std::thread> th;
+        for (int K = 5; K <= 7; K++)
+            if (s.numBits >= K + 2)
+                th.emplace_back([&, K]() {
+                    dense[K - 5] = predictDenseSeconds(s, K, &blocks[K - 5], tile * cm.denseMargin, &cut[K - 5]);
+                });
+        for (auto &x : th) x.join();
+    }
+    s.stats.denseBound = 0;
+    int best = 0;
+    double bestT = tile * cm.denseMargin;
+    for (int K = 5; K <= 7; K++) {
+        s.stats.predictedDenseMs[K - 5] = dense[K - 5] * 1e3;
+        if (cut[K - 5]) s.stats.denseBound |= 1 << (K - 5);
+        if (s.numBits >= K + 2 && blocks[K - 5] > 0 && !cut[K - 5] && dense[K - 5] < bestT) {
+            bestT = dense[K - 5];
+            best = K;
         }
     }
     return best;
@@ -496,7 +607,6 @@ void freeOn(void *ptr, cudaStream_t st);
 
 // Dense 6-target unitaries on complex64 registers run on the tensor cores
 // (dgq_setTensorCores(0): the SIMT dense kernel instead).
-std::atomic<int> g_tensorCores{1};
 
 // 0: compile specialised kernels when a plan needs them; 1: specialise only
 // plans whose kernels are compiled already, interpret the others while
@@ -573,8 +683,18 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     if (s.pending.empty() && !s.initPending) return true;
     const double t0 = nowMillis();
     int denseBlocks = 0;
-    if (s.denseFusion > 0 && s.numBits >= s.denseFusion + 2 && !s.pending.empty())
-        s.pending = dgq::fuseDenseBlocks(s.pending, s.numBits, s.denseFusion, s.pool, &denseBlocks);
+    int formK = s.denseFusion > 0 ? s.denseFusion : 0;
+    s.stats.formAuto = 0;
+    s.formTileBits = 0;
+    s.stats.predictedTileMs = 0.0;
+    for (double &x : s.stats.predictedDenseMs) x = 0.0;
+    if (s.denseFusion < 0 && !s.pending.empty()) {
+        formK = chooseForm(s);
+        s.stats.formAuto = 1;
+    }
+    s.stats.formK = formK;
+    if (formK > 0 && s.numBits >= formK + 2 && !s.pending.empty())
+        s.pending = dgq::fuseDenseBlocks(s.pending, s.numBits, formK, s.pool, &denseBlocks);
     const bool jitOn = dgq::jitEnabled();
     const bool wantJit = jitOn && (!specialise || s.numBits >= jitMinBits());
     // complex64 registers of >= 2^10 amplitudes run the paired form (two
@@ -634,7 +754,15 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
     auto build = [&](bool pairedForm, bool interpret) -> int {
         paired = pairedForm;
         s.planLookahead = -1;
-        W = paired ? pairedTileBits(s) : chooseTileBits(s);
+        if (paired) {
+            W = pairedTileBits(s);
+        } else if (s.formTileBits > 0 && formK == 0) {
+            // the form choice planned the tile widths already
+            W = s.formTileBits;
+            s.planLookahead = s.formLookahead;
+        } else {
+            W = chooseTileBits(s);
+        }
         if (interpret) W = std::min(W, dgq::kMaxTileBitsF64);
         st = dgq::PlanStats();
         err.clear();
@@ -681,8 +809,9 @@ bool planPending(QuregState &s, const char *func, bool specialise = true, bool l
             s.stats.jitMillis = js.compileMillis;
         }
     }
-    if (!s.denseHost.empty()) {
+    if (!s.denseHost.empty() && specialise) {
         // a new buffer per plan, freed in stream order after earlier launches
+        // (the host-only planner entry points, specialise = false, upload nothing)
         freeOn(s.dDense, s.stream);
         s.dDense = nullptr;
         if (!cudaOk(allocOn((void **) &s.dDense, s.denseHost.size() * sizeof(double), s.stream), func) ||
@@ -2324,9 +2453,9 @@ int dgq_getPlanStats(Qureg q, dgq_plan_stats *out) {
 
 int dgq_setDenseFusion(Qureg q, int qubits) {
     if (!vQureg(q, __func__)) return -1;
-    if (qubits != 0 && (qubits < dgq::kMinDenseTargets || qubits > dgq::kMaxDenseTargets)) {
-        raise(E_INVALID_ARGUMENT, __func__, "dense fusion takes 0 or 5..7 qubits");
-        return -1;
+    if (qubits != 0 && qubits != -1 && (qubits < dgq::kMinDenseTargets || qubits > dgq::kMaxDenseTargets)) {
+        raise(E_INVALID_ARGUMENT, __func__, "dense fusion takes -1 (the predictor chooses), 0 or 5..7 qubits");
+        return -2;
     }
     QuregState &s = *stateOf(q);
     const int prev = s.denseFusion;
@@ -2349,7 +2478,24 @@ int dgq_loadCostModel(const char *path) {
     double sw = 0.0, ph = 0.0;
     if (!path || !readCostFile(path, sw, ph))
         return raise(E_INVALID_ARGUMENT, __func__, "missing or malformed cost file") ? 0 : -1;
-    return dgq_setCostModel(sw, ph);
+    if (dgq_setCostModel(sw, ph) != 0) return -1;
+    std::lock_guard<std::mutex> lk(g_costMutex);
+    readCostFileExtras(path, g_cost);
+    return 0;
+}
+
+int dgq_setDenseCost(int variant, int K, double msPer2p30) {
+    if (variant < 0 || variant > 2 || K < 5 || K > 7 || !(msPer2p30 >= 0.0) || !std::isfinite(msPer2p30))
+        return raise(E_INVALID_ARGUMENT, __func__, "variant 0..2, K 5..7, a finite rate >= 0") ? 0 : -1;
+    costModel();  // a DGQ_COST_FILE is read first, so this call is not overwritten by it
+    std::lock_guard<std::mutex> lk(g_costMutex);
+    g_cost.denseMs[variant][K - 5] = msPer2p30;
+    return 0;
+}
+
+double dgq_getDenseCost(int variant, int K) {
+    if (variant < 0 || variant > 2 || K < 5 || K > 7) return -1.0;
+    return costModel().denseMs[variant][K - 5];
 }
 
 int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30) {

@@ -117,9 +117,11 @@ void applyGateLocal(const Gate &g, const MatrixPool &pool, const int local[64], 
 }
 
 std::vector<Gate> fuseDenseBlocks(const std::vector<Gate> &gates, int numBits, int K, MatrixPool &pool,
-                                  int *blocks) {
+                                  int *blocks, int maxBlocks, bool *stopped) {
     std::vector<Gate> out;
     if (blocks) *blocks = 0;
+    if (stopped) *stopped = false;
+    int made = 0;
     if (K < 1 || K > 7 || K > numBits) return gates;
     GateDag dag(numBits, true);
     dag.setTouchCost(true);
@@ -127,6 +129,10 @@ std::vector<Gate> fuseDenseBlocks(const std::vector<Gate> &gates, int numBits, i
     const int D = 1 << K;
     std::vector<double> u((size_t) 2 * D * D);
     while (!dag.empty()) {
+        if (maxBlocks > 0 && made >= maxBlocks) {
+            if (stopped) *stopped = true;
+            break;
+        }
         u64 mask = 0;
         for (;;) {
             size_t best = 0;
@@ -183,6 +189,7 @@ std::vector<Gate> fuseDenseBlocks(const std::vector<Gate> &gates, int numBits, i
         f.multiIndex = (int32_t) pool.mats.size();
         pool.mats.push_back(std::move(m));
         out.push_back(f);
+        made++;
         if (blocks) (*blocks)++;
     }
     return out;

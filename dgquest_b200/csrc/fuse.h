@@ -23,8 +23,11 @@ namespace dgq {
 // qubits passes through unchanged, with the gates that the same greedy step
 // takes beside it. *blocks (if given) counts the dense gates made.
 // Requires 1 <= K <= 7 and K <= numBits.
+// maxBlocks > 0 stops after that many blocks (the rest of the gates are
+// dropped; *stopped, if given, is set): a cost estimate that only needs to
+// know whether the form stays below a bound.
 std::vector<Gate> fuseDenseBlocks(const std::vector<Gate> &gates, int numBits, int K, MatrixPool &pool,
-                                  int *blocks = nullptr);
+                                  int *blocks = nullptr, int maxBlocks = 0, bool *stopped = nullptr);
 
 // Applies one recorded gate to the 2^K-amplitude vectors v[c * 2^K ..] for
 // c < numVectors, where local[b] is the vector index bit of address bit b

@@ -57,7 +57,11 @@ struct QuregState {
     int tileBitsSetting = 0;  // 0 = cost model
     int planLookahead = -1;   // block selection with lookahead (the cost model's choice; -1: by size)
     bool allowPaired = true;  // complex64: the paired form where it applies
-    int denseFusion = 0;      // > 0: gates fused into dense blocks of this many qubits
+    int denseFusion = -1;     // > 0: gates fused into dense blocks of this many qubits;
+                              // -1: the predictor chooses tiles or dense blocks per plan
+    double predictedTileSeconds = 0.0;  // the tile-width choice's predicted plan time
+    int formTileBits = 0;   // the form choice's tile width for the plan being made (0: none)
+    int formLookahead = -1;
     // matrices of the planned dense sweeps (host copy and device buffer)
     std::vector<double> denseHost;
     double *dDense = nullptr;

@@ -66,6 +66,11 @@ class PlanStats(Structure):
         ("launchBytes", ctypes.c_int64),
         ("streamedSweeps", ctypes.c_int32),
         ("denseBlocks", ctypes.c_int32),
+        ("formK", ctypes.c_int32),
+        ("formAuto", ctypes.c_int32),
+        ("predictedTileMs", c_double),
+        ("predictedDenseMs", c_double * 3),
+        ("denseBound", ctypes.c_int32),
     ]
 
 
@@ -185,6 +190,8 @@ _SIGS = {
     "dgq_setCostModel": (I, [D, D]),
     "dgq_loadCostModel": (I, [ctypes.c_char_p]),
     "dgq_getCostModel": (I, [P(D), P(D)]),
+    "dgq_setDenseCost": (I, [I, I, D]),
+    "dgq_getDenseCost": (D, [I, I]),
     "dgq_getHostTierStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),
     "dgq_createShardedQureg": (Qureg, [I, E, I, P(I), I]),
     "dgq_getShardStats": (I, [Q, P(I), P(ctypes.c_int64), P(ctypes.c_int64), P(ctypes.c_int64)]),

@@ -60,6 +60,12 @@ typedef struct dgq_plan_stats {
     int32_t streamedSweeps; /* sweeps launched while the rest of the plan was
                                still being made (their kernels were compiled) */
     int32_t denseBlocks;    /* dense fused blocks (dgq_setDenseFusion) */
+    int32_t formK;          /* form of the plan: 0 register-phase tiles, K dense K-qubit blocks */
+    int32_t formAuto;       /* 1 when the predictor chose the form (dgq_setDenseFusion -1) */
+    double predictedTileMs; /* predictions of the form choice (0 when not made): the tile form */
+    double predictedDenseMs[3]; /* and the dense-block forms with K = 5, 6, 7 */
+    int32_t denseBound;     /* bit K - 5 set: the K estimate stopped counting blocks once they
+                               cost more than the tile form, and is that lower bound */
 } dgq_plan_stats;
 int dgq_getPlanStats(Qureg qureg, dgq_plan_stats *out);
 
@@ -81,6 +87,14 @@ void dgq_shutdown(void);
 int dgq_setCostModel(double sweepMsPer2p30, double phaseMsPer2p30);
 int dgq_loadCostModel(const char *path);
 int dgq_getCostModel(double *sweepMsPer2p30, double *phaseMsPer2p30);
+/* Rates of the dense-block forms in the form choice: ms per dense block per
+ * 2^30 amplitudes for variant 0 (complex128, SIMT), 1 (complex64, SIMT) or
+ * 2 (complex64, tensor cores; K = 6), K = 5..7. A cost file may carry them
+ * as "dense_ms_per_2p30_<f64|c64|c64tc>_k<K> <ms>", and the complex64 tile
+ * factor as "c64_tile_factor <x>". Set returns 0 or -1; get returns the
+ * rate, or -1 on a bad argument. */
+int dgq_setDenseCost(int variant, int K, double msPer2p30);
+double dgq_getDenseCost(int variant, int K);
 
 /* Host tier. A register whose state is larger than the device's memory (or
  * than the budget set here for registers created later, capped by free
@@ -122,14 +136,19 @@ Qureg dgq_createShardedQureg(int numQubits, QuESTEnv env, int shardBits, const i
  * error. */
 int dgq_getShardStats(Qureg qureg, int *shardBits, int64_t *passes, int64_t *exchanges, int64_t *bytesExchanged);
 
-/* Dense-block form. qubits = 5, 6 or 7: the register's gates are fused into
- * dense unitaries on that many qubits (dgQuEST's greedy block rule,
- * DAG.cpp:219-259, with every qubit a gate touches counted), composed in
- * FP64 on the host and applied one per sweep as a complex GEMM over the
- * state: on the tensor cores (tcgen05, 3xTF32) for complex64 registers and
- * 6 qubits, the SIMT dense kernel otherwise. 0 (the default) runs gates in
- * register-phase sweeps. Registers of fewer than qubits + 2 address bits
- * are not fused. Returns the previous setting, or -1 on a bad argument. */
+/* Form of a register's plans (the recast of dgQuEST's time predictor,
+ * time_predictor.cpp:343-395, which takes the argmin over its block width).
+ * qubits = 5, 6 or 7: the register's gates are fused into dense unitaries
+ * on that many qubits (dgQuEST's greedy block rule, DAG.cpp:219-259, with
+ * every qubit a gate touches counted), composed in FP64 on the host and
+ * applied one per sweep as a complex GEMM over the state: on the tensor
+ * cores (tcgen05, 3xTF32) for complex64 registers and 6 qubits, the SIMT
+ * dense kernel otherwise. 0 runs gates in register-phase sweeps. -1 (the
+ * default) lets the cost model choose per plan between the register-phase
+ * tiles (and their width) and dense blocks of 5, 6 or 7 qubits; the plan
+ * statistics report the choice (formK) and every prediction. Registers of
+ * fewer than qubits + 2 address bits are not fused. Returns the previous
+ * setting, or -2 on a bad argument. */
 int dgq_setDenseFusion(Qureg qureg, int qubits);
 
 /* Plans the pending gates (and pending initialisation / collapse) into

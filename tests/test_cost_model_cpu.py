@@ -73,3 +73,54 @@ def test_errors_are_recorded_per_thread(restore_rates):
     t.join()
     assert seen["other"] != 0
     assert lib.dgq_getLastError(None, 0) == 0
+
+
+@pytest.fixture
+def restore_dense():
+    prev = {(v, k): Q.dgq_getDenseCost(v, k) for v in range(3) for k in (5, 6, 7)}
+    yield
+    for (v, k), r in prev.items():
+        Q.dgq_setDenseCost(v, k, r)
+
+
+def test_form_choice_defaults_to_tiles_for_gate_circuits(restore_rates, restore_dense):
+    # built-in rates: a dense block sweep costs far more than a register-phase
+    # sweep covers, so rotation circuits stay in the tile form
+    n = 24
+    st = ir.plan(C.random_layers(n, 12, C.config_seed(2, 712)), n, 0)
+    assert st.formAuto == 1 and st.formK == 0 and st.denseBlocks == 0
+    assert st.predictedTileMs > 0
+    # every dense estimate stopped early at a bound above the tile form's
+    assert st.denseBound == 0b111
+    assert min(st.predictedDenseMs) > 0.8 * st.predictedTileMs
+
+
+@pytest.mark.parametrize("rates,expect", [((5.0, 0.001, 5.0), 6), ((0.001, 5.0, 5.0), 5), ((5.0, 5.0, 0.0005), 7)])
+def test_form_choice_is_the_cheapest_dense_width(rates, expect, restore_rates, restore_dense):
+    n = 26  # large enough that a block's launch overhead (3 us) does not decide
+    for k, r in zip((5, 6, 7), rates):
+        assert Q.dgq_setDenseCost(0, k, r) == 0
+    st = ir.plan(C.random_layers(n, 12, C.config_seed(2, 713)), n, 0)
+    assert st.formAuto == 1 and st.formK == expect and st.denseBlocks > 0
+    pred = list(st.predictedDenseMs)
+    assert not (st.denseBound >> (expect - 5)) & 1
+    assert pred[expect - 5] < 0.8 * st.predictedTileMs
+    # the chosen width's prediction is the smallest of the complete ones
+    full = [p for i, p in enumerate(pred) if not (st.denseBound >> i) & 1]
+    assert pred[expect - 5] == min(full)
+
+
+def test_dense_rates_from_a_cost_file(tmp_path, restore_rates, restore_dense):
+    path = tmp_path / "cost.txt"
+    path.write_text("dgq_cost 1\nsweep_ms_per_2p30 2.6\nphase_ms_per_2p30 1.8\n"
+                    "dense_ms_per_2p30_f64_k6 0.002\ndense_ms_per_2p30_c64tc_k6 1.5\nc64_tile_factor 0.5\n")
+    assert Q.dgq_loadCostModel(str(path).encode()) == 0
+    assert Q.dgq_getDenseCost(0, 6) == pytest.approx(0.002)
+    assert Q.dgq_getDenseCost(2, 6) == pytest.approx(1.5)
+    n = 26
+    st = ir.plan(C.random_layers(n, 12, C.config_seed(2, 714)), n, 0)
+    assert st.formK == 6
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_setDenseCost(3, 6, 1.0)
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_setDenseCost(0, 8, 1.0)

@@ -24,3 +24,25 @@ def test_calibration_measures_and_installs(quest, env, tmp_path):
         assert CAL.current() == pytest.approx((sweep_ms, phase_ms), rel=1e-5)
     finally:
         quest.dgq_setCostModel(*prev)
+
+
+def test_dense_rate_calibration(quest, env, tmp_path):
+    # the form choice's dense-block rates: measured per variant and width,
+    # positive, complex64 on the tensor cores faster than SIMT at K = 6, and
+    # written to / read back from the cost file
+    prev_rates = CAL.current()
+    keys = [(v, k) for v in range(3) for k in (5, 6, 7)]
+    prev = {key: quest.dgq_getDenseCost(*key) for key in keys}
+    path = tmp_path / "cost.txt"
+    try:
+        dense = CAL.measure_dense(22, Ks=(5, 6), repeats=2)
+        assert set(dense) == {("f64", 5), ("f64", 6), ("c64", 5), ("c64", 6), ("c64tc", 6)}
+        assert all(ms > 0 and math.isfinite(ms) for ms in dense.values())
+        CAL.write(str(path), *prev_rates, dense=dense)
+        assert quest.dgq_loadCostModel(str(path).encode()) == 0
+        assert quest.dgq_getDenseCost(0, 6) == pytest.approx(dense[("f64", 6)], rel=1e-5)
+        assert quest.dgq_getDenseCost(2, 6) == pytest.approx(dense[("c64tc", 6)], rel=1e-5)
+    finally:
+        quest.dgq_setCostModel(*prev_rates)
+        for key, r in prev.items():
+            quest.dgq_setDenseCost(*key, r)
