@@ -28,7 +28,7 @@ def test_calibration_measures_and_installs(quest, env, tmp_path):
 
 def test_dense_rate_calibration(quest, env, tmp_path):
     # the form choice's dense-block rates: measured per variant and width,
-    # positive, complex64 on the tensor cores faster than SIMT at K = 6, and
+    # positive and finite, and
     # written to / read back from the cost file
     prev_rates = CAL.current()
     keys = [(v, k) for v in range(3) for k in (5, 6, 7)]
