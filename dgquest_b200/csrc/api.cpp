@@ -558,8 +558,14 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
         for (int i = 0; i < g.numMultiTargets; i++) p.denseTargets[i] = (uint8_t) g.multiTargets[i];
         const auto &m = s.pool.mats[(size_t) g.multiIndex];
         s.denseHost.insert(s.denseHost.end(), m.begin(), m.end());
-        if (s.single && g.numMultiTargets == 6 && s.numBits >= 12) {
-            // the tensor-core operand: 2 x 128 x 128 floats in the doubles buffer
+        if (s.single && tcBlockSupported(s.numBits, g.numMultiTargets)) {
+            // the pipelined tensor-core operand ([Whi | Wlo], FP16) in the doubles buffer
+            const size_t nf = tcBlockMatrixFloats(g.numMultiTargets);
+            p.denseTcOff = (uint32_t) s.denseHost.size();
+            s.denseHost.resize(s.denseHost.size() + (nf + 1) / 2, 0.0);
+            packTcBlockMatrix(g.numMultiTargets, m.data(), reinterpret_cast<float *>(s.denseHost.data() + p.denseTcOff));
+        } else if (s.single && g.numMultiTargets == 6 && s.numBits >= 12) {
+            // the tensor-core operand of 4096-amplitude registers: 2 x 128 x 128 floats
             const size_t nf = tcDenseMatrixFloats();
             p.denseTcOff = (uint32_t) s.denseHost.size();
             s.denseHost.resize(s.denseHost.size() + (nf + 1) / 2, 0.0);
@@ -627,8 +633,10 @@ bool launchProgram(QuregState &s, size_t i, const char *func) {
         if (p.renormOut) da.normOut = p.normOut;
         if (p.denseTcOff && g_tensorCores.load()) {
             static uint32_t *errWord = dgq::tcDenseErrorWord();
-            e = dgq::launchTcDense((float2 *) s.dState, da, reinterpret_cast<const float *>(s.dDense + p.denseTcOff),
-                                   errWord, s.stream);
+            const float *op = reinterpret_cast<const float *>(s.dDense + p.denseTcOff);
+            e = dgq::tcBlockSupported(s.numBits, p.denseK)
+                    ? dgq::launchTcBlock((float2 *) s.dState, p.denseK, da, op, errWord, s.stream)
+                    : dgq::launchTcDense((float2 *) s.dState, da, op, errWord, s.stream);
         } else {
             e = dgq::launchDense(s.dState, s.single, p.denseK, da, s.dDense + p.denseOff, s.stream);
         }

@@ -96,6 +96,16 @@ size_t tcDenseMatrixFloats();
 uint32_t *tcDenseErrorWord();
 cudaError_t launchTcDense(float2 *st, const DenseArgs &a, const float *Apacked, uint32_t *error, cudaStream_t s);
 
+// Pipelined tensor-core form (tc_block.cu): complex64, K = 5 or 6 targets,
+// split FP16 on tcgen05 kind::f16, for registers of at least K + 7 address
+// bits (tcBlockSupported). Its operand is packed on the host
+// (packTcBlockMatrix, tcBlockMatrixFloats(K) floats).
+bool tcBlockSupported(int numBits, int K);
+size_t tcBlockMatrixFloats(int K);
+void packTcBlockMatrix(int K, const double *U, float *out);
+cudaError_t launchTcBlock(float2 *st, int K, const DenseArgs &a, const float *Wpacked, uint32_t *error,
+                          cudaStream_t s);
+
 struct SampleArgs {
     uint64_t numAmps;
     uint64_t restrictMask, restrictValue;  // lazy collapse (mask 0: none)
