@@ -784,6 +784,27 @@ def run_precision_form(args, world):
     return out
 
 
+def l2_copy_gbs():
+    """Copy bandwidth of a buffer pair that stays in L2 (2 x 24 MiB, read +
+    write bytes, best of 5 runs of 50 copies, CUDA events): the yardstick of
+    work whose data lives in L2, like a batch of small registers."""
+    import torch
+    a = torch.empty(24 << 20, dtype=torch.uint8, device="cuda")
+    b = torch.empty_like(a)
+    a.fill_(1)
+    best = 0.0
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(50):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * a.numel() * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
+
+
 def run_batch_form(args, world):
     """Batched form: 4096 ansatz circuits (n in [10, 22], depth in [4, 32]) in
     one persistent launch per step, complex128 and complex64; tile width and
@@ -797,6 +818,11 @@ def run_batch_form(args, world):
     out = {"workload": f"{len(wl)} hardware-efficient ansatz circuits, n~U[10,22], depth~U[4,32], <Z_q> of every qubit",
            "circuits": len(wl), "gates": int(sum(len(o) for _, _, o in wl))}
     steps = max(1, min(args.steps, 5))
+    l2 = l2_copy_gbs()
+    pk = ctypes.c_double(0.0)
+    Q.dgq_measureFp64Peak(ctypes.byref(pk))
+    out["l2_copy_gbs_measured"] = l2
+    out["fp64_peak_tflops_measured"] = pk.value
     for name, single in (("complex128", False), ("complex64", True)):
         regs = [Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env) for n, _, _ in wl]
         t0 = time.perf_counter()
@@ -841,6 +867,11 @@ def run_batch_form(args, world):
         out[name] = {"ms_per_launch": ms, "circuits_per_s": world * len(wl) / (ms / 1e3),
                      "hbm_gbs_algorithmic": st.sweepBytes / (ms / 1e3) / 1e9,
                      "roofline_frac": st.sweepBytes / (ms / 1e3) / 1e9 / hbm,
+                     "l2_frac": st.sweepBytes / (ms / 1e3) / 1e9 / l2,
+                     "flop_tflops_algorithmic": st.flopsPerLaunch / (ms / 1e3) / 1e12,
+                     "fp64_frac": (st.flopsPerLaunch / (ms / 1e3) / 1e12 / pk.value) if not single else None,
+                     "bound_note": "registers of <= 2^22 amplitudes stay in L2: against HBM, the L2 copy "
+                                   "bandwidth and (complex128) the FP64 peak",
                      "sweep_bytes": int(st.sweepBytes), "state_bytes": int(st.stateBytes),
                      "tile_bits": st.tileBits, "group_factor": st.groupFactor, "grid": st.grid,
                      "ctas_per_sm": st.ctasPerSm, "items": int(st.items), "sweeps": st.sweeps,

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 def run(quest, env, n, ops, k, single):
     q = quest.dgq_createQuregF32(n, env) if single else quest.createQureg(n, env)
     try:
-        assert quest.dgq_setDenseFusion(q, k) == 0
+        assert quest.dgq_setDenseFusion(q, k) == -1  # the default: the predictor chooses
         quest.initZeroState(q)
         C.replay(q, ops)
         amps = quest.state_vector(q)
@@ -58,7 +58,8 @@ def test_dense_fusion_argument_checks(quest, env):
     try:
         with pytest.raises(quest.QuESTError):
             quest.dgq_setDenseFusion(q, 4)
-        assert quest.dgq_setDenseFusion(q, 6) == 0
+        assert quest.dgq_setDenseFusion(q, 6) == -1
         assert quest.dgq_setDenseFusion(q, 0) == 6
+        assert quest.dgq_setDenseFusion(q, -1) == 0
     finally:
         quest.destroyQureg(q, env)
