@@ -20,19 +20,21 @@
 // operand [Whi | Wlo] (the A operand is read once for both), the third as an
 // MMA of width KR on Whi; the epilogue adds the two halves of D.
 //
-// Pipeline (one CTA per SM, persistent over tiles, thirteen warps):
-//   warps 0-7   producer: two threads per column m of tile i (lanes l and
-//               l + 16 of a warp, each half of the column's 2^K amplitudes;
-//               loads coalesced across the half-warp when the lowest
-//               non-target bits are the lowest address bits) load, agree on
-//               the column's scale through a shuffle, split, and store into
-//               X buffer i % 2 (16-byte stores, K-major operand layout);
-//   warp 12     issuer: one thread issues the MMAs of tile i into tensor
+// Pipeline (one CTA per SM, persistent over tiles, 21 warps):
+//   warps 0-15  producer: four threads per column m of tile i (lanes c,
+//               c + 8, c + 16, c + 24 of a warp, a quarter of the column's
+//               2^K amplitudes each; eight consecutive columns per quarter
+//               warp, contiguous when the lowest non-target bits are the
+//               lowest address bits) load the tile, issue the loads of the
+//               next tile into a second set of registers, agree on the
+//               column's scale through shuffles, split, and store into X
+//               buffer i % 2 (16-byte stores, K-major operand layout);
+//   warp 20     issuer: one thread issues the MMAs of tile i into tensor
 //               memory buffer i % 2 and commits them to two mbarriers (the X
 //               buffer is free again; the accumulator is ready);
-//   warps 8-11  consumer: thread m reads row m of the accumulator (TMEM lane
-//               m; warp 8 + j reaches lanes 32 j .. 32 j + 31), releases it,
-//               and writes column m's 2^K outputs back to global memory.
+//   warps 16-19 consumer: thread m reads row m of the accumulator (TMEM lane
+//               m; warp 16 + j reaches lanes 32 j .. 32 j + 31), releases
+//               it, and writes column m's 2^K outputs back to global memory.
 // So the loads of tile i + 1, the MMAs of tile i and the stores of tile
 // i - 1 overlap. All waits poll an mbarrier a bounded number of times; on a
 // timeout the CTA raises the error word, every role stops at its next wait,
@@ -61,8 +63,11 @@ namespace {
 
 constexpr int kTbCols = 128;         // M: tile columns
 constexpr int kTbColBits = 7;
-constexpr int kTbProducers = 256;    // warps 0-7: two threads per column
-constexpr int kTbThreads = 416;      // + consumers (warps 8-11) + issuer (warp 12)
+constexpr int kTbQuarters = 4;       // producer threads per column
+constexpr int kTbProducerWarps = 16;
+constexpr int kTbProducers = 32 * kTbProducerWarps;  // warps 0-15: four threads per column
+constexpr int kTbIssuerWarp = kTbProducerWarps + 4;  // after the consumers (warps 16-19)
+constexpr int kTbThreads = 32 * (kTbIssuerWarp + 1);
 constexpr float kTbWScale = 256.0f;  // W carries 2^8
 
 template <int K>
@@ -73,7 +78,7 @@ struct TbShape {
     static constexpr int WBytes = KR * 2 * KR * 2;       // [Whi | Wlo]: 2 KR rows of KR FP16
     static constexpr int TmemCols = 2 * KR;              // one accumulator (both halves)
     static constexpr int TmemAlloc = 2 * TmemCols;       // double-buffered
-    static constexpr int Smem = WBytes + 4 * XBytes + 4 * kTbCols * 4 + D * 8 + 8 * 16 + 1024;
+    static constexpr int Smem = WBytes + 4 * XBytes + 4 * kTbCols * 4 + 8 * 16 + 1024;
 };
 
 struct TbArgs {
@@ -157,21 +162,31 @@ __host__ __device__ __forceinline__ uint32_t tbOffset(uint32_t row, uint32_t k, 
 
 __device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t *>(&h); }
 
+// Address offset of target pattern s, from the offsets of its bits.
+template <int NB>
+__device__ __forceinline__ uint64_t tbPattern(uint32_t s, const uint64_t (&bit)[NB]) {
+    uint64_t o = 0;
+#pragma unroll
+    for (int i = 0; i < NB; i++) o |= (s >> i) & 1u ? bit[i] : 0ULL;
+    return o;
+}
+
 template <int K>
 __global__ void __launch_bounds__(kTbThreads, 1)
     tcBlockKernel(float2 *__restrict__ st, const __grid_constant__ TbArgs a, const uint4 *__restrict__ Wpacked,
                   uint32_t *__restrict__ error) {
     typedef TbShape<K> S;
+    constexpr int P = S::D / kTbQuarters;  // amplitudes a producer thread holds per tile
+    constexpr int PB = K - 2;              // their pattern bits (the low bits of s)
     extern __shared__ __align__(1024) unsigned char smRaw[];
     unsigned char *base = smRaw + ((1024u - (smemAddr(smRaw) & 1023u)) & 1023u);
     unsigned char *W = base;
     unsigned char *X = base + S::WBytes;  // [buffer][hi, lo]
     float *colInv = reinterpret_cast<float *>(X + 4 * S::XBytes);  // [tile & 3][column]
-    uint64_t *tgtOff = reinterpret_cast<uint64_t *>(colInv + 4 * kTbCols);
-    uint64_t *bars = tgtOff + S::D;  // xFull[2], xEmpty[2], dFull[2], dEmpty[2], drain
+    uint64_t *bars = reinterpret_cast<uint64_t *>(colInv + 4 * kTbCols);  // xFull[2] xEmpty[2] dFull[2] dEmpty[2] drain
     __shared__ uint32_t tmemBase;
     __shared__ volatile uint32_t abortFlag;
-    __shared__ double red[9];
+    __shared__ double red[4];
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t numTiles = 1u << (a.numBits - K - kTbColBits);
@@ -181,11 +196,6 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     // resident W, already in the operand layout
     for (uint32_t i = tid; i < (uint32_t) S::WBytes / 16u; i += kTbThreads)
         reinterpret_cast<uint4 *>(W)[i] = __ldg(Wpacked + i);
-    for (uint32_t s = tid; s < (uint32_t) S::D; s += kTbThreads) {
-        uint64_t o = 0;
-        for (int i = 0; i < K; i++) o |= (uint64_t) ((s >> i) & 1u) << a.tgtPos[i];
-        tgtOff[s] = o;
-    }
     if (tid == 0) {
         abortFlag = 0;
         for (int b = 0; b < 2; b++) {
@@ -199,7 +209,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barDrain) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 12) {
+    if (warp == kTbIssuerWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(&tmemBase)),
                      "r"((uint32_t) S::TmemAlloc)
                      : "memory");
@@ -218,47 +228,57 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     };
     const uint32_t myTiles = blockIdx.x < numTiles ? (numTiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-    if (warp < 8) {
+    if (warp < kTbProducerWarps) {
         // ------------------------------------------------------- producer
-        const uint32_t m = warp * 16u + (lane & 15u), h = lane >> 4;  // column, half
+        // lane = quarter * 8 + c: column m = 8 warp + c, patterns quarter * P + j
+        const uint32_t c8 = lane & 7u, qd = lane >> 3, m = warp * 8u + c8;
         uint64_t colAddr = 0;
         for (int j = 0; j < kTbColBits; j++) colAddr |= (uint64_t) ((m >> j) & 1u) << a.colPos[j];
+        uint64_t lowBit[PB];
+        for (int i = 0; i < PB; i++) lowBit[i] = 1ULL << a.tgtPos[i];
+        const uint64_t qOff = (uint64_t) (qd & 1u) << a.tgtPos[PB] | (uint64_t) (qd >> 1) << a.tgtPos[PB + 1];
         const float inScale = a.normIn ? (float) rsqrt(*a.normIn) : 1.0f;
+        float2 v[P], nv[P];
+        auto loadTile = [&](uint32_t i, float2 (&dst)[P]) {
+            const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr | qOff;
+#pragma unroll
+            for (int j = 0; j < P; j++) dst[j] = __ldg(st + (tb | tbPattern<PB>((uint32_t) j, lowBit)));
+        };
+        if (myTiles > 0) loadTile(0, v);
         for (uint32_t i = 0; i < myTiles; i++) {
             const uint32_t b = i & 1u, u = i >> 1;
+            // the next tile's loads go out first: their latency overlaps this
+            // tile's conversion and the MMAs still reading the buffer
+            if (i + 1 < myTiles) loadTile(i + 1, nv);
             if (u > 0 && !tbWait(barXEmpty + 8 * b, (u - 1) & 1u, &abortFlag, kTbPollLimit)) {
                 if (!abortFlag) atomicOr(error, 2u);
                 abortFlag = 1;
                 break;
             }
-            const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr;
-            constexpr int H = S::D / 2;  // amplitudes of this thread: patterns h H .. h H + H - 1
-            const uint64_t *to = tgtOff + h * H;
-            float2 v[H];
-#pragma unroll
-            for (int s = 0; s < H; s++) v[s] = __ldg(st + (tb | to[s]));
             if (a.hasRestrict) {
+                const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr | qOff;
 #pragma unroll
-                for (int s = 0; s < H; s++) {
-                    const bool keep = ((tb | to[s]) & a.restrictMask) == a.restrictValue;
+                for (int j = 0; j < P; j++) {
+                    const bool keep = ((tb | tbPattern<PB>((uint32_t) j, lowBit)) & a.restrictMask) == a.restrictValue;
                     const float k = keep ? a.restrictScale : 0.0f;
-                    v[s] = make_float2(v[s].x * k, v[s].y * k);
+                    v[j] = make_float2(v[j].x * k, v[j].y * k);
                 }
             }
             float mx = 0.0f;
 #pragma unroll
-            for (int s = 0; s < H; s++) mx = fmaxf(mx, fmaxf(fabsf(v[s].x), fabsf(v[s].y)));
+            for (int j = 0; j < P; j++) mx = fmaxf(mx, fmaxf(fabsf(v[j].x), fabsf(v[j].y)));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
             mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
             // power of two taking the column's largest magnitude to [2^13, 2^14)
             int e = 0;
             if (mx > 0.0f) e = (int) ((__float_as_uint(mx) >> 23) & 0xFFu) - 127;
             const int sh = min(max(13 - e, -100), 100);
             const float scale = ldexpf(1.0f, sh);
-            if (h == 0) colInv[(i & 3u) * kTbCols + m] = ldexpf(1.0f, -sh) * inScale * (1.0f / kTbWScale);
+            if (qd == 0) colInv[(i & 3u) * kTbCols + m] = ldexpf(1.0f, -sh) * inScale * (1.0f / kTbWScale);
             unsigned char *xh = X + b * 2 * S::XBytes;
             unsigned char *xl = xh + S::XBytes;
 #pragma unroll
-            for (int c = 0; c < H / 4; c++) {
+            for (int c = 0; c < P / 4; c++) {
                 uint32_t hi[4], lo[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
@@ -268,19 +288,23 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                     hi[q] = h2bits(hh);
                     lo[q] = h2bits(__floats2half2_rn(xr - hf.x, xi - hf.y));
                 }
-                // patterns h H + 4 c .. + 3: K elements 2 (h H + 4 c) .. + 7
-                const uint32_t off = tbOffset(m, 2u * (h * (uint32_t) H + 4u * (uint32_t) c), kTbCols / 8);
+                // patterns qd P + 4 c .. + 3: K elements 2 (qd P + 4 c) .. + 7
+                const uint32_t off = tbOffset(m, 2u * (qd * (uint32_t) P + 4u * (uint32_t) c), kTbCols / 8);
                 *reinterpret_cast<uint4 *>(xh + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 *reinterpret_cast<uint4 *>(xl + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tbArrive(barXFull + 8 * b);
+#pragma unroll
+            for (int j = 0; j < P; j++) v[j] = nv[j];
         }
-    } else if (warp < 12) {
+    } else if (warp < kTbProducerWarps + 4) {
         // ------------------------------------------------------- consumer
-        const uint32_t j = warp - 8, m = 32u * j + lane;
+        const uint32_t j = warp - kTbProducerWarps, m = 32u * j + lane;  // warp % 4 == j: TMEM lanes 32 j ..
         uint64_t colAddr = 0;
         for (int q = 0; q < kTbColBits; q++) colAddr |= (uint64_t) ((m >> q) & 1u) << a.colPos[q];
+        uint64_t tBit[K];
+        for (int q = 0; q < K; q++) tBit[q] = 1ULL << a.tgtPos[q];
         double norm = 0.0;
         for (uint32_t i = 0; i < myTiles; i++) {
             const uint32_t d = i & 1u, v2 = i >> 1;
@@ -318,8 +342,8 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                 for (int q = 0; q < 8; q++) {
                     const float2 y = make_float2((__uint_as_float(r0[2 * q]) + __uint_as_float(r1[2 * q])) * inv,
                                                  (__uint_as_float(r0[2 * q + 1]) + __uint_as_float(r1[2 * q + 1])) * inv);
-                    st[tb | tgtOff[8 * c + q]] = y;
-                    norm += (double) (y.x * y.x + y.y * y.y);
+                    st[tb | tbPattern<K>((uint32_t) (8 * c + q), tBit)] = y;
+                    if (a.normOut) norm += (double) (y.x * y.x + y.y * y.y);
                 }
             }
             // every value of the accumulator is read: hand the buffer back
@@ -375,7 +399,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         for (int w = 0; w < 4; w++) t += red[w];
         atomicAdd(a.normOut, t);
     }
-    if (warp == 12) {
+    if (warp == kTbIssuerWarp) {
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t) S::TmemAlloc)
