@@ -563,7 +563,8 @@ int buildPrograms(QuregState &s, int W, std::vector<TileProgram> &out, PlanStats
             const size_t nf = tcBlockMatrixFloats(g.numMultiTargets);
             p.denseTcOff = (uint32_t) s.denseHost.size();
             s.denseHost.resize(s.denseHost.size() + (nf + 1) / 2, 0.0);
-            packTcBlockMatrix(g.numMultiTargets, m.data(), reinterpret_cast<float *>(s.denseHost.data() + p.denseTcOff));
+            packTcBlockMatrix(g.numMultiTargets, m.data(), p.denseTargets,
+                              reinterpret_cast<float *>(s.denseHost.data() + p.denseTcOff));
         } else if (s.single && g.numMultiTargets == 6 && s.numBits >= 12) {
             // the tensor-core operand of 4096-amplitude registers: 2 x 128 x 128 floats
             const size_t nf = tcDenseMatrixFloats();

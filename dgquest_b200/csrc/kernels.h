@@ -102,7 +102,9 @@ cudaError_t launchTcDense(float2 *st, const DenseArgs &a, const float *Apacked, 
 // (packTcBlockMatrix, tcBlockMatrixFloats(K) floats).
 bool tcBlockSupported(int numBits, int K);
 size_t tcBlockMatrixFloats(int K);
-void packTcBlockMatrix(int K, const double *U, float *out);
+// targets: address bit of matrix bit i (the kernel's pattern order is
+// ascending by address; the packing permutes U to it)
+void packTcBlockMatrix(int K, const double *U, const uint8_t *targets, float *out);
 cudaError_t launchTcBlock(float2 *st, int K, const DenseArgs &a, const float *Wpacked, uint32_t *error,
                           cudaStream_t s);
 

@@ -50,10 +50,12 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "kernels.h"
 
@@ -171,7 +173,35 @@ __device__ __forceinline__ uint64_t tbPattern(uint32_t s, const uint64_t (&bit)[
     return o;
 }
 
-template <int K>
+// VA: amplitudes moved per global access (1, 2 or 4): 2^L when the L lowest
+// address bits are the lowest targets (adjacent patterns are adjacent
+// amplitudes, so 16- or 32-byte accesses fill whole sectors).
+template <int VA>
+__device__ __forceinline__ void tbLoadRun(const float2 *p, float2 *dst) {
+    if (VA == 1) {
+        dst[0] = __ldg(p);
+    } else {
+        const float4 f = __ldg(reinterpret_cast<const float4 *>(p));
+        dst[0] = make_float2(f.x, f.y);
+        dst[1] = make_float2(f.z, f.w);
+        if (VA == 4) {
+            const float4 g = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+            dst[2] = make_float2(g.x, g.y);
+            dst[3] = make_float2(g.z, g.w);
+        }
+    }
+}
+template <int VA>
+__device__ __forceinline__ void tbStoreRun(float2 *p, const float2 *src) {
+    if (VA == 1) {
+        p[0] = src[0];
+    } else {
+        reinterpret_cast<float4 *>(p)[0] = make_float4(src[0].x, src[0].y, src[1].x, src[1].y);
+        if (VA == 4) reinterpret_cast<float4 *>(p)[1] = make_float4(src[2].x, src[2].y, src[3].x, src[3].y);
+    }
+}
+
+template <int K, int VA>
 __global__ void __launch_bounds__(kTbThreads, 1)
     tcBlockKernel(float2 *__restrict__ st, const __grid_constant__ TbArgs a, const uint4 *__restrict__ Wpacked,
                   uint32_t *__restrict__ error) {
@@ -242,7 +272,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         auto loadTile = [&](uint32_t i, float2 (&dst)[P]) {
             const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr | qOff;
 #pragma unroll
-            for (int j = 0; j < P; j++) dst[j] = __ldg(st + (tb | tbPattern<PB>((uint32_t) j, lowBit)));
+            for (int j = 0; j < P; j += VA) tbLoadRun<VA>(st + (tb | tbPattern<PB>((uint32_t) j, lowBit)), dst + j);
         };
         if (myTiles > 0) loadTile(0, v);
         for (uint32_t i = 0; i < myTiles; i++) {
@@ -338,13 +368,15 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                     : "r"(tbase + (uint32_t) S::KR + 16u * (uint32_t) c)
                     : "memory");
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float2 y[8];
 #pragma unroll
                 for (int q = 0; q < 8; q++) {
-                    const float2 y = make_float2((__uint_as_float(r0[2 * q]) + __uint_as_float(r1[2 * q])) * inv,
-                                                 (__uint_as_float(r0[2 * q + 1]) + __uint_as_float(r1[2 * q + 1])) * inv);
-                    st[tb | tbPattern<K>((uint32_t) (8 * c + q), tBit)] = y;
-                    if (a.normOut) norm += (double) (y.x * y.x + y.y * y.y);
+                    y[q] = make_float2((__uint_as_float(r0[2 * q]) + __uint_as_float(r1[2 * q])) * inv,
+                                       (__uint_as_float(r0[2 * q + 1]) + __uint_as_float(r1[2 * q + 1])) * inv);
+                    if (a.normOut) norm += (double) (y[q].x * y[q].x + y[q].y * y[q].y);
                 }
+#pragma unroll
+                for (int q = 0; q < 8; q += VA) tbStoreRun<VA>(st + (tb | tbPattern<K>((uint32_t) (8 * c + q), tBit)), y + q);
             }
             // every value of the accumulator is read: hand the buffer back
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -411,10 +443,36 @@ __global__ void __launch_bounds__(kTbThreads, 1)
 
 size_t tcBlockMatrixFloats(int K) { return K == 5 ? TbShape<5>::WBytes / 4 : TbShape<6>::WBytes / 4; }
 
+// The kernel takes the targets in ascending address order (pattern bit i =
+// the i-th lowest target), so that the lowest targets, when they are the
+// lowest address bits, make adjacent patterns adjacent amplitudes. perm[s]:
+// the matrix index (bit j = target j as given) of the ascending-order
+// pattern s.
+static void ascendingPatterns(int K, const uint8_t *targets, int *perm) {
+    int order[8];
+    for (int i = 0; i < K; i++) order[i] = i;
+    std::sort(order, order + K, [&](int x, int y) { return targets[x] < targets[y]; });
+    for (int s = 0; s < (1 << K); s++) {
+        int m = 0;
+        for (int i = 0; i < K; i++)
+            if ((s >> i) & 1) m |= 1 << order[i];
+        perm[s] = m;
+    }
+}
+
 // [Whi | Wlo] in the K-major FP16 operand layout: row n < KR is output real
-// index n of Whi, row KR + n the same of Wlo; both scaled by 2^8.
-void packTcBlockMatrix(int K, const double *U, float *out) {
+// index n of Whi, row KR + n the same of Wlo; both scaled by 2^8; patterns in
+// ascending target order.
+void packTcBlockMatrix(int K, const double *Uin, const uint8_t *targets, float *out) {
     const int D = 1 << K, KR = 2 * D;
+    int perm[64];
+    ascendingPatterns(K, targets, perm);
+    std::vector<double> U((size_t) 2 * D * D);
+    for (int r = 0; r < D; r++)
+        for (int c = 0; c < D; c++) {
+            U[(size_t) 2 * (r * D + c)] = Uin[2 * (perm[r] * D + perm[c])];
+            U[(size_t) 2 * (r * D + c) + 1] = Uin[2 * (perm[r] * D + perm[c]) + 1];
+        }
     const uint32_t groups = (uint32_t) (2 * KR / 8);
     unsigned char *bytes = reinterpret_cast<unsigned char *>(out);
     std::memset(bytes, 0, (size_t) KR * 2 * KR * 2);
@@ -435,6 +493,16 @@ void packTcBlockMatrix(int K, const double *U, float *out) {
         }
 }
 
+template <int K, int VA>
+static cudaError_t launchTcBlockKV(float2 *st, const TbArgs &a, const uint4 *w, uint32_t *error, unsigned grid,
+                                   cudaStream_t s) {
+    static std::atomic<uint64_t> optIn{0};
+    cudaError_t e = ensureSmemOptIn((const void *) tcBlockKernel<K, VA>, TbShape<K>::Smem, optIn);
+    if (e != cudaSuccess) return e;
+    tcBlockKernel<K, VA><<<grid, kTbThreads, TbShape<K>::Smem, s>>>(st, a, w, error);
+    return cudaGetLastError();
+}
+
 bool tcBlockSupported(int numBits, int K) { return (K == 5 || K == 6) && numBits >= K + kTbColBits; }
 
 cudaError_t launchTcBlock(float2 *st, int K, const DenseArgs &da, const float *Wpacked, uint32_t *error,
@@ -449,13 +517,16 @@ cudaError_t launchTcBlock(float2 *st, int K, const DenseArgs &da, const float *W
     a.restrictScale = (float) da.restrictScale;
     a.normIn = da.normIn;
     a.normOut = da.normOut;
-    // targets from the dense map; columns: the 7 lowest other bits; the rest index tiles
+    // targets in ascending address order (the operand was packed in that
+    // order); columns: the 7 lowest other bits; the rest index tiles
     uint64_t tmask = 0;
     for (int b = 0; b < da.tileBits; b++)
-        if (da.rowBit[b] >= 0) {
-            a.tgtPos[da.rowBit[b]] = da.tilePos[b];
-            tmask |= 1ULL << da.tilePos[b];
-        }
+        if (da.rowBit[b] >= 0) tmask |= 1ULL << da.tilePos[b];
+    int nt0 = 0;
+    for (int b = 0; b < da.numBits; b++)
+        if ((tmask >> b) & 1ULL) a.tgtPos[nt0++] = (uint8_t) b;
+    int low = 0;  // targets that are the lowest address bits 0, 1, ...
+    while (low < nt0 && a.tgtPos[low] == low) low++;
     int nc = 0, nt = 0;
     for (int b = 0; b < da.numBits; b++) {
         if ((tmask >> b) & 1ULL) continue;
@@ -471,21 +542,16 @@ cudaError_t launchTcBlock(float2 *st, int K, const DenseArgs &da, const float *W
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = 1u << (a.numBits - K - kTbColBits);
     const unsigned grid = (unsigned) (tiles < (uint32_t) sms ? tiles : (uint32_t) sms);
-    cudaError_t e;
+    const int va = low >= 2 ? 4 : (low == 1 ? 2 : 1);
+    const uint4 *w = reinterpret_cast<const uint4 *>(Wpacked);
     if (K == 5) {
-        static std::atomic<uint64_t> optIn{0};
-        e = ensureSmemOptIn((const void *) tcBlockKernel<5>, TbShape<5>::Smem, optIn);
-        if (e != cudaSuccess) return e;
-        tcBlockKernel<5><<<grid, kTbThreads, TbShape<5>::Smem, s>>>(st, a, reinterpret_cast<const uint4 *>(Wpacked),
-                                                                    error);
-    } else {
-        static std::atomic<uint64_t> optIn{0};
-        e = ensureSmemOptIn((const void *) tcBlockKernel<6>, TbShape<6>::Smem, optIn);
-        if (e != cudaSuccess) return e;
-        tcBlockKernel<6><<<grid, kTbThreads, TbShape<6>::Smem, s>>>(st, a, reinterpret_cast<const uint4 *>(Wpacked),
-                                                                    error);
+        if (va == 4) return launchTcBlockKV<5, 4>(st, a, w, error, grid, s);
+        if (va == 2) return launchTcBlockKV<5, 2>(st, a, w, error, grid, s);
+        return launchTcBlockKV<5, 1>(st, a, w, error, grid, s);
     }
-    return cudaGetLastError();
+    if (va == 4) return launchTcBlockKV<6, 4>(st, a, w, error, grid, s);
+    if (va == 2) return launchTcBlockKV<6, 2>(st, a, w, error, grid, s);
+    return launchTcBlockKV<6, 1>(st, a, w, error, grid, s);
 }
 
 }  // namespace dgq
