@@ -20,21 +20,22 @@
 // operand [Whi | Wlo] (the A operand is read once for both), the third as an
 // MMA of width KR on Whi; the epilogue adds the two halves of D.
 //
-// Pipeline (one CTA per SM, persistent over tiles, 21 warps):
+// Pipeline (one CTA per SM, persistent over tiles, 25 warps):
 //   warps 0-15  producer: four threads per column m of tile i (lanes c,
 //               c + 8, c + 16, c + 24 of a warp, a quarter of the column's
 //               2^K amplitudes each; eight consecutive columns per quarter
 //               warp, contiguous when the lowest non-target bits are the
-//               lowest address bits) load the tile, issue the loads of the
-//               next tile into a second set of registers, agree on the
-//               column's scale through shuffles, split, and store into X
+//               lowest address bits) load the tile (before waiting for the
+//               buffer), agree on the column's scale through shuffles,
+//               split, and store into X
 //               buffer i % 2 (16-byte stores, K-major operand layout);
-//   warp 20     issuer: one thread issues the MMAs of tile i into tensor
+//   warp 24     issuer: one thread issues the MMAs of tile i into tensor
 //               memory buffer i % 2 and commits them to two mbarriers (the X
 //               buffer is free again; the accumulator is ready);
-//   warps 16-19 consumer: thread m reads row m of the accumulator (TMEM lane
-//               m; warp 16 + j reaches lanes 32 j .. 32 j + 31), releases
-//               it, and writes column m's 2^K outputs back to global memory.
+//   warps 16-23 consumer: row m of the accumulator (TMEM lane m; warps
+//               16 + j and 20 + j reach lanes 32 j .. 32 j + 31) is read by
+//               two threads, each half of the outputs; they release it and
+//               write column m's 2^K outputs back to global memory.
 // So the loads of tile i + 1, the MMAs of tile i and the stores of tile
 // i - 1 overlap. All waits poll an mbarrier a bounded number of times; on a
 // timeout the CTA raises the error word, every role stops at its next wait,
@@ -68,7 +69,8 @@ constexpr int kTbColBits = 7;
 constexpr int kTbQuarters = 4;       // producer threads per column
 constexpr int kTbProducerWarps = 16;
 constexpr int kTbProducers = 32 * kTbProducerWarps;  // warps 0-15: four threads per column
-constexpr int kTbIssuerWarp = kTbProducerWarps + 4;  // after the consumers (warps 16-19)
+constexpr int kTbConsumerWarps = 8;                  // warps 16-23: two per TMEM lane quarter
+constexpr int kTbIssuerWarp = kTbProducerWarps + kTbConsumerWarps;
 constexpr int kTbThreads = 32 * (kTbIssuerWarp + 1);
 constexpr float kTbWScale = 256.0f;  // W carries 2^8
 
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     uint64_t *bars = reinterpret_cast<uint64_t *>(colInv + 4 * kTbCols);  // xFull[2] xEmpty[2] dFull[2] dEmpty[2] drain
     __shared__ uint32_t tmemBase;
     __shared__ volatile uint32_t abortFlag;
-    __shared__ double red[4];
+    __shared__ double red[kTbConsumerWarps];
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t numTiles = 1u << (a.numBits - K - kTbColBits);
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                          : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barXEmpty + 8 * b) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barDFull + 8 * b) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barDEmpty + 8 * b), "r"(kTbCols)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barDEmpty + 8 * b), "r"(32 * kTbConsumerWarps)
                          : "memory");
         }
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barDrain) : "memory");
@@ -268,18 +270,16 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         for (int i = 0; i < PB; i++) lowBit[i] = 1ULL << a.tgtPos[i];
         const uint64_t qOff = (uint64_t) (qd & 1u) << a.tgtPos[PB] | (uint64_t) (qd >> 1) << a.tgtPos[PB + 1];
         const float inScale = a.normIn ? (float) rsqrt(*a.normIn) : 1.0f;
-        float2 v[P], nv[P];
-        auto loadTile = [&](uint32_t i, float2 (&dst)[P]) {
-            const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr | qOff;
-#pragma unroll
-            for (int j = 0; j < P; j += VA) tbLoadRun<VA>(st + (tb | tbPattern<PB>((uint32_t) j, lowBit)), dst + j);
-        };
-        if (myTiles > 0) loadTile(0, v);
+        float2 v[P];
         for (uint32_t i = 0; i < myTiles; i++) {
             const uint32_t b = i & 1u, u = i >> 1;
-            // the next tile's loads go out first: their latency overlaps this
-            // tile's conversion and the MMAs still reading the buffer
-            if (i + 1 < myTiles) loadTile(i + 1, nv);
+            // the tile's loads go out before the wait for the buffer: their
+            // latency overlaps the MMAs still reading it
+            {
+                const uint64_t tb = tileBase(blockIdx.x + i * gridDim.x) | colAddr | qOff;
+#pragma unroll
+                for (int j = 0; j < P; j += VA) tbLoadRun<VA>(st + (tb | tbPattern<PB>((uint32_t) j, lowBit)), v + j);
+            }
             if (u > 0 && !tbWait(barXEmpty + 8 * b, (u - 1) & 1u, &abortFlag, kTbPollLimit)) {
                 if (!abortFlag) atomicOr(error, 2u);
                 abortFlag = 1;
@@ -325,12 +325,13 @@ __global__ void __launch_bounds__(kTbThreads, 1)
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tbArrive(barXFull + 8 * b);
-#pragma unroll
-            for (int j = 0; j < P; j++) v[j] = nv[j];
         }
-    } else if (warp < kTbProducerWarps + 4) {
+    } else if (warp < kTbIssuerWarp) {
         // ------------------------------------------------------- consumer
-        const uint32_t j = warp - kTbProducerWarps, m = 32u * j + lane;  // warp % 4 == j: TMEM lanes 32 j ..
+        // warp % 4 == j reaches TMEM lanes 32 j ..; the two warps of a lane
+        // quarter take the first and the second half of the outputs
+        const uint32_t j = (warp - kTbProducerWarps) & 3u, half = (warp - kTbProducerWarps) >> 2;
+        const uint32_t m = 32u * j + lane;
         uint64_t colAddr = 0;
         for (int q = 0; q < kTbColBits; q++) colAddr |= (uint64_t) ((m >> q) & 1u) << a.colPos[q];
         uint64_t tBit[K];
@@ -349,7 +350,8 @@ __global__ void __launch_bounds__(kTbThreads, 1)
             const uint32_t tbase = tmem + ((32u * j) << 16) + d * (uint32_t) S::TmemCols;
             // 16 output reals (8 amplitudes) per chunk, written back as they come
 #pragma unroll
-            for (int c = 0; c < S::KR / 16; c++) {
+            for (int cc = 0; cc < S::KR / 32; cc++) {
+                const int c = (int) half * (S::KR / 32) + cc;
                 uint32_t r0[16], r1[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         if (a.normOut) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) norm += __shfl_xor_sync(0xffffffffu, norm, o);
-            if (lane == 0) red[j] = norm;
+            if (lane == 0) red[warp - kTbProducerWarps] = norm;
         }
     } else if (lane == 0) {
         // ------------------------------------------------------- issuer
@@ -428,7 +430,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     __syncthreads();
     if (a.normOut && tid == 0) {
         double t = 0.0;
-        for (int w = 0; w < 4; w++) t += red[w];
+        for (int w = 0; w < kTbConsumerWarps; w++) t += red[w];
         atomicAdd(a.normOut, t);
     }
     if (warp == kTbIssuerWarp) {
