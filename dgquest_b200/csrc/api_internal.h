@@ -75,13 +75,25 @@ enum ErrorCode {
     E_INVALID_ARGUMENT = 104,
 };
 
+// The predictor also chooses the form of a plan (dgq_setDenseFusion(q, -1),
+// the default): register-phase tiles, or the gates fused into dense blocks of
+// K = 5, 6 or 7 qubits, each block one dense sweep. A dense sweep costs a
+// fixed time per block per amplitude (denseMs, ms per block per 2^30
+// amplitudes) for three variants: complex128 SIMT, complex64 SIMT and
+// complex64 on the tensor cores (K = 5 and 6). Built-in: figures measured on
+// B200 at 30 qubits (K = 6: 58.1, 37.4 and 5.5 ms; K = 5 on the tensor
+// cores 5.24 ms), the SIMT K = 5 and 7 scaled by 2^K (the SIMT dense kernel
+// is compute-bound, 8 x 2^K flops per amplitude). Tiles on a complex64
+// register (the paired form) cost c64TileFactor times the complex128
+// prediction (measured: 77 of 140 ms on the 30-qubit circuit). A dense form
+// is taken when its prediction is below denseMargin times the tile form's.
 enum DenseVariant { DV_F64 = 0, DV_C64 = 1, DV_C64_TC = 2 };
 
 struct CostModel {
     double sweepSecondsPerAmp = 2.6e-3 / 1073741824.0;
     double phaseSecondsPerAmp = 1.8e-3 / 1073741824.0;
     double launchSeconds = 3e-6;
-    double denseMs[3][3] = {{29.05, 58.1, 116.2}, {18.7, 37.4, 74.8}, {0.0, 14.8, 0.0}};  // [variant][K - 5]
+    double denseMs[3][3] = {{29.05, 58.1, 116.2}, {18.7, 37.4, 74.8}, {5.24, 5.5, 0.0}};  // [variant][K - 5]
     double c64TileFactor = 0.55;
     double denseMargin = 0.8;
 };

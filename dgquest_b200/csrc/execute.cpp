@@ -25,19 +25,7 @@ namespace dgq_api {
 // The rates can be replaced by a calibration of this GPU
 // (dgquest_b200/calibrate.py measures them; dgq_setCostModel installs them,
 // dgq_loadCostModel or DGQ_COST_FILE reads the file it writes).
-// The predictor also chooses the form of a plan (dgq_setDenseFusion(q, -1),
-// the default): register-phase tiles, or the gates fused into dense blocks of
-// K = 5, 6 or 7 qubits, each block one dense sweep. A dense sweep costs a
-// fixed time per block per amplitude (denseMs, ms per block per 2^30
-// amplitudes) for three variants: complex128 SIMT, complex64 SIMT and
-// complex64 on the tensor cores (K = 6 only). Built-in: the K = 6 figures
-// measured on B200 at 30 qubits (58.1, 37.4 and 14.8 ms), K = 5 and 7 scaled
-// by 2^K (the SIMT dense kernel is compute-bound, 8 x 2^K flops per
-// amplitude). Tiles on a complex64 register (the paired form) cost
-// c64TileFactor times the complex128 prediction (measured: 77 of 140 ms on
-// the 30-qubit circuit). A dense form is taken when its prediction is below
-// denseMargin times the tile form's.
-// complex64 dense 6-qubit sweeps on the tensor cores (dgq_setTensorCores)
+// complex64 dense 5- and 6-qubit sweeps on the tensor cores (dgq_setTensorCores)
 std::atomic<int> g_tensorCores{1};
 
 std::mutex g_costMutex;
