@@ -901,6 +901,7 @@ def run_serving_form(args, world):
         # a running server: memory pool grown, then a warm-up stream of other
         # requests (same distribution, another seed) before the measured one
         srv.prewarm(single)
+        specialised = srv.prespecialise(single)
         warm = S.make_requests(args.serve_warmup, rate=200.0, single=single, seed=C.config_seed(5, 900000),
                                first_id=200000)
         cold = S.summarize(srv.serve(warm, realtime=True)) if warm else None
@@ -915,6 +916,7 @@ def run_serving_form(args, world):
                                     "p50_ms": lo["p50_ms"], "p99_ms": lo["p99_ms"],
                                     "circuits_per_s": lo["circuits_per_s"]}
         st["registers_reused"] = srv.reused
+        st["prespecialised_kernels"] = specialised
         srv.close()
         if cold:
             st["warmup_stream"] = {"requests": cold["requests"], "p50_ms": cold["p50_ms"], "p99_ms": cold["p99_ms"],

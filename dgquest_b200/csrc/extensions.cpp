@@ -496,6 +496,44 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
     return (int) src.size() < len ? (int) s.planned.size() : -2;
 }
 
+int dgq_specialiseGates(int numQubits, int precision, int count, const int32_t *types, const uint64_t *targetMasks,
+                        const uint64_t *controlMasks, const double *operands, int background) {
+    if (numQubits < 1 || numQubits > dgq::kMaxStateBits - 2 || count < 0 || precision < 1 || precision > 3 ||
+        (count > 0 && (!types || !targetMasks || !controlMasks || !operands))) {
+        raise(E_INVALID_ARGUMENT, __func__);
+        return -1;
+    }
+    if (!dgq::jitEnabled()) return 0;
+    // the plan a register of this size and precision makes for these gates
+    // after initZeroState (the same planning as dgq_sweepSource)
+    QuregState s;
+    s.numQubits = numQubits;
+    s.numBits = std::max(numQubits, dgq::kMinTileBits);
+    s.single = precision == 1 || precision == 3;
+    s.allowPaired = precision == 1;
+    resetMapping(s);
+    if (!gatesFromArrays(numQubits, count, types, targetMasks, controlMasks, operands, s.pending, __func__)) return -1;
+    s.initPending = true;
+    s.initKind = dgq::INIT_CLASSICAL;
+    if (!planPending(s, __func__, false)) return -1;
+    std::vector<std::string> sources;
+    for (auto &p : s.planned) {
+        p.isSingle = s.single ? 1 : 0;
+        if (!p.denseK) sources.push_back(dgq::generateSweepSource(p, s.plannedTileBits));
+    }
+    if (background) {
+        dgq::jitCompileInBackground(sources);
+        return (int) sources.size();
+    }
+    std::vector<CUfunction> fns;
+    std::string err;
+    if (!dgq::jitGetKernels(sources, fns, nullptr, &err)) {
+        raise(E_UNSUPPORTED, __func__, err.c_str());
+        return -1;
+    }
+    return (int) sources.size();
+}
+
 int dgq_compileSweepSource(const char *source, char *log, int len) {
     if (!source) return -1;
     std::vector<char> cubin;

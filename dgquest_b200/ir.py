@@ -114,3 +114,17 @@ def plan(ops, n, tile_bits=0, want_merged=False):
     if want_merged:
         return st, merged[:nm.value].tolist()
     return st
+
+
+def specialise(ops, n, precision, background=True):
+    """Compiles ahead of time the specialised sweep kernels a register of n
+    qubits (precision 1 complex64, 2 complex128) would use for the op list
+    after initZeroState; returns the number of kernels."""
+    from .quest import _check, _library
+    P = ctypes.POINTER
+    t, tm, cm, o = ops_to_ir(ops, n)
+    r = _library().dgq_specialiseGates(n, precision, len(t), t.ctypes.data_as(P(ctypes.c_int32)),
+                                       tm.ctypes.data_as(P(ctypes.c_uint64)), cm.ctypes.data_as(P(ctypes.c_uint64)),
+                                       o.ctypes.data_as(P(ctypes.c_double)), 1 if background else 0)
+    _check()
+    return r

@@ -217,6 +217,7 @@ _SIGS = {
     "dgq_sweepSource": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I, I,
                             ctypes.c_char_p, I]),
     "dgq_compileSweepSource": (I, [ctypes.c_char_p, ctypes.c_char_p, I]),
+    "dgq_specialiseGates": (I, [I, I, I, P(ctypes.c_int32), P(ctypes.c_uint64), P(ctypes.c_uint64), P(D), I]),
     "dgq_setSpecialisationMinBits": (I, [I]),
     "dgq_setSpecialisationPolicy": (I, [I]),
     "dgq_setTensorCores": (I, [I]),

@@ -178,6 +178,18 @@ class Server:
                 Q.destroyQureg(q, self.env)
         return used
 
+    def prespecialise(self, single=False, n_range=None, background=True):
+        """Queues the compiles of the specialised kernels of the circuit
+        structures that recur in the stream: GHZ+QFT of every size from the
+        JIT threshold (22 qubits) up (random-layer and Bernstein-Vazirani
+        structures depend on each request's seed). Returns the kernels queued."""
+        from . import ir
+        lo, hi = n_range or ((16, 33) if single else (16, 32))
+        total = 0
+        for n in range(max(lo, 22), hi + 1):
+            total += ir.specialise(C.ghz_qft(n), n, 1 if single else 2, background=background)
+        return total
+
     def _take(self, r, in_use):
         """With the lock held: an idle register for r (or None: create one),
         and the idle registers to destroy so that a new one fits."""

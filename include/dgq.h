@@ -268,6 +268,18 @@ int dgq_sweepSource(int numQubits, int tileBits, int count, const int32_t *types
                     int len);
 int dgq_compileSweepSource(const char *source, char *log, int len);
 
+/* Compiles ahead of time the specialised sweep kernels that a register of
+ * numQubits and `precision` (1 complex64, 2 complex128, 3 complex64 without
+ * the paired form) would use for these gates after initZeroState, so that
+ * a later run of the same circuit structure finds them compiled. With
+ * background = 1 the compiles are queued on the library's compile threads
+ * and the call returns at once (no GPU work); with 0 they are compiled and
+ * loaded for the current device before it returns. Returns the number of
+ * kernels, or -1 on error. No counterpart in dgQuEST (the serving loop uses
+ * it for circuit structures that recur, such as GHZ+QFT of each size). */
+int dgq_specialiseGates(int numQubits, int precision, int count, const int32_t *types, const uint64_t *targetMasks,
+                        const uint64_t *controlMasks, const double *operands, int background);
+
 /* Circuit records: one 80-byte record per API call, applied in order
  * through the entry points of QuEST.h (same validation, same lazy
  * recording). kind: 0 hadamard, 1 pauliX, 2 pauliY, 3 pauliZ, 4 sGate,

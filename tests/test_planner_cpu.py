@@ -94,3 +94,14 @@ def test_plan_gates_rejects_invalid_gates(bad):
         Q.dgq_sweepSource(n, 0, len(t), t.ctypes.data_as(P(ctypes.c_int32)), tm.ctypes.data_as(P(ctypes.c_uint64)),
                           cm.ctypes.data_as(P(ctypes.c_uint64)), o.ctypes.data_as(P(ctypes.c_double)), 0, 2, buf,
                           len(buf))
+
+
+def test_specialise_ahead_counts_the_plans_kernels():
+    # host-only: the number of kernels equals the number of sweeps the plan
+    # of the same gates would launch (GHZ+QFT has no dense sweeps)
+    n = 24
+    ops = C.ghz_qft(n)
+    count = ir.specialise(ops, n, 2, background=True)
+    assert count == ir.plan(ops, n, 0).sweeps
+    with pytest.raises(Q.QuESTError):
+        Q.dgq_specialiseGates(n, 4, 0, None, None, None, None, 1)
