@@ -776,8 +776,8 @@ def run_precision_form(args, world):
             "fidelity": Q.calcFidelity(q64, q), "max_abs_err_sampled": err,
             "device_errors": int(Q.dgq_getDeviceErrors()),
             "vs_paired_form": ms / out["complex64"]["ms_per_circuit"],
-            "note": "gates fused into dense 6-qubit unitaries (FP64 composition), one tcgen05 kind::tf32 "
-                    "3xTF32 GEMM sweep per block; warm-up 1, timed 1"}
+            "note": "gates fused into dense 6-qubit unitaries (FP64 composition), one tcgen05 kind::f16 "
+                    "split-FP16 GEMM sweep per block; warm-up 1, timed 1"}
         Q.destroyQureg(q, env)
     Q.destroyQureg(q64, env)
     Q.destroyQuESTEnv(env)
@@ -785,11 +785,11 @@ def run_precision_form(args, world):
 
 
 def l2_copy_gbs():
-    """Copy bandwidth of a buffer pair that stays in L2 (2 x 24 MiB, read +
-    write bytes, best of 5 runs of 50 copies, CUDA events): the yardstick of
+    """Copy bandwidth of a buffer pair that stays in L2 (2 x 8 MiB, read +
+    write bytes, best of 5 runs of 200 copies, CUDA events): the yardstick of
     work whose data lives in L2, like a batch of small registers."""
     import torch
-    a = torch.empty(24 << 20, dtype=torch.uint8, device="cuda")
+    a = torch.empty(8 << 20, dtype=torch.uint8, device="cuda")
     b = torch.empty_like(a)
     a.fill_(1)
     best = 0.0
@@ -797,11 +797,11 @@ def l2_copy_gbs():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(50):
+        for _ in range(200):
             b.copy_(a)
         e1.record()
         torch.cuda.synchronize()
-        best = max(best, 2.0 * a.numel() * 50 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+        best = max(best, 2.0 * a.numel() * 200 / (e0.elapsed_time(e1) / 1e3) / 1e9)
     return best
 
 
