@@ -907,14 +907,25 @@ def run_serving_form(args, world):
         cold = S.summarize(srv.serve(warm, realtime=True)) if warm else None
         res = srv.serve(reqs, realtime=True)
         st = S.summarize(res)
-        if args.serve_low_rate > 0:
-            # the same server below its capacity: latency is service time, not queueing
-            low = S.make_requests(args.serve_low_requests, rate=args.serve_low_rate, single=single,
-                                  seed=C.config_seed(5, 910000), first_id=300000)
-            lo = S.summarize(srv.serve(low, realtime=True))
-            st["below_capacity"] = {"offered_rate": args.serve_low_rate, "requests": lo["requests"],
-                                    "p50_ms": lo["p50_ms"], "p99_ms": lo["p99_ms"],
-                                    "circuits_per_s": lo["circuits_per_s"]}
+        # the same server at lower offered rates: where latency stops being
+        # queueing (service time = done - admitted, queueing = admitted - arrival)
+        sweep = []
+        for k, rate in enumerate(float(x) for x in args.serve_rates.split(",") if x):
+            low = S.make_requests(args.serve_rate_requests, rate=rate, single=single,
+                                  seed=C.config_seed(5, 910000 + k), first_id=300000 + 1000 * k)
+            rs = srv.serve(low, realtime=True)
+            lo = S.summarize(rs)
+            svc = np.array([r.done - r.admitted for r in rs]) * 1e3
+            que = np.array([r.admitted - r.arrival for r in rs]) * 1e3
+            big = [r.latency * 1e3 for r, q in zip(rs, low) if q.n >= 31]
+            small = [r.latency * 1e3 for r, q in zip(rs, low) if q.n <= 28]
+            sweep.append({"offered_rate": rate, "requests": lo["requests"], "p50_ms": lo["p50_ms"],
+                          "p99_ms": lo["p99_ms"], "circuits_per_s": lo["circuits_per_s"],
+                          "service_p50_ms": float(np.percentile(svc, 50)), "service_p99_ms": float(np.percentile(svc, 99)),
+                          "queue_p99_ms": float(np.percentile(que, 99)),
+                          "p99_ms_n_le_28": float(np.percentile(small, 99)) if small else None,
+                          "p50_ms_n_ge_31": float(np.percentile(big, 50)) if big else None})
+        st["rate_sweep"] = sweep
         st["registers_reused"] = srv.reused
         st["prespecialised_kernels"] = specialised
         srv.close()
@@ -947,9 +958,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-grid32", action="store_true")
     ap.add_argument("--serve-warmup", type=int, default=60, help="requests of the serving warm-up stream")
-    ap.add_argument("--serve-low-rate", type=float, default=4.0,
-                    help="arrival rate (req/s) of a second, below-capacity serving stream (0: skip)")
-    ap.add_argument("--serve-low-requests", type=int, default=40)
+    ap.add_argument("--serve-rates", default="4,8,12",
+                    help="offered rates (req/s) of the serving rate sweep on the same server ('' to skip)")
+    ap.add_argument("--serve-rate-requests", type=int, default=60, help="requests per rate of the sweep")
     ap.add_argument("--serve-policy", type=int, default=1, choices=[1, 2],
                     help="specialisation policy of the serving loop (2: no background compiles)")
     ap.add_argument("--no-host-tier", action="store_true", help="skip the host-tier (pinned host memory) run")
