@@ -63,3 +63,35 @@ def test_dense_fusion_argument_checks(quest, env):
         assert quest.dgq_setDenseFusion(q, -1) == 0
     finally:
         quest.destroyQureg(q, env)
+
+
+def test_form_choice_takes_dense_blocks_when_cheaper(quest, env):
+    """With dense rates that make 6-qubit blocks cheap, the default form
+    choice fuses the circuit into dense blocks: the same result as forcing
+    that form, and the oracle's amplitudes (complex128, 1e-12)."""
+    Q = quest
+    keys = [(v, k) for v in range(3) for k in (5, 6, 7)]
+    prev = {key: Q.dgq_getDenseCost(*key) for key in keys}
+    n = 22  # large enough that a block's launch overhead (3 us) does not decide
+    ops = C.random_layers(n, 6, C.config_seed(2, 777))
+    try:
+        for k in (5, 7):
+            Q.dgq_setDenseCost(0, k, 1e3)
+        Q.dgq_setDenseCost(0, 6, 1e-3)
+        out = {}
+        for name, fusion in (("auto", -1), ("forced", 6)):
+            q = Q.createQureg(n, env)
+            Q.dgq_setDenseFusion(q, fusion)
+            C.replay(q, ops)
+            Q.dgq_planPending(q)
+            st = Q.plan_stats(q)
+            Q.dgq_launchPlanned(q)
+            out[name] = (Q.state_vector(q), st.formK, st.formAuto, st.denseBlocks)
+            Q.destroyQureg(q, env)
+        assert out["auto"][1:] == (6, 1, out["forced"][3]) and out["forced"][3] > 0
+        assert np.abs(out["auto"][0] - out["forced"][0]).max() == 0.0
+        ref, _, _ = oracle.run(n, ops)
+        assert np.abs(out["auto"][0] - ref).max() <= 1e-12
+    finally:
+        for key, r in prev.items():
+            Q.dgq_setDenseCost(*key, r)

@@ -76,3 +76,33 @@ print("ok")
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip().endswith("ok")
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_specialise_ahead_of_time(quest, env, single):
+    """dgq_specialiseGates (foreground) compiles and loads the kernels a
+    register's plan of the same gates uses: the plan then compiles nothing
+    and reuses every kernel, with the oracle's result."""
+    from dgquest_b200 import ir
+    Q = quest
+    prev_bits = Q.dgq_setSpecialisationMinBits(1)
+    try:
+        n = 16
+        ops = C.random_layers(n, 4, C.config_seed(2, 5150 + int(single)))  # a structure no other test plans
+        count = ir.specialise(ops, n, 1 if single else 2, background=False)
+        q = Q.dgq_createQuregF32(n, env) if single else Q.createQureg(n, env)
+        C.replay(q, ops)
+        Q.dgq_planPending(q)
+        st = Q.plan_stats(q)
+        Q.dgq_launchPlanned(q)
+        amps = Q.state_vector(q)
+        Q.destroyQureg(q, env)
+        assert count == st.sweeps
+        assert st.jitCompiled == 0 and st.jitReused == st.sweeps
+        ref, _, _ = oracle.run(n, ops)
+        if single:
+            assert abs(np.vdot(ref, amps)) ** 2 >= 1 - 1e-6
+        else:
+            assert np.abs(amps - ref).max() <= 1e-12
+    finally:
+        Q.dgq_setSpecialisationMinBits(-1 if prev_bits == 22 else prev_bits)
