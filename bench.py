@@ -13,7 +13,9 @@ perfect matching; 20 layers; seed 20261203 + 2000; MT19937 draws.
           for every qubit; kernel programs travel host->device as kernel
           parameters, the amplitude and probabilities come back
   roofline  the tile kernel (the only kernel of a step) against the measured
-          HBM copy bandwidth; algorithmic bytes per launch = 2 * 2^30 * 16 B
+          HBM copy bandwidth; algorithmic bytes per step = (2 x sweeps - 1)
+          x 2^30 x 16 B (the first sweep writes |0...0> without reading),
+          per launch their average over the step's sweeps
 
 Inputs are larger than L2 (16 GiB state vs 126 MB L2), so no flush is needed.
 With --gpus N (torchrun), each rank runs an independent replica (the path
@@ -376,7 +378,11 @@ def run_gpu(args, world, rank, local, ref_gpu=None):
     d2h = 16 + (n + 1) * 8
 
     hbm, hbm_kind = peaks()
-    bytes_per_launch = 2.0 * (1 << n) * 16
+    # algorithmic bytes: every sweep reads and writes the state once, except
+    # the first, which initialises |0...0> in the kernel and only writes
+    state_bytes = float(1 << n) * 16
+    bytes_per_step = (2.0 * st.sweeps - 1.0) * state_bytes
+    bytes_per_launch = bytes_per_step / st.sweeps  # average over the step's launches
     avg_launch_s = (ms_step / 1000.0) / st.sweeps
     achieved = bytes_per_launch / avg_launch_s / 1e9
     flops = st.flopsPerAmp * (1 << n)
@@ -438,7 +444,7 @@ def run_gpu(args, world, rank, local, ref_gpu=None):
                            "phases": st.phases, "gates_after_merge": st.gates,
                            "l2": "inputs larger than L2 (16 GiB state)", "parallelism": f"replicas x{world}"},
                 "gate_layers_per_s": depth / (ms_step / 1000.0),
-                "hbm_gbs_step": bytes_per_launch * st.sweeps / (ms_step / 1000.0) / 1e9,
+                "hbm_gbs_step": bytes_per_step / (ms_step / 1000.0) / 1e9,
                 "fp64_tflops_algorithmic": flops / (ms_step / 1000.0) / 1e12,
                 "norm_error": abs(norm - 1.0),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -450,7 +456,7 @@ def run_gpu(args, world, rank, local, ref_gpu=None):
                                   "peak_tflops": fp64_peak, "frac": flops / (ms_step / 1000.0) / 1e12 / fp64_peak,
                                   "peak_source": "measured live (DFMA loop, dgq_measureFp64Peak)",
                                   "circuit_floor_ms": max(flops / (fp64_peak * 1e12),
-                                                          st.sweeps * bytes_per_launch / (hbm * 1e9)) * 1e3},
+                                                          bytes_per_step / (hbm * 1e9)) * 1e3},
                 "e2e": {"value": world / e2e_t, "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t * 1000.0,
                         "record_ms": float(np.mean(record_times)) * 1000.0,
