@@ -559,6 +559,8 @@ void loadAmps(QuregState &s, const double *reals, const double *imags, const cha
     const uint64_t total = 1ULL << s.numBits;
     if (s.hostTier || s.sharded) {
         if (s.hostTier) cudaOk(dgq::hostTierSync(s, func) ? cudaSuccess : cudaErrorUnknown, func);
+        // every page is written below: none is all-zero any more
+        if (s.hostTier) s.pageZero.assign(s.pageZero.size(), 0);
         // shards: the amplitudes in storage type on the host, then one copy per shard
         std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
         void *dst = s.sharded ? (void *) staged.data() : s.hState;
@@ -626,7 +628,9 @@ void setAmps(Qureg qureg, long long int startInd, qreal *reals, qreal *imags, lo
     if (!normaliseLayout(s, __func__)) return;
     s.probsValid = false;
     if (s.hostTier || s.sharded) {
-        // shards: read, change and write back the whole state (virtual order)
+        // shards: read, change and write back the whole state (virtual order);
+        // host tier: all-zero pages get their zeros first
+        dgq::hostTierMaterialise(s);
         std::vector<char> staged(s.sharded ? ampBytes(s) << s.numBits : 0);
         if (s.sharded && !dgq::shardReadVirtual(s, 0, 1ULL << s.numBits, staged.data(), __func__)) return;
         void *dst = s.sharded ? (void *) staged.data() : s.hState;
@@ -686,6 +690,7 @@ void cloneQureg(Qureg targetQureg, Qureg copyQureg) {
     if (t.hostTier) {
         if (!dgq::hostTierSync(t, __func__)) return;
         std::memcpy(t.hState, c.hState, ampBytes(t) << t.numBits);
+        t.pageZero = c.pageZero;
     } else if (t.sharded) {
         if (!dgq::shardSync(t, __func__) || !dgq::shardCopy(t, c, __func__)) return;
     } else if (!cudaOk(cudaMemcpyAsync(t.dState, c.dState, ampBytes(t) << t.numBits, cudaMemcpyDeviceToDevice,

@@ -281,12 +281,24 @@ bool runShardPass(QuregState &s, const char *func) {
 
 // Runs s.planned on every page: copy in (unless the first sweep writes the
 // whole page), the plan's sweeps, copy out.
+// A page-local plan maps a page of zeros to zeros, so all-zero pages are
+// skipped (no copies, no kernels); an initialisation to a basis state leaves
+// every other page all-zero, and a blank one every page.
 bool runPagePass(QuregState &s, const char *func) {
     if (!planIsPageLocal(s, func)) return false;
     const uint64_t pages = 1ULL << (s.numBits - s.pageBits);
     const size_t pageBytes = ampBytesOf(s) << s.pageBits;
     const bool load = s.planned.empty() || s.planned[0].initKind == INIT_NONE;
+    const int32_t initKind = s.planned.empty() ? INIT_NONE : s.planned[0].initKind;
+    const uint64_t initPage = s.planned.empty() ? 0 : s.planned[0].initIndex >> s.pageBits;
+    s.pageZero.resize(pages, 0);
     for (uint64_t page = 0; page < pages; page++) {
+        if (load && s.pageZero[page]) continue;
+        if ((initKind == INIT_CLASSICAL && page != initPage) || initKind == INIT_BLANK) {
+            s.pageZero[page] = 1;
+            continue;
+        }
+        if (!load) s.pageZero[page] = 0;
         const int b = (int) (page % QuregState::kPageBufs);
         cudaStream_t st = s.pageStream[b];
         if (load && !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, page), pageBytes, cudaMemcpyHostToDevice, st), func))
@@ -309,21 +321,32 @@ bool runSwapPass(QuregState &s, int h, int l, bool thenPlan, const char *func) {
     const uint64_t hb = 1ULL << (h - s.pageBits);
     const size_t pageBytes = ampBytesOf(s) << s.pageBits;
     int pair = 0;
+    s.pageZero.resize(pages, 0);
     for (uint64_t p0 = 0; p0 < pages; p0++) {
         if (p0 & hb) continue;
         const uint64_t p1 = p0 | hb;
+        // two all-zero pages stay all-zero (exchange and segment alike)
+        if (s.pageZero[p0] && s.pageZero[p1]) continue;
         const int a = 2 * (pair % (QuregState::kPageBufs / 2)), b = a + 1;
         cudaStream_t st = s.pageStream[a];
-        if (!ok(cudaMemcpyAsync(s.dPage[a], hostPage(s, p0), pageBytes, cudaMemcpyHostToDevice, st), func) ||
-            !ok(cudaMemcpyAsync(s.dPage[b], hostPage(s, p1), pageBytes, cudaMemcpyHostToDevice, st), func) ||
-            !ok(launchPageSwap(s.dPage[a], s.dPage[b], s.single, s.pageBits, l, st), func))
+        // an all-zero page is cleared on the device instead of copied in
+        auto bringIn = [&](uint64_t pg, int buf) {
+            return s.pageZero[pg] ? ok(cudaMemsetAsync(s.dPage[buf], 0, pageBytes, st), func)
+                                  : ok(cudaMemcpyAsync(s.dPage[buf], hostPage(s, pg), pageBytes,
+                                                       cudaMemcpyHostToDevice, st),
+                                       func);
+        };
+        const int loaded = (s.pageZero[p0] ? 0 : 1) + (s.pageZero[p1] ? 0 : 1);
+        if (!bringIn(p0, a) || !bringIn(p1, b) || !ok(launchPageSwap(s.dPage[a], s.dPage[b], s.single, s.pageBits, l, st), func))
             return false;
+        s.pageZero[p0] = 0;
+        s.pageZero[p1] = 0;
         if (thenPlan && (!launchPlanOnPage(s, p0, a, st, func) || !launchPlanOnPage(s, p1, b, st, func)))
             return false;
         if (!ok(cudaMemcpyAsync(hostPage(s, p0), s.dPage[a], pageBytes, cudaMemcpyDeviceToHost, st), func) ||
             !ok(cudaMemcpyAsync(hostPage(s, p1), s.dPage[b], pageBytes, cudaMemcpyDeviceToHost, st), func))
             return false;
-        s.hostTierBytes += 4 * pageBytes;
+        s.hostTierBytes += (2 + loaded) * pageBytes;
         pair++;
     }
     if (!hostTierSync(s, func)) return false;
@@ -402,6 +425,22 @@ bool runShardExchange(QuregState &s, const std::vector<std::pair<int, int>> &swa
 
 }  // namespace
 
+void hostTierMaterialise(QuregState &s) {
+    if (!s.hostTier || s.sharded) return;
+    const size_t pageBytes = ampBytesOf(s) << s.pageBits;
+    for (size_t page = 0; page < s.pageZero.size(); page++)
+        if (s.pageZero[page]) {
+            std::memset(hostPage(s, page), 0, pageBytes);
+            s.pageZero[page] = 0;
+        }
+}
+
+bool hostTierPageZero(const QuregState &s, uint64_t index) {
+    if (!s.hostTier || s.sharded) return false;
+    const uint64_t page = index >> s.pageBits;
+    return page < s.pageZero.size() && s.pageZero[page];
+}
+
 bool hostTierSync(QuregState &s, const char *func) {
     for (int b = 0; b < QuregState::kPageBufs; b++)
         if (s.pageStream[b] && !ok(cudaStreamSynchronize(s.pageStream[b]), func)) return false;
@@ -421,6 +460,7 @@ bool hostTierAttach(QuregState &s, size_t budgetBytes, std::string &err) {
         return false;
     }
     s.pageBits = p;
+    s.pageZero.assign((size_t) 1 << (s.numBits - p), 0);
     if (cudaHostAlloc(&s.hState, ab << s.numBits, cudaHostAllocDefault) != cudaSuccess) {
         s.hState = nullptr;
         err = "pinned host memory for the state is not available";
@@ -453,6 +493,7 @@ void hostTierRelease(QuregState &s) {
     }
     if (s.hState) cudaFreeHost(s.hState);
     s.hState = nullptr;
+    s.pageZero.clear();
     s.hostTier = false;
 }
 
@@ -550,8 +591,10 @@ bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const 
     std::vector<double> sums(pages * (size_t) (nf + 1), 0.0);
     std::vector<char> used(pages, 0);
     for (uint64_t page = 0; page < pages; page++) {
-        // pages outside a collapse on page-index bits hold no probability
+        // pages outside a collapse on page-index bits hold no probability,
+        // and neither do all-zero pages
         if (((page << p) & rMask & ~localMask) != (rValue & ~localMask)) continue;
+        if (!s.sharded && page < s.pageZero.size() && s.pageZero[page]) continue;
         used[page] = 1;
         double *sum = &sums[page * (size_t) (nf + 1)];
         const size_t sumBytes = sizeof(double) * (size_t) (nf + 1);

@@ -78,6 +78,11 @@ struct QuregState {
     // brought into the page by a page-pair exchange of two address bits
     bool hostTier = false;
     void *hState = nullptr;
+    // pageZero[p] = 1: page p holds only zeros and its host memory is stale
+    // (never read: passes skip it or clear its device buffer, read-outs see
+    // zeros); the counterpart of dgQuEST's all-zero pages (OPTIMIZE_ZERO,
+    // src/cpp/QuEST_backend_distributed.cpp:17,343-347)
+    std::vector<uint8_t> pageZero;
     int pageBits = 0;
     static constexpr int kPageBufs = 4;
     void *dPage[kPageBufs] = {};
@@ -138,6 +143,11 @@ bool hostTierAttach(QuregState &s, size_t budgetBytes, std::string &err);
 void hostTierRelease(QuregState &s);
 bool hostTierFlush(QuregState &s, const char *func);
 bool hostTierProbs(QuregState &s, std::vector<double> &p0, double &total, const char *func);
+// Writes zeros into the host memory of the all-zero pages (before the host
+// copy of the state is read or written as a whole) and clears their flags.
+void hostTierMaterialise(QuregState &s);
+// Whether the amplitude at virtual index `index` lies in an all-zero page.
+bool hostTierPageZero(const QuregState &s, uint64_t index);
 bool hostTierSync(QuregState &s, const char *func);
 
 // sharded registers (host_tier.cpp). attach: 2^shardBits shards on the

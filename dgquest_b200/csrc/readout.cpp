@@ -152,8 +152,10 @@ static Complex ampAt(QuregState &s, uint64_t index, const char *func) {
             return out;
         }
     } else if (s.hostTier) {
-        // the flushed state is in pinned host memory
-        if (s.single) {
+        // the flushed state is in pinned host memory (an all-zero page is not read)
+        if (dgq::hostTierPageZero(s, v)) {
+            a = make_double2(0.0, 0.0);
+        } else if (s.single) {
             const float2 f = reinterpret_cast<const float2 *>(s.hState)[v];
             a = make_double2(f.x, f.y);
         } else {
@@ -288,7 +290,7 @@ static bool readLogical(QuregState &s, double *re, double *im, const char *func)
             } else {
                 a = reinterpret_cast<const double2 *>(src)[v];
             }
-            const bool keep = !s.restrictActive || (v & s.rMask) == s.rValue;
+            const bool keep = (!s.restrictActive || (v & s.rMask) == s.rValue) && !dgq::hostTierPageZero(s, v);
             re[i] = keep ? a.x * sc : 0.0;
             im[i] = keep ? a.y * sc : 0.0;
         }

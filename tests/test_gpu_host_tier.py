@@ -161,3 +161,43 @@ def test_host_tier_collapse_before_exchange(quest, env, small_budget):
     ref, _, ref_out = oracle.run(n, ops, seed_keys=[3, 4])
     assert out == ref_out
     assert np.abs(amps - ref).max() <= 1e-12
+
+
+def test_host_tier_skips_all_zero_pages(quest, env, small_budget):
+    """After initZeroState only page 0 holds amplitudes; gates inside the
+    page keep the other pages all-zero, so the pass moves page 0 alone, an
+    exchange brings in only the non-zero page of each pair, and the
+    read-outs see zeros in the pages never written (dgQuEST's all-zero
+    pages, OPTIMIZE_ZERO). Amplitudes within 1e-12 of the oracle."""
+    n, page = 18, 14
+    b = C.OpList()
+    for k in range(page):
+        b.add(C.H, k)
+    b.add(C.CNOT, 0, 5).add(C.RY, 3, p=[0.3])
+    ops1 = b.array()
+    ops2 = C.OpList().add(C.H, n - 1).add(C.CNOT, n - 1, 2).array()  # one exchange, then more gates
+    q = quest.createQureg(n, env)
+    try:
+        pb, _, _, _ = quest.host_tier_stats(q)
+        assert pb == page
+        page_bytes = 16 << page
+        quest.initZeroState(q)
+        C.replay(q, ops1)
+        quest.getAmp(q, 0)  # runs the first pass
+        _, _, _, moved1 = quest.host_tier_stats(q)
+        assert moved1 == page_bytes  # page 0 copied out; the other 15 pages skipped
+        a_far = quest.getAmp(q, (1 << n) - 1)
+        assert a_far.real == 0.0 and a_far.imag == 0.0
+        C.replay(q, ops2)
+        amps = quest.state_vector(q)
+        p0 = quest.prob_all_zero(q)
+        _, _, exchanges, moved2 = quest.host_tier_stats(q)
+    finally:
+        quest.destroyQureg(q, env)
+    assert exchanges >= 1
+    # the exchange brought in one non-zero page per non-zero pair, not every page
+    assert moved2 - moved1 < 2 * (16 << n)
+    ops = np.concatenate([ops1, ops2])
+    ref, ref_p0, _ = oracle.run(n, ops)
+    assert np.abs(amps - ref).max() <= 1e-12
+    assert np.abs(p0 - ref_p0).max() <= 1e-12
