@@ -637,8 +637,10 @@ def run_sharded_form(args, world):
 
 def run_dense_form(args, world):
     """Dense 6-qubit blocks: multiQubitUnitary with 6 targets on a 30-qubit
-    register, complex64 on the tensor cores (tcgen05, 3xTF32) and on the SIMT
-    dense kernel, complex128 on the SIMT dense kernel. Time per dense sweep."""
+    register, complex64 on the tensor cores (tcgen05, split FP16) and on the
+    SIMT dense kernel, complex128 on the SIMT dense kernel. Time per dense
+    sweep (the plan's time over its blocks), and for the tensor cores the
+    time of one block alone (5 and 6 targets) from plans of 4 and 8 blocks."""
     import torch
 
     from dgquest_b200 import circuits as C
@@ -686,6 +688,37 @@ def run_dense_form(args, world):
                      "hbm_gbs": 2.0 * (1 << n) * amp / (per / 1e3) / 1e9,
                      "device_errors": Q.dgq_getDeviceErrors()}
         states[name] = q
+    # one tensor-core block alone: plans of 4 and of 8 blocks differ by 4
+    # blocks (the initialisation and renormalisation passes cancel)
+    hbm = peaks()[0]
+    marginal = {}
+    for K in (5, 6):
+        t_plan = []
+        for reps in (1, 2):
+            q = Q.dgq_createQuregF32(n, env)
+            Q.initPlusState(q)
+            g2 = np.random.default_rng(11)
+            for _ in range(reps):
+                for t, _u in blocks:
+                    m = Q.matrixN(C.random_unitary(g2, 1 << K))
+                    Q.multiQubitUnitary(q, Q.int_array(t[:K]), K, m)
+                    Q.destroyComplexMatrixN(m)
+            Q.dgq_planPending(q)
+            stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
+            Q.dgq_launchPlanned(q)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(3):
+                Q.dgq_launchPlanned(q)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_plan.append(e0.elapsed_time(e1) / 3)
+            Q.destroyQureg(q, env)
+        per = (t_plan[1] - t_plan[0]) / len(blocks)
+        marginal[f"k{K}"] = {"ms_per_block": per, "hbm_frac": 2.0 * (1 << n) * 8 / (per / 1e3) / 1e9 / hbm}
+    out["complex64_tensor_cores"]["marginal_per_block"] = marginal
     out["fidelity_tc_vs_complex128"] = Q.calcFidelity(states["complex128_simt"], states["complex64_tensor_cores"])
     out["fidelity_simt_complex64_vs_complex128"] = Q.calcFidelity(states["complex128_simt"],
                                                                   states["complex64_simt"])
