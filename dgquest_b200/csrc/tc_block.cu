@@ -208,6 +208,10 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     tcBlockKernel(float2 *__restrict__ st, const __grid_constant__ TbArgs a, const uint4 *__restrict__ Wpacked,
                   uint32_t *__restrict__ error) {
     typedef TbShape<K> S;
+    // when the lowest targets are address bits 0 and 1, each column is one
+    // run in memory: the consumers stage the tile in its X buffer and write
+    // whole columns per warp instruction (X is then released by them)
+    constexpr bool STAGE = VA == 4;
     constexpr int P = S::D / kTbQuarters;  // amplitudes a producer thread holds per tile
     constexpr int PB = K - 2;              // their pattern bits (the low bits of s)
     extern __shared__ __align__(1024) unsigned char smRaw[];
@@ -233,7 +237,9 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         for (int b = 0; b < 2; b++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barXFull + 8 * b), "r"(kTbProducers)
                          : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barXEmpty + 8 * b) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barXEmpty + 8 * b),
+                         "r"(STAGE ? 32u * kTbConsumerWarps : 1u)
+                         : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barDFull + 8 * b) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barDEmpty + 8 * b), "r"(32 * kTbConsumerWarps)
                          : "memory");
@@ -377,12 +383,44 @@ __global__ void __launch_bounds__(kTbThreads, 1)
                                        (__uint_as_float(r0[2 * q + 1]) + __uint_as_float(r1[2 * q + 1])) * inv);
                     if (a.normOut) norm += (double) (y[q].x * y[q].x + y[q].y * y[q].y);
                 }
+                if constexpr (STAGE) {
+                    // into the tile's X buffer (its MMAs are complete), column m
+                    // at m D amplitudes, 16-byte chunks rotated by m against
+                    // bank conflicts
+                    float4 *col = reinterpret_cast<float4 *>(X + (i & 1u) * 2 * S::XBytes) + m * (S::D / 2);
 #pragma unroll
-                for (int q = 0; q < 8; q += VA) tbStoreRun<VA>(st + (tb | tbPattern<K>((uint32_t) (8 * c + q), tBit)), y + q);
+                    for (int q = 0; q < 4; q++)
+                        col[((uint32_t) (4 * c + q)) ^ (m & (S::D / 2 - 1u))] =
+                            make_float4(y[2 * q].x, y[2 * q].y, y[2 * q + 1].x, y[2 * q + 1].y);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 8; q += VA)
+                        tbStoreRun<VA>(st + (tb | tbPattern<K>((uint32_t) (8 * c + q), tBit)), y + q);
+                }
             }
             // every value of the accumulator is read: hand the buffer back
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             tbArrive(barDEmpty + 8 * d);
+            if constexpr (STAGE) {
+                // each warp writes 16 whole columns back, a column's adjacent
+                // amplitude pairs on adjacent lanes (one contiguous run per
+                // column when the targets are the lowest address bits)
+                asm volatile("bar.sync 2, %0;" ::"r"(32 * kTbConsumerWarps) : "memory");
+                const float4 *stage = reinterpret_cast<const float4 *>(X + (i & 1u) * 2 * S::XBytes);
+                constexpr uint32_t CPI = 64u / S::D;  // columns per warp instruction (32 lanes x 2 amplitudes)
+                const uint32_t wq = warp - kTbProducerWarps;
+                const uint64_t tbase0 = tileBase(blockIdx.x + i * gridDim.x);
+#pragma unroll 1
+                for (uint32_t k = 0; k < kTbCols / kTbConsumerWarps; k += CPI) {
+                    const uint32_t mc = wq * (kTbCols / kTbConsumerWarps) + k + lane / (S::D / 2);
+                    const uint32_t ch = lane % (S::D / 2);
+                    uint64_t ca = 0;
+                    for (int q = 0; q < kTbColBits; q++) ca |= (uint64_t) ((mc >> q) & 1u) << a.colPos[q];
+                    const float4 v = stage[mc * (S::D / 2) + (ch ^ (mc & (S::D / 2 - 1u)))];
+                    *reinterpret_cast<float4 *>(st + (tbase0 | ca | tbPattern<K>(2u * ch, tBit))) = v;
+                }
+                tbArrive(barXEmpty + 8 * (i & 1u));
+            }
         }
         if (a.normOut) {
 #pragma unroll
@@ -413,7 +451,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
             for (int ks = 0; ks < S::KR / 16; ks++)
                 tbMma(acc, tbDesc(xl + (uint32_t) ks * 2 * lboX, lboX, 128), tbDesc(wAddr + (uint32_t) ks * 2 * lboW, lboW, 128),
                       tbIdesc(S::KR), 1u);
-            tbCommit(barXEmpty + 8 * b);
+            if (!STAGE) tbCommit(barXEmpty + 8 * b);  // staged: the consumers release X
             tbCommit(barDFull + 8 * d);
         }
         // every MMA issued here has completed before tensor memory is released

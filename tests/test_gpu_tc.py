@@ -27,7 +27,8 @@ def run(Q, env, n, targs, u, pre, post):
 @pytest.mark.parametrize("n,targs", [(12, [0, 1, 2, 3, 4, 5]), (12, [11, 3, 7, 0, 9, 5]), (16, [15, 2, 9, 4, 12, 0]),
                                      (20, [6, 19, 1, 13, 8, 3]), (13, [12, 6, 7, 8, 9, 10]),
                                      (14, [0, 1, 2, 3, 4, 5]), (12, [3, 11, 0, 6, 9]), (17, [16, 8, 1, 4, 12]),
-                                     (21, [20, 19, 18, 17, 16])])
+                                     (21, [20, 19, 18, 17, 16]), (13, [0, 1, 2, 7, 12]),
+                                     (16, [1, 0, 9, 12, 4, 15])])
 def test_tensor_core_dense(quest, env, n, targs):
     Q = quest
     u = C.random_unitary(np.random.default_rng(n + targs[0]), 1 << len(targs))
