@@ -831,14 +831,14 @@ def l2_read_gbs():
     x = torch.ones(12 << 20, dtype=torch.float32, device="cuda")
     out = torch.empty((), dtype=torch.float32, device="cuda")
     for _ in range(3):
-        torch.sum(x, out=out)
+        torch.sum(x, dim=0, out=out)
     best = 0.0
     for _ in range(5):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(100):
-            torch.sum(x, out=out)
+            torch.sum(x, dim=0, out=out)
         e1.record()
         torch.cuda.synchronize()
         best = max(best, 4.0 * x.numel() * 100 / (e0.elapsed_time(e1) / 1e3) / 1e9)
