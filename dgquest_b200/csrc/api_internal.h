@@ -144,6 +144,7 @@ double predictPlanSeconds(const std::vector<Gate> &gates, int numBits, int W, co
 int chooseTileBits(QuregState &s);
 double predictDenseSeconds(const QuregState &s, int K, int *blocksOut, double bound, bool *stopped);
 int chooseForm(QuregState &s);
+int chooseFormUncached(QuregState &s, const CostModel &cm);
 extern std::atomic<int> g_jitMinBits;
 bool pairedEnabled();
 int pairedTileBits(const QuregState &s);
