@@ -124,3 +124,19 @@ def test_dense_rates_from_a_cost_file(tmp_path, restore_rates, restore_dense):
         Q.dgq_setDenseCost(3, 6, 1.0)
     with pytest.raises(Q.QuESTError):
         Q.dgq_setDenseCost(0, 8, 1.0)
+
+
+def test_form_choice_is_kept_per_structure(restore_rates, restore_dense):
+    # a second plan of the same gate structure (other angles) reuses the
+    # choice: same width, form and predictions
+    n = 26
+    a = ir.plan(C.random_layers(n, 10, C.config_seed(2, 715)), n, 0)
+    ops = C.random_layers(n, 10, C.config_seed(2, 715)).copy()
+    ops["p"][:, 0] += 0.125  # same structure, other angles
+    b = ir.plan(ops, n, 0)
+    assert (a.tileBits, a.sweeps, a.formK) == (b.tileBits, b.sweeps, b.formK)
+    assert a.predictedTileMs == b.predictedTileMs
+    # a different cost model is a different key: the choice is made again
+    Q.dgq_setCostModel(100.0, 0.01)
+    c = ir.plan(ops, n, 0)
+    assert c.predictedTileMs != b.predictedTileMs
