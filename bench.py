@@ -219,19 +219,21 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args):
+def run_reference_gpu(args, n=None, ops=None):
     """dgQuEST's own GPU path, built from the reference's sources for sm_100a
     (oracle/_ref/ref_harness, `make -C oracle ref`), on the same circuit and
-    GPU: its QuEST calls, searchQuregTaskPartitions and getAmp(q, 0) with
-    K = 5 (QuEST.conf "5 5 5"), timed by the harness around getAmp. Also
-    reads 64 sampled amplitudes for a comparison with this library's."""
+    GPU (by default the 30-qubit depth-20 random circuit): its QuEST calls,
+    searchQuregTaskPartitions and getAmp(q, 0) with K = 5 (QuEST.conf
+    "5 5 5"), timed by the harness around getAmp. Also reads 64 sampled
+    amplitudes for a comparison with this library's."""
     import tempfile
     from dgquest_b200 import circuits as C
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if not os.path.exists(harness):
         return {"unavailable": "oracle/_ref/ref_harness not built (make -C oracle ref needs the reference sources)"}
-    n = N_QUBITS
-    ops = C.random_layers(n, DEPTH, C.config_seed(2))
+    if n is None:
+        n = N_QUBITS
+        ops = C.random_layers(n, DEPTH, C.config_seed(2))
     idx = np.unique(np.random.RandomState(11).randint(0, 1 << n, size=64).astype(np.int64))
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "QuEST.conf"), "w") as f:
@@ -741,6 +743,9 @@ def run_precision_form(args, world):
     from dgquest_b200 import quest as Q
     n, depth = 32, 16
     ops = C.grid_sqrt(4, 8, depth, C.config_seed(3))
+    # dgQuEST's own GPU path on the same circuit first (its process needs the
+    # 64 GiB of a complex128 state while this one holds none)
+    ref = run_reference_gpu(args, n, ops) if not args.no_ref_gpu and world == 1 else None
     env = Q.createQuESTEnv()
     out = {"workload": "4x8 grid, depth 16, sqrt-X/Y/W + CZ patterns, 32 qubits", "qubits": n, "depth": depth}
     regs = {}
@@ -778,6 +783,17 @@ def run_precision_form(args, world):
         err = max(err, abs(complex(a.real, a.imag) - complex(b.real, b.imag)))
     out["max_abs_err_sampled"] = err
     out["amplitudes_sampled"] = len(idx)
+    if ref is not None and "sample_amps" in ref:
+        # both precisions against the reference's own amplitudes
+        ridx = ref.pop("sample_indices")
+        ramps = ref.pop("sample_amps")
+        for name in ("complex128", "complex64"):
+            amps = [Q.getAmp(regs[name], int(i)) for i in ridx]
+            ours = np.array([complex(a.real, a.imag) for a in amps])
+            ref[f"max_abs_err_{name}_vs_reference"] = float(np.abs(ours - ramps).max())
+        ref["amplitudes_compared"] = len(ridx)
+    if ref is not None:
+        out["reference_gpu"] = ref
     out["speedup_complex64"] = out["complex128"]["ms_per_circuit"] / out["complex64"]["ms_per_circuit"]
     out["arithmetic"] = "complex64 paired form (packed FP32 SIMT register phases)"
     for name in ("complex128", "complex64"):
@@ -785,7 +801,7 @@ def run_precision_form(args, world):
         out[name]["form_choice"] = form_report(st_, {"tiles": out[name]["ms_per_circuit"]})
     Q.destroyQureg(q32, env)
     if not args.no_tc_blocks:
-        # the same circuit fused into dense 6-qubit blocks, each a 3xTF32 GEMM
+        # the same circuit fused into dense 6-qubit blocks, each a split-FP16 GEMM
         # on the tensor cores (one warm-up and one timed run: seconds each)
         q = Q.dgq_createQuregF32(n, env)
         Q.dgq_setDenseFusion(q, 6)
