@@ -292,12 +292,307 @@ std::string selExpr(const KOp &op) {
     return any ? sel.str() : std::string("false");
 }
 
-void emitOpPaired(std::ostringstream &o, const KOp &op) {
+// Compile-time signs of the paired form. Bit j of negR (negI) is set when
+// slot j's stored real (imaginary) pair holds the negated values. The
+// negations inside gates (CZ and the other sign flips, the -1 entries of
+// the factored Rx / Ry / H forms, the component swaps of Y and of the
+// factors +-i) become changes of these masks or the choice of a
+// coefficient's sign, so no instruction carries them. Round-to-nearest is
+// symmetric, so every stored value equals the untracked computation's up
+// to its sign. A phase's closing factor absorbs the masks (or sign flips
+// on the integer pipe restore the values, when the phase has none), so
+// values leave the registers with their true signs.
+struct PairedSigns {
+    uint32_t negR = 0, negI = 0;
+    // component c of the pair (j0, j1): 0 R[j0], 1 I[j0], 2 R[j1], 3 I[j1]
+    int sign(int c, int j0, int j1) const {
+        const int j = c < 2 ? j0 : j1;
+        const uint32_t m = (c & 1) ? negI : negR;
+        return ((m >> j) & 1u) ? -1 : 1;
+    }
+    void set(int c, int j0, int j1, int s) {
+        const int j = c < 2 ? j0 : j1;
+        uint32_t &m = (c & 1) ? negI : negR;
+        m = s < 0 ? (m | (1u << j)) : (m & ~(1u << j));
+    }
+};
+
+const char *const kPairIn[4] = {"x0_", "x1_", "x2_", "x3_"};
+
+void flushSigns(std::ostringstream &o, PairedSigns &sg) {
+    for (int j = 0; j < kRegs; j++) {
+        if ((sg.negR >> j) & 1u) o << "    R[" << j << "] = dgq::flip2(R[" << j << "]);\n";
+        if ((sg.negI >> j) & 1u) o << "    I[" << j << "] = dgq::flip2(I[" << j << "]);\n";
+    }
+    sg.negR = sg.negI = 0;
+}
+
+std::string pairDest(int c, int j0, int j1) {
+    return std::string((c & 1) ? "I[" : "R[") + std::to_string(c < 2 ? j0 : j1) + "]";
+}
+
+template <class F>
+void forPairsHost(int K, uint32_t cr, F f) {
+    for (int p = 0; p < kRegs / 2; p++) {
+        const int j0 = ((p >> K) << (K + 1)) | (p & ((1 << K) - 1));
+        const int j1 = j0 | (1 << K);
+        if ((j0 & (int) cr) != (int) cr) continue;
+        f(j0, j1);
+    }
+}
+
+// Output c of a factored pair gate, in true values: u * in[b] + k * coef * in[a]
+// (u, k = +-1; coef is the op's coefficient, or 1 for H).
+struct LinearOut {
+    int b, u, a, k;
+};
+
+// Emits a factored pair gate on every pair of register bit K; cp_ / cn_
+// (+-coefficient) and m1_ (-1) are in scope. Output c is stored as
+// fma2(+-coef, in[a], in[b]) with the sign of u * (sign of in[b]): no
+// negation is computed.
+void emitLinearPairs(std::ostringstream &o, PairedSigns &sg, int K, const LinearOut (&outs)[4], bool unit) {
+    forPairsHost(K, 0u, [&](int j0, int j1) {
+        o << "    { const float2 x0_ = R[" << j0 << "], x1_ = I[" << j0 << "], x2_ = R[" << j1 << "], x3_ = I[" << j1
+          << "];";
+        int ns[4];
+        for (int c = 0; c < 4; c++) {
+            const LinearOut &L = outs[c];
+            const int sB = sg.sign(L.b, j0, j1), sA = sg.sign(L.a, j0, j1);
+            ns[c] = L.u * sB;
+            const int coefSign = L.k * sA * L.u * sB;
+            o << " " << pairDest(c, j0, j1) << " = ";
+            if (unit)
+                o << (coefSign > 0 ? "dgq::add2(" + std::string(kPairIn[L.b]) + ", " + kPairIn[L.a] + ")"
+                                   : "dgq::fma2(m1_, " + std::string(kPairIn[L.a]) + ", " + kPairIn[L.b] + ")");
+            else
+                o << "dgq::fma2(" << (coefSign > 0 ? "cp_" : "cn_") << ", " << kPairIn[L.a] << ", " << kPairIn[L.b] << ")";
+            o << ";";
+        }
+        for (int c = 0; c < 4; c++) sg.set(c, j0, j1, ns[c]);
+        o << " }\n";
+    });
+}
+
+// Output c of a pair permutation (X, Y, Y*), in true values: m * in[src].
+struct PermOut {
+    int src, m;
+};
+
+// keep = true (the op runs under a condition known only at run time): the
+// outputs keep their slots' signs, with a flip where the two differ.
+void emitPermPairs(std::ostringstream &o, PairedSigns &sg, int K, uint32_t cr, const PermOut (&outs)[4], bool keep) {
+    forPairsHost(K, cr, [&](int j0, int j1) {
+        o << "    { const float2 x0_ = R[" << j0 << "], x1_ = I[" << j0 << "], x2_ = R[" << j1 << "], x3_ = I[" << j1
+          << "];";
+        int ns[4];
+        for (int c = 0; c < 4; c++) {
+            const int trueSign = outs[c].m * sg.sign(outs[c].src, j0, j1);
+            const std::string src = kPairIn[outs[c].src];
+            if (keep) {
+                const bool flip = trueSign * sg.sign(c, j0, j1) < 0;
+                o << " " << pairDest(c, j0, j1) << " = " << (flip ? "dgq::flip2(" + src + ")" : src) << ";";
+                ns[c] = sg.sign(c, j0, j1);
+            } else {
+                o << " " << pairDest(c, j0, j1) << " = " << src << ";";
+                ns[c] = trueSign;
+            }
+        }
+        for (int c = 0; c < 4; c++) sg.set(c, j0, j1, ns[c]);
+        o << " }\n";
+    });
+}
+
+// Slot j times (c + i s), keeping the slot's signs; c / s / ns are float2
+// expressions in scope (ns = -s).
+void emitPhaseSlot(std::ostringstream &o, const PairedSigns &sg, int j, const std::string &c, const std::string &s,
+                   const std::string &ns) {
+    const bool differ = (((sg.negR ^ sg.negI) >> j) & 1u) != 0;
+    const std::string &k1 = differ ? s : ns, &k2 = differ ? ns : s;
+    o << "    { const float2 r_ = R[" << j << "]; R[" << j << "] = dgq::fma2(" << c << ", r_, dgq::mul2(" << k1 << ", I["
+      << j << "])); I[" << j << "] = dgq::fma2(" << c << ", I[" << j << "], dgq::mul2(" << k2 << ", r_)); }\n";
+}
+
+// Every slot times (gr + i gi), absorbing the signs (the values leave with
+// their true signs); gr / gi are double expressions.
+void emitGlobalAbsorb(std::ostringstream &o, PairedSigns &sg, const std::string &gr, const std::string &gi) {
+    o << "    { const float2 c_ = dgq::b2((float) (" << gr << ")), nc_ = dgq::b2(-(float) (" << gr
+      << ")), s_ = dgq::b2((float) (" << gi << ")), ns_ = dgq::b2(-(float) (" << gi << "));\n";
+    for (int j = 0; j < kRegs; j++) {
+        const bool nR = (sg.negR >> j) & 1u, nI = (sg.negI >> j) & 1u;
+        o << "      { const float2 r_ = R[" << j << "]; R[" << j << "] = dgq::fma2(" << (nR ? "nc_" : "c_")
+          << ", r_, dgq::mul2(" << (nI ? "s_" : "ns_") << ", I[" << j << "])); I[" << j << "] = dgq::fma2("
+          << (nI ? "nc_" : "c_") << ", I[" << j << "], dgq::mul2(" << (nR ? "ns_" : "s_") << ", r_)); }\n";
+    }
+    o << "    }\n";
+    sg.negR = sg.negI = 0;
+}
+
+// The sign-aware form of an op, written to `body`; false when the op has
+// none (the caller flushes the signs and emits the plain form). keep: the
+// op runs under a run-time condition, so it must leave the signs as they
+// are (phases and flips do by construction).
+bool emitSignedPaired(std::ostringstream &body, const KOp &op, PairedSigns &sg, bool keep) {
+    const uint32_t cr = op.ctrlReg;
+    const int k = op.k, off = op.coef;
+    const std::string c0 = cf(off), c1 = cf(off + 1);
+    auto slotsOf = [&](uint32_t need, uint32_t sel, auto f) {
+        for (int j = 0; j < kRegs; j++) {
+            if ((j & (int) need) != (int) need) continue;
+            if (sel && (j & (int) sel) == 0) continue;
+            f(j);
+        }
+    };
+    auto phaseAll = [&](const std::string &cExpr, const std::string &sExpr, const std::string &nsExpr, uint32_t need,
+                        uint32_t sel) {
+        body << "    { const float2 pc_ = " << cExpr << ", ps_ = " << sExpr << ", pn_ = " << nsExpr << ";\n";
+        slotsOf(need, sel, [&](int j) { emitPhaseSlot(body, sg, j, "pc_", "ps_", "pn_"); });
+        body << "    }\n";
+    };
+    const bool slotKind = op.kind == KOP_NEG || op.kind == KOP_MULI || op.kind == KOP_MULNI || op.kind == KOP_PH ||
+                          op.kind == KOP_Z2 || op.kind == KOP_PH1;
+    if (k == 4 && !slotKind) return false;  // a gate inside the slot
+    switch (op.kind) {
+        case KOP_RY1:
+        case KOP_RY2:
+        case KOP_RX1:
+        case KOP_RX2:
+        case KOP_H1: {
+            if (keep) return false;
+            static const LinearOut ry1[4] = {{0, 1, 2, -1}, {1, 1, 3, -1}, {2, 1, 0, 1}, {3, 1, 1, 1}};
+            static const LinearOut ry2[4] = {{2, -1, 0, 1}, {3, -1, 1, 1}, {0, 1, 2, 1}, {1, 1, 3, 1}};
+            static const LinearOut rx1[4] = {{0, 1, 3, 1}, {1, 1, 2, -1}, {2, 1, 1, 1}, {3, 1, 0, -1}};
+            static const LinearOut rx2[4] = {{3, 1, 0, 1}, {2, -1, 1, 1}, {1, 1, 2, 1}, {0, -1, 3, 1}};
+            static const LinearOut h1[4] = {{0, 1, 2, 1}, {1, 1, 3, 1}, {0, 1, 2, -1}, {1, 1, 3, -1}};
+            const LinearOut(&t)[4] = op.kind == KOP_RY1   ? ry1
+                                     : op.kind == KOP_RY2 ? ry2
+                                     : op.kind == KOP_RX1 ? rx1
+                                     : op.kind == KOP_RX2 ? rx2
+                                                          : h1;
+            const bool unit = op.kind == KOP_H1;
+            body << "  {\n";
+            if (unit)
+                body << "    const float2 m1_ = dgq::b2(-1.0f);\n";
+            else
+                body << "    const float2 cp_ = dgq::b2(" << c0 << "), cn_ = dgq::b2(-" << c0 << ");\n";
+            emitLinearPairs(body, sg, k, t, unit);
+            body << "  }\n";
+            return true;
+        }
+        case KOP_X:
+        case KOP_Y:
+        case KOP_YC: {
+            static const PermOut px[4] = {{2, 1}, {3, 1}, {0, 1}, {1, 1}};
+            static const PermOut py[4] = {{3, 1}, {2, -1}, {1, -1}, {0, 1}};
+            static const PermOut pyc[4] = {{3, -1}, {2, 1}, {1, 1}, {0, -1}};
+            emitPermPairs(body, sg, k, cr, op.kind == KOP_X ? px : op.kind == KOP_Y ? py : pyc, keep);
+            return true;
+        }
+        case KOP_NEG:
+            if (keep) {
+                slotsOf(cr, 0u, [&](int j) {
+                    body << "    R[" << j << "] = dgq::flip2(R[" << j << "]); I[" << j << "] = dgq::flip2(I[" << j
+                         << "]);\n";
+                });
+            } else {
+                slotsOf(cr, 0u, [&](int j) {
+                    sg.negR ^= 1u << j;
+                    sg.negI ^= 1u << j;
+                });
+            }
+            return true;
+        case KOP_MULI:
+        case KOP_MULNI: {
+            // +i: (r, i) -> (-i, r); -i: (r, i) -> (i, -r)
+            const int mr = op.kind == KOP_MULI ? -1 : 1, mi = -mr;
+            slotsOf(cr, 0u, [&](int j) {
+                const int sR = ((sg.negR >> j) & 1u) ? -1 : 1, sI = ((sg.negI >> j) & 1u) ? -1 : 1;
+                const int tR = mr * sI, tI = mi * sR;  // signs of the swapped stored values
+                const std::string js = std::to_string(j);
+                if (keep) {
+                    body << "    { const float2 r_ = R[" << js << "]; R[" << js << "] = "
+                         << (tR * sR < 0 ? "dgq::flip2(I[" + js + "])" : "I[" + js + "]") << "; I[" << js
+                         << "] = " << (tI * sI < 0 ? "dgq::flip2(r_)" : "r_") << "; }\n";
+                } else {
+                    body << "    { const float2 r_ = R[" << js << "]; R[" << js << "] = I[" << js << "]; I[" << js
+                         << "] = r_; }\n";
+                    sg.negR = tR < 0 ? (sg.negR | (1u << j)) : (sg.negR & ~(1u << j));
+                    sg.negI = tI < 0 ? (sg.negI | (1u << j)) : (sg.negI & ~(1u << j));
+                }
+            });
+            return true;
+        }
+        case KOP_PH:
+            phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", cr, 0u);
+            return true;
+        case KOP_Z2:
+            if (op.code < KC_Z2T) {
+                // (c + i s) where register bit k is 1, (c - i s) where it is 0
+                body << "    { const float2 pc_ = dgq::b2(" << c0 << "), ps_ = dgq::b2(" << c1 << "), pn_ = dgq::b2(-"
+                     << c1 << ");\n";
+                slotsOf(cr, 0u, [&](int j) {
+                    if ((j >> k) & 1)
+                        emitPhaseSlot(body, sg, j, "pc_", "ps_", "pn_");
+                    else
+                        emitPhaseSlot(body, sg, j, "pc_", "pn_", "ps_");
+                });
+                body << "    }\n";
+            } else if (op.selLoc == 1u) {
+                phaseAll("dgq::b2(" + c0 + ")", "make_float2(-" + c1 + ", " + c1 + ")",
+                         "make_float2(" + c1 + ", -" + c1 + ")", cr, 0u);
+            } else {
+                body << "    { const bool b_ = " << selExpr(op) << ";\n";
+                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(b_ ? " + c1 + " : -" + c1 + ")",
+                         "dgq::b2(b_ ? -" + c1 + " : " + c1 + ")", cr, 0u);
+                body << "    }\n";
+            }
+            return true;
+        case KOP_PH1:
+            if (op.code < KC_PH1T) {
+                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", 0u, 1u << k);
+            } else if (op.selLoc == 1u) {
+                phaseAll("make_float2(1.0f, " + c0 + ")", "make_float2(0.0f, " + c1 + ")",
+                         "make_float2(-0.0f, -" + c1 + ")", 0u, 0u);
+            } else {
+                body << "    if (" << selExpr(op) << ") {\n";
+                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", 0u, 0u);
+                body << "    }\n";
+            }
+            return true;
+        default:
+            return false;
+    }
+}
+
+void emitOpPaired(std::ostringstream &o, const KOp &op, PairedSigns &sg) {
     const unsigned cr = op.ctrlReg;
     const bool ctrl = cr != 0;
     const bool hi = (op.ctrlLoc & 1u) != 0;  // controlled on address bit 0
     const int off = op.coef;
     const int k = op.k;
+    const unsigned clr = op.ctrlLoc & ~1u;
+    const bool runtimeCond = clr || op.ctrlCta;
+    if (!hi) {
+        std::ostringstream sbody;
+        PairedSigns trial = sg;
+        if (emitSignedPaired(sbody, op, trial, runtimeCond)) {
+            sg = trial;
+            if (runtimeCond) {
+                std::ostringstream cond;
+                bool any = false;
+                if (clr) {
+                    cond << "((loc & " << clr << "u) == " << clr << "u)";
+                    any = true;
+                }
+                if (op.ctrlCta) cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+                o << "    if (" << cond.str() << ") {\n" << sbody.str() << "    }\n";
+            } else {
+                o << sbody.str();
+            }
+            return;
+        }
+    }
+    flushSigns(o, sg);
     const std::string tpl3 = std::string(ctrl ? "true" : "false") + ", " + std::to_string(cr) + "u, " + (hi ? "true" : "false");
     std::ostringstream body;
     const bool pairKind = op.kind == KOP_M2R || op.kind == KOP_M2I || op.kind == KOP_M2C || op.kind == KOP_X ||
@@ -505,13 +800,17 @@ std::string generatePairedSource(const TileProgram &prog, int W) {
             o << "    double2 acc_ = make_double2(prog.globalRe, prog.globalIm);\n";
         else if (fold)
             o << "    double2 acc_ = make_double2(1.0, 0.0);\n";
+        PairedSigns sg;
         for (int k = ph.opBegin; k < ph.opEnd; k++) {
             if (fold && scalarKindPaired(prog.ops[k]))
                 emitScalarAccPaired(o, prog.ops[k]);
             else
-                emitOpPaired(o, prog.ops[k]);
+                emitOpPaired(o, prog.ops[k], sg);
         }
-        if (fold) o << "    dgq::pGlobal(R, I, acc_.x, acc_.y);\n";
+        if (fold)
+            emitGlobalAbsorb(o, sg, "acc_.x", "acc_.y");
+        else
+            flushSigns(o, sg);
         if (writeSmem) {
             for (int j = 0; j < kRegs; j++)
                 o << "    sm[sb ^ " << ph.regOff[j] << "u] = make_float4(R[" << j << "].x, R[" << j << "].y, I[" << j
