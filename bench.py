@@ -690,12 +690,13 @@ def run_dense_form(args, world):
                      "hbm_gbs": 2.0 * (1 << n) * amp / (per / 1e3) / 1e9,
                      "device_errors": Q.dgq_getDeviceErrors()}
         states[name] = q
-    # one tensor-core block alone: plans of 4 and of 8 blocks differ by 4
-    # blocks (the initialisation and renormalisation passes cancel)
+    # one tensor-core block alone: plans of 4 and of 8 gates differ by the
+    # sweeps they plan (the initialisation and final renormalisation passes
+    # cancel; gates that commute onto the same targets share one block)
     hbm = peaks()[0]
     marginal = {}
     for K in (5, 6):
-        t_plan = []
+        t_plan, n_blocks = [], []
         for reps in (1, 2):
             q = Q.dgq_createQuregF32(n, env)
             Q.initPlusState(q)
@@ -706,6 +707,7 @@ def run_dense_form(args, world):
                     Q.multiQubitUnitary(q, Q.int_array(t[:K]), K, m)
                     Q.destroyComplexMatrixN(m)
             Q.dgq_planPending(q)
+            n_blocks.append(Q.plan_stats(q).sweeps)
             stream = torch.cuda.ExternalStream(Q.dgq_getStream(q))
             Q.dgq_launchPlanned(q)
             torch.cuda.synchronize()
@@ -718,8 +720,9 @@ def run_dense_form(args, world):
             torch.cuda.synchronize()
             t_plan.append(e0.elapsed_time(e1) / 3)
             Q.destroyQureg(q, env)
-        per = (t_plan[1] - t_plan[0]) / len(blocks)
-        marginal[f"k{K}"] = {"ms_per_block": per, "hbm_frac": 2.0 * (1 << n) * 8 / (per / 1e3) / 1e9 / hbm}
+        per = (t_plan[1] - t_plan[0]) / max(1, n_blocks[1] - n_blocks[0])
+        marginal[f"k{K}"] = {"ms_per_block": per, "hbm_frac": 2.0 * (1 << n) * 8 / (per / 1e3) / 1e9 / hbm,
+                             "sweeps_planned": n_blocks}
     out["complex64_tensor_cores"]["marginal_per_block"] = marginal
     out["fidelity_tc_vs_complex128"] = Q.calcFidelity(states["complex128_simt"], states["complex64_tensor_cores"])
     out["fidelity_simt_complex64_vs_complex128"] = Q.calcFidelity(states["complex128_simt"],

@@ -250,8 +250,10 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
                 const bool bit = ((loc & op.selLoc) != 0u) || (op.selCta >= 0 && ((cta >> op.selCta) & 1u));
                 if (bit) forAll(a, 0u, [&](V &x, int) { x = mk<V>(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
             } else {
-                const uint32_t sr = 1u << op.k;
-                forAll(a, sr, [&](V &x, int) { x = mk<V>(cs * x.x - sn * x.y, cs * x.y + sn * x.x); });
+                // the selector bit as a compile-time mask: 8 amplitudes, no predicates
+                DGQ_DISPATCH_K(op.k, forAll(a, 1u << K, [&](V &x, int) {
+                    x = mk<V>(cs * x.x - sn * x.y, cs * x.y + sn * x.x);
+                }));
             }
             break;
         }
