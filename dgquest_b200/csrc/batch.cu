@@ -164,7 +164,15 @@ __device__ __forceinline__ void sweepTile(const BatchArgs &args, const BatchSwee
                 const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(ops + o));
                 KOp op;
                 memcpy(&op, &raw, sizeof(op));
-                applyOp<V, DENSE, LEAN>(op, coef, a, loc, tile);
+                if constexpr (LEAN) {
+                    // the lean kinds' two coefficients, loaded beside the
+                    // record instead of after it
+                    const double2 cc = __ldg(args.leanCoef + h.opOff + o);
+                    const double cv[2] = {cc.x, cc.y};
+                    applyOpAt<V, DENSE, LEAN>(op, cv, a, loc, tile);
+                } else {
+                    applyOp<V, DENSE, LEAN>(op, coef, a, loc, tile);
+                }
             }
 #pragma unroll
             for (int j = 0; j < kRegs; j++) sm[sb ^ ph.regOff[j]] = a[j];

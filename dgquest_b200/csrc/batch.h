@@ -65,6 +65,7 @@ struct BatchArgs {
     const BatchSweep *sweeps;
     const KPhase *phases;
     const KOp *ops;
+    const double2 *leanCoef;  // lean form: the first two coefficients of each op, by op index
     const double *coef;
     const uint64_t *items;  // c | s << 20 | t << 36
     uint32_t numItems;

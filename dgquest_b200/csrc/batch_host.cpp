@@ -144,6 +144,7 @@ struct DeviceBatch {
     BatchSweep *sweeps = nullptr;
     KPhase *phases = nullptr;
     KOp *ops = nullptr;
+    double2 *leanCoef = nullptr;
     double *coef = nullptr;
     uint64_t *items = nullptr;
     uint32_t *counters = nullptr;  // ticket, then the done counters
@@ -160,7 +161,7 @@ struct DeviceBatch {
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        void *ptrs[] = {circ, sweeps, phases, ops, coef, items, counters, zsum, error};
+        void *ptrs[] = {circ, sweeps, phases, ops, leanCoef, coef, items, counters, zsum, error};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         *this = DeviceBatch();
@@ -235,6 +236,17 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
         lean = lean && ((dgq::kLeanKinds >> op.kind) & 1u);
     }
     const int form = dense ? dgq::kBatchFormDense : lean ? dgq::kBatchFormLean : dgq::kBatchFormGeneral;
+    // the lean form reads each op's (at most two) coefficients beside its record
+    std::vector<double2> leanCoef;
+    if (form == dgq::kBatchFormLean) {
+        leanCoef.assign(ops.size(), make_double2(0.0, 0.0));
+        for (const BatchSweep &h : sweeps)
+            for (int o = 0; o < h.numOps; o++) {
+                const size_t c = (size_t) h.coefOff + ops[h.opOff + o].coef;
+                if (c < coef.size()) leanCoef[h.opOff + o].x = coef[c];
+                if (c + 1 < coef.size()) leanCoef[h.opOff + o].y = coef[c + 1];
+            }
+    }
     d.numZ = std::max<uint32_t>(1, zOff);
 
     // work list: largest registers first; registers of several tiles in
@@ -275,6 +287,7 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
     if ((e = upload(&d.sweeps, sweeps, &d.programBytes)) != cudaSuccess) return e;
     if ((e = upload(&d.phases, phases, &d.programBytes)) != cudaSuccess) return e;
     if ((e = upload(&d.ops, ops, &d.programBytes)) != cudaSuccess) return e;
+    if ((e = upload(&d.leanCoef, leanCoef, &d.programBytes)) != cudaSuccess) return e;
     if ((e = upload(&d.coef, coef, &d.programBytes)) != cudaSuccess) return e;
     if ((e = upload(&d.items, items, &d.programBytes)) != cudaSuccess) return e;
     if ((e = cudaMalloc((void **) &d.counters, d.numCounters * sizeof(uint32_t))) != cudaSuccess) return e;
@@ -287,6 +300,7 @@ cudaError_t buildDevice(const std::vector<QuregState *> &regs, const std::vector
     a.sweeps = d.sweeps;
     a.phases = d.phases;
     a.ops = d.ops;
+    a.leanCoef = d.leanCoef;
     a.coef = d.coef;
     a.items = d.items;
     a.numItems = (uint32_t) d.numItems;

@@ -106,13 +106,13 @@ __device__ __forceinline__ void denseApply(V (&a)[kRegs], uint32_t ctrlReg, cons
 // (kLeanKinds, tile_program.h): every case is a path that updates the thread's amplitudes in
 // place, and fewer paths leave the compiler fewer register moves to
 // reconcile after the switch.
+// c: the op's own coefficients (coef + op.coef of its program).
 template <class V, bool DENSE = true, bool LEAN = false>
-__device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a)[kRegs], uint32_t loc,
-                                        uint32_t cta) {
+__device__ __forceinline__ void applyOpAt(const KOp &op, const double *c, V (&a)[kRegs], uint32_t loc,
+                                          uint32_t cta) {
     typedef typename Real<V>::T R;
     if ((cta & op.ctrlCta) != op.ctrlCta || (loc & op.ctrlLoc) != op.ctrlLoc) return;
     const uint32_t cr = op.ctrlReg;
-    const double *c = coef + op.coef;
     switch (op.kind) {
         case KOP_M2R:
             if constexpr (LEAN) break; {
@@ -280,6 +280,12 @@ __device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a
         default:
             break;
     }
+}
+
+template <class V, bool DENSE = true, bool LEAN = false>
+__device__ __forceinline__ void applyOp(const KOp &op, const double *coef, V (&a)[kRegs], uint32_t loc,
+                                        uint32_t cta) {
+    applyOpAt<V, DENSE, LEAN>(op, coef + op.coef, a, loc, cta);
 }
 
 }  // namespace dgq
