@@ -572,20 +572,37 @@ void emitOpPaired(std::ostringstream &o, const KOp &op, PairedSigns &sg) {
     const int k = op.k;
     const unsigned clr = op.ctrlLoc & ~1u;
     const bool runtimeCond = clr || op.ctrlCta;
+    auto condExpr = [&]() {
+        std::ostringstream cond;
+        bool any = false;
+        if (clr) {
+            cond << "((loc & " << clr << "u) == " << clr << "u)";
+            any = true;
+        }
+        if (op.ctrlCta) cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
+        return cond.str();
+    };
+    if (hi && op.kind == KOP_NEG) {
+        // -1 on the high amplitude of each (controlled) slot: flipping the
+        // stored high halves is right whatever their tracked signs
+        std::ostringstream body;
+        for (int j = 0; j < kRegs; j++)
+            if ((j & (int) cr) == (int) cr)
+                body << "    R[" << j << "].y = dgq::jFlip(R[" << j << "].y); I[" << j << "].y = dgq::jFlip(I[" << j
+                     << "].y);\n";
+        if (runtimeCond)
+            o << "    if (" << condExpr() << ") {\n" << body.str() << "    }\n";
+        else
+            o << body.str();
+        return;
+    }
     if (!hi) {
         std::ostringstream sbody;
         PairedSigns trial = sg;
         if (emitSignedPaired(sbody, op, trial, runtimeCond)) {
             sg = trial;
             if (runtimeCond) {
-                std::ostringstream cond;
-                bool any = false;
-                if (clr) {
-                    cond << "((loc & " << clr << "u) == " << clr << "u)";
-                    any = true;
-                }
-                if (op.ctrlCta) cond << (any ? " && " : "") << "((cta & " << op.ctrlCta << "u) == " << op.ctrlCta << "u)";
-                o << "    if (" << cond.str() << ") {\n" << sbody.str() << "    }\n";
+                o << "    if (" << condExpr() << ") {\n" << sbody.str() << "    }\n";
             } else {
                 o << sbody.str();
             }
