@@ -317,114 +317,94 @@ struct PairedSigns {
     }
 };
 
-const char *const kPairIn[4] = {"x0_", "x1_", "x2_", "x3_"};
+// template argument of a mask
+std::string hexu(uint32_t m) {
+    char b[16];
+    snprintf(b, sizeof b, "0x%xu", m);
+    return b;
+}
 
 void flushSigns(std::ostringstream &o, PairedSigns &sg) {
-    for (int j = 0; j < kRegs; j++) {
-        if ((sg.negR >> j) & 1u) o << "    R[" << j << "] = dgq::flip2(R[" << j << "]);\n";
-        if ((sg.negI >> j) & 1u) o << "    I[" << j << "] = dgq::flip2(I[" << j << "]);\n";
-    }
+    if (sg.negR | sg.negI) o << "    dgq::pFlushS<" << hexu(sg.negR) << ", " << hexu(sg.negI) << ">(R, I);\n";
     sg.negR = sg.negI = 0;
 }
 
-std::string pairDest(int c, int j0, int j1) {
-    return std::string((c & 1) ? "I[" : "R[") + std::to_string(c < 2 ? j0 : j1) + "]";
-}
-
+// f(p, j0, j1) for the pairs of register bit K whose j0 matches cr, p the
+// pair's index among all 8 (the index the prelude's masks use)
 template <class F>
 void forPairsHost(int K, uint32_t cr, F f) {
     for (int p = 0; p < kRegs / 2; p++) {
         const int j0 = ((p >> K) << (K + 1)) | (p & ((1 << K) - 1));
         const int j1 = j0 | (1 << K);
         if ((j0 & (int) cr) != (int) cr) continue;
-        f(j0, j1);
+        f(p, j0, j1);
     }
 }
 
-// Output c of a factored pair gate, in true values: u * in[b] + k * coef * in[a]
-// (u, k = +-1; coef is the op's coefficient, or 1 for H).
+// Output o of a factored pair gate, in true values: u * in[b] + k * coef * in[a]
+// (u, k = +-1; coef is the op's coefficient, or 1 for H). The prelude's
+// p*s templates fix b and a per kind; these tables give the signs.
 struct LinearOut {
     int b, u, a, k;
 };
 
-// Emits a factored pair gate on every pair of register bit K; cp_ / cn_
-// (+-coefficient) and m1_ (-1) are in scope. Output c is stored as
-// fma2(+-coef, in[a], in[b]) with the sign of u * (sign of in[b]): no
-// negation is computed.
-void emitLinearPairs(std::ostringstream &o, PairedSigns &sg, int K, const LinearOut (&outs)[4], bool unit) {
-    forPairsHost(K, 0u, [&](int j0, int j1) {
-        o << "    { const float2 x0_ = R[" << j0 << "], x1_ = I[" << j0 << "], x2_ = R[" << j1 << "], x3_ = I[" << j1
-          << "];";
+// Coefficient-sign mask of a factored pair gate on bit K: output o is
+// stored as fma2(+-coef, in[a], in[b]) with the sign of u * (sign of in[b]),
+// so no negation is computed.
+uint32_t linearMask(PairedSigns &sg, int K, const LinearOut (&outs)[4]) {
+    uint32_t cs = 0;
+    forPairsHost(K, 0u, [&](int p, int j0, int j1) {
         int ns[4];
         for (int c = 0; c < 4; c++) {
             const LinearOut &L = outs[c];
             const int sB = sg.sign(L.b, j0, j1), sA = sg.sign(L.a, j0, j1);
             ns[c] = L.u * sB;
-            const int coefSign = L.k * sA * L.u * sB;
-            o << " " << pairDest(c, j0, j1) << " = ";
-            if (unit)
-                o << (coefSign > 0 ? "dgq::add2(" + std::string(kPairIn[L.b]) + ", " + kPairIn[L.a] + ")"
-                                   : "dgq::fma2(m1_, " + std::string(kPairIn[L.a]) + ", " + kPairIn[L.b] + ")");
-            else
-                o << "dgq::fma2(" << (coefSign > 0 ? "cp_" : "cn_") << ", " << kPairIn[L.a] << ", " << kPairIn[L.b] << ")";
-            o << ";";
+            if (L.k * sA * L.u * sB < 0) cs |= 1u << (4 * p + c);
         }
         for (int c = 0; c < 4; c++) sg.set(c, j0, j1, ns[c]);
-        o << " }\n";
     });
+    return cs;
 }
 
-// Output c of a pair permutation (X, Y, Y*), in true values: m * in[src].
+// Output o of a pair permutation (X, Y, Y*), in true values: m * in[src].
 struct PermOut {
     int src, m;
 };
 
-// keep = true (the op runs under a condition known only at run time): the
-// outputs keep their slots' signs, with a flip where the two differ.
-void emitPermPairs(std::ostringstream &o, PairedSigns &sg, int K, uint32_t cr, const PermOut (&outs)[4], bool keep) {
-    forPairsHost(K, cr, [&](int j0, int j1) {
-        o << "    { const float2 x0_ = R[" << j0 << "], x1_ = I[" << j0 << "], x2_ = R[" << j1 << "], x3_ = I[" << j1
-          << "];";
+// Flip mask of a pair permutation; keep = true (the op runs under a
+// condition known only at run time): the outputs keep their slots' signs,
+// with a flip where the two differ; otherwise the signs move with the values.
+uint32_t permMask(PairedSigns &sg, int K, uint32_t cr, const PermOut (&outs)[4], bool keep) {
+    uint32_t fm = 0;
+    forPairsHost(K, cr, [&](int p, int j0, int j1) {
         int ns[4];
         for (int c = 0; c < 4; c++) {
             const int trueSign = outs[c].m * sg.sign(outs[c].src, j0, j1);
-            const std::string src = kPairIn[outs[c].src];
             if (keep) {
-                const bool flip = trueSign * sg.sign(c, j0, j1) < 0;
-                o << " " << pairDest(c, j0, j1) << " = " << (flip ? "dgq::flip2(" + src + ")" : src) << ";";
+                if (trueSign * sg.sign(c, j0, j1) < 0) fm |= 1u << (4 * p + c);
                 ns[c] = sg.sign(c, j0, j1);
             } else {
-                o << " " << pairDest(c, j0, j1) << " = " << src << ";";
                 ns[c] = trueSign;
             }
         }
         for (int c = 0; c < 4; c++) sg.set(c, j0, j1, ns[c]);
-        o << " }\n";
     });
+    return fm;
 }
 
-// Slot j times (c + i s), keeping the slot's signs; c / s / ns are float2
-// expressions in scope (ns = -s).
-void emitPhaseSlot(std::ostringstream &o, const PairedSigns &sg, int j, const std::string &c, const std::string &s,
-                   const std::string &ns) {
-    const bool differ = (((sg.negR ^ sg.negI) >> j) & 1u) != 0;
-    const std::string &k1 = differ ? s : ns, &k2 = differ ? ns : s;
-    o << "    { const float2 r_ = R[" << j << "]; R[" << j << "] = dgq::fma2(" << c << ", r_, dgq::mul2(" << k1 << ", I["
-      << j << "])); I[" << j << "] = dgq::fma2(" << c << ", I[" << j << "], dgq::mul2(" << k2 << ", r_)); }\n";
+// (c + i s) on the slots in `slots` ((c - i s) on those in `sw`), keeping
+// their signs; c / s / ns are float2 expressions (ns = -s)
+void emitPhaseSlots(std::ostringstream &o, const PairedSigns &sg, uint32_t slots, uint32_t sw, const std::string &c,
+                    const std::string &s, const std::string &ns) {
+    if (!slots) return;
+    o << "    dgq::pPhaseS<" << hexu(slots) << ", " << hexu((sg.negR ^ sg.negI) & slots) << ", " << hexu(sw & slots)
+      << ">(R, I, " << c << ", " << s << ", " << ns << ");\n";
 }
 
 // Every slot times (gr + i gi), absorbing the signs (the values leave with
 // their true signs); gr / gi are double expressions.
 void emitGlobalAbsorb(std::ostringstream &o, PairedSigns &sg, const std::string &gr, const std::string &gi) {
-    o << "    { const float2 c_ = dgq::b2((float) (" << gr << ")), nc_ = dgq::b2(-(float) (" << gr
-      << ")), s_ = dgq::b2((float) (" << gi << ")), ns_ = dgq::b2(-(float) (" << gi << "));\n";
-    for (int j = 0; j < kRegs; j++) {
-        const bool nR = (sg.negR >> j) & 1u, nI = (sg.negI >> j) & 1u;
-        o << "      { const float2 r_ = R[" << j << "]; R[" << j << "] = dgq::fma2(" << (nR ? "nc_" : "c_")
-          << ", r_, dgq::mul2(" << (nI ? "s_" : "ns_") << ", I[" << j << "])); I[" << j << "] = dgq::fma2("
-          << (nI ? "nc_" : "c_") << ", I[" << j << "], dgq::mul2(" << (nR ? "ns_" : "s_") << ", r_)); }\n";
-    }
-    o << "    }\n";
+    o << "    dgq::pGlobalS<" << hexu(sg.negR) << ", " << hexu(sg.negI) << ">(R, I, " << gr << ", " << gi << ");\n";
     sg.negR = sg.negI = 0;
 }
 
@@ -436,18 +416,11 @@ bool emitSignedPaired(std::ostringstream &body, const KOp &op, PairedSigns &sg, 
     const uint32_t cr = op.ctrlReg;
     const int k = op.k, off = op.coef;
     const std::string c0 = cf(off), c1 = cf(off + 1);
-    auto slotsOf = [&](uint32_t need, uint32_t sel, auto f) {
-        for (int j = 0; j < kRegs; j++) {
-            if ((j & (int) need) != (int) need) continue;
-            if (sel && (j & (int) sel) == 0) continue;
-            f(j);
-        }
-    };
-    auto phaseAll = [&](const std::string &cExpr, const std::string &sExpr, const std::string &nsExpr, uint32_t need,
-                        uint32_t sel) {
-        body << "    { const float2 pc_ = " << cExpr << ", ps_ = " << sExpr << ", pn_ = " << nsExpr << ";\n";
-        slotsOf(need, sel, [&](int j) { emitPhaseSlot(body, sg, j, "pc_", "ps_", "pn_"); });
-        body << "    }\n";
+    auto slotsOf = [&](uint32_t need, uint32_t sel) {
+        uint32_t m = 0;
+        for (int j = 0; j < kRegs; j++)
+            if ((j & (int) need) == (int) need && (!sel || (j & (int) sel))) m |= 1u << j;
+        return m;
     };
     const bool slotKind = op.kind == KOP_NEG || op.kind == KOP_MULI || op.kind == KOP_MULNI || op.kind == KOP_PH ||
                           op.kind == KOP_Z2 || op.kind == KOP_PH1;
@@ -469,14 +442,14 @@ bool emitSignedPaired(std::ostringstream &body, const KOp &op, PairedSigns &sg, 
                                      : op.kind == KOP_RX1 ? rx1
                                      : op.kind == KOP_RX2 ? rx2
                                                           : h1;
-            const bool unit = op.kind == KOP_H1;
-            body << "  {\n";
-            if (unit)
-                body << "    const float2 m1_ = dgq::b2(-1.0f);\n";
-            else
-                body << "    const float2 cp_ = dgq::b2(" << c0 << "), cn_ = dgq::b2(-" << c0 << ");\n";
-            emitLinearPairs(body, sg, k, t, unit);
-            body << "  }\n";
+            const char *name = op.kind == KOP_RY1   ? "pRY1s"
+                               : op.kind == KOP_RY2 ? "pRY2s"
+                               : op.kind == KOP_RX1 ? "pRX1s"
+                               : op.kind == KOP_RX2 ? "pRX2s"
+                                                    : "pH1s";
+            const uint32_t cs = linearMask(sg, k, t);
+            body << "    dgq::" << name << "<" << k << ", " << hexu(cs) << ">(R, I"
+                 << (op.kind == KOP_H1 ? std::string() : ", prog.coef + " + std::to_string(off)) << ");\n";
             return true;
         }
         case KOP_X:
@@ -485,77 +458,73 @@ bool emitSignedPaired(std::ostringstream &body, const KOp &op, PairedSigns &sg, 
             static const PermOut px[4] = {{2, 1}, {3, 1}, {0, 1}, {1, 1}};
             static const PermOut py[4] = {{3, 1}, {2, -1}, {1, -1}, {0, 1}};
             static const PermOut pyc[4] = {{3, -1}, {2, 1}, {1, 1}, {0, -1}};
-            emitPermPairs(body, sg, k, cr, op.kind == KOP_X ? px : op.kind == KOP_Y ? py : pyc, keep);
+            const uint32_t fm = permMask(sg, k, cr, op.kind == KOP_X ? px : op.kind == KOP_Y ? py : pyc, keep);
+            body << "    dgq::" << (op.kind == KOP_X ? "pXs" : "pYs") << "<" << k << ", " << cr << "u, " << hexu(fm)
+                 << ">(R, I);\n";
             return true;
         }
         case KOP_NEG:
             if (keep) {
-                slotsOf(cr, 0u, [&](int j) {
-                    body << "    R[" << j << "] = dgq::flip2(R[" << j << "]); I[" << j << "] = dgq::flip2(I[" << j
-                         << "]);\n";
-                });
+                // flips the stored values: right whatever their signs
+                body << "    dgq::pNEG<" << (cr ? "true" : "false") << ", " << cr << "u, false>(R, I);\n";
             } else {
-                slotsOf(cr, 0u, [&](int j) {
-                    sg.negR ^= 1u << j;
-                    sg.negI ^= 1u << j;
-                });
+                const uint32_t m = slotsOf(cr, 0u);
+                sg.negR ^= m;
+                sg.negI ^= m;
             }
             return true;
         case KOP_MULI:
         case KOP_MULNI: {
             // +i: (r, i) -> (-i, r); -i: (r, i) -> (i, -r)
             const int mr = op.kind == KOP_MULI ? -1 : 1, mi = -mr;
-            slotsOf(cr, 0u, [&](int j) {
+            const uint32_t slots = slotsOf(cr, 0u);
+            uint32_t fm = 0;
+            for (int j = 0; j < kRegs; j++) {
+                if (!((slots >> j) & 1u)) continue;
                 const int sR = ((sg.negR >> j) & 1u) ? -1 : 1, sI = ((sg.negI >> j) & 1u) ? -1 : 1;
                 const int tR = mr * sI, tI = mi * sR;  // signs of the swapped stored values
-                const std::string js = std::to_string(j);
                 if (keep) {
-                    body << "    { const float2 r_ = R[" << js << "]; R[" << js << "] = "
-                         << (tR * sR < 0 ? "dgq::flip2(I[" + js + "])" : "I[" + js + "]") << "; I[" << js
-                         << "] = " << (tI * sI < 0 ? "dgq::flip2(r_)" : "r_") << "; }\n";
+                    if (tR * sR < 0) fm |= 1u << (2 * j);
+                    if (tI * sI < 0) fm |= 1u << (2 * j + 1);
                 } else {
-                    body << "    { const float2 r_ = R[" << js << "]; R[" << js << "] = I[" << js << "]; I[" << js
-                         << "] = r_; }\n";
                     sg.negR = tR < 0 ? (sg.negR | (1u << j)) : (sg.negR & ~(1u << j));
                     sg.negI = tI < 0 ? (sg.negI | (1u << j)) : (sg.negI & ~(1u << j));
                 }
-            });
+            }
+            body << "    dgq::pSwapRIs<" << cr << "u, " << hexu(fm) << ">(R, I);\n";
             return true;
         }
         case KOP_PH:
-            phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", cr, 0u);
+            emitPhaseSlots(body, sg, slotsOf(cr, 0u), 0u, "dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")",
+                           "dgq::b2(-" + c1 + ")");
             return true;
         case KOP_Z2:
             if (op.code < KC_Z2T) {
                 // (c + i s) where register bit k is 1, (c - i s) where it is 0
-                body << "    { const float2 pc_ = dgq::b2(" << c0 << "), ps_ = dgq::b2(" << c1 << "), pn_ = dgq::b2(-"
-                     << c1 << ");\n";
-                slotsOf(cr, 0u, [&](int j) {
-                    if ((j >> k) & 1)
-                        emitPhaseSlot(body, sg, j, "pc_", "ps_", "pn_");
-                    else
-                        emitPhaseSlot(body, sg, j, "pc_", "pn_", "ps_");
-                });
-                body << "    }\n";
+                const uint32_t slots = slotsOf(cr, 0u);
+                emitPhaseSlots(body, sg, slots, slots & ~slotsOf(0u, 1u << k), "dgq::b2(" + c0 + ")",
+                               "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")");
             } else if (op.selLoc == 1u) {
-                phaseAll("dgq::b2(" + c0 + ")", "make_float2(-" + c1 + ", " + c1 + ")",
-                         "make_float2(" + c1 + ", -" + c1 + ")", cr, 0u);
+                emitPhaseSlots(body, sg, slotsOf(cr, 0u), 0u, "dgq::b2(" + c0 + ")",
+                               "make_float2(-" + c1 + ", " + c1 + ")", "make_float2(" + c1 + ", -" + c1 + ")");
             } else {
                 body << "    { const bool b_ = " << selExpr(op) << ";\n";
-                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(b_ ? " + c1 + " : -" + c1 + ")",
-                         "dgq::b2(b_ ? -" + c1 + " : " + c1 + ")", cr, 0u);
+                emitPhaseSlots(body, sg, slotsOf(cr, 0u), 0u, "dgq::b2(" + c0 + ")",
+                               "dgq::b2(b_ ? " + c1 + " : -" + c1 + ")", "dgq::b2(b_ ? -" + c1 + " : " + c1 + ")");
                 body << "    }\n";
             }
             return true;
         case KOP_PH1:
             if (op.code < KC_PH1T) {
-                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", 0u, 1u << k);
+                emitPhaseSlots(body, sg, slotsOf(0u, 1u << k), 0u, "dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")",
+                               "dgq::b2(-" + c1 + ")");
             } else if (op.selLoc == 1u) {
-                phaseAll("make_float2(1.0f, " + c0 + ")", "make_float2(0.0f, " + c1 + ")",
-                         "make_float2(-0.0f, -" + c1 + ")", 0u, 0u);
+                emitPhaseSlots(body, sg, 0xFFFFu, 0u, "make_float2(1.0f, " + c0 + ")", "make_float2(0.0f, " + c1 + ")",
+                               "make_float2(-0.0f, -" + c1 + ")");
             } else {
                 body << "    if (" << selExpr(op) << ") {\n";
-                phaseAll("dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")", "dgq::b2(-" + c1 + ")", 0u, 0u);
+                emitPhaseSlots(body, sg, 0xFFFFu, 0u, "dgq::b2(" + c0 + ")", "dgq::b2(" + c1 + ")",
+                               "dgq::b2(-" + c1 + ")");
                 body << "    }\n";
             }
             return true;
@@ -586,10 +555,7 @@ void emitOpPaired(std::ostringstream &o, const KOp &op, PairedSigns &sg) {
         // -1 on the high amplitude of each (controlled) slot: flipping the
         // stored high halves is right whatever their tracked signs
         std::ostringstream body;
-        for (int j = 0; j < kRegs; j++)
-            if ((j & (int) cr) == (int) cr)
-                body << "    R[" << j << "].y = dgq::jFlip(R[" << j << "].y); I[" << j << "].y = dgq::jFlip(I[" << j
-                     << "].y);\n";
+        body << "    dgq::pNEG<" << (cr ? "true" : "false") << ", " << cr << "u, true>(R, I);\n";
         if (runtimeCond)
             o << "    if (" << condExpr() << ") {\n" << body.str() << "    }\n";
         else

@@ -746,6 +746,115 @@ __device__ __forceinline__ void pGlobal(PRegs &R, PRegs &I, double grd, double g
 #pragma unroll
     for (int j = 0; j < kRegs; j++) pMulPhase(R[j], I[j], c, s, ns);
 }
+
+// ------------------------------------------- sign-tracked paired forms
+// The generator tracks which stored pairs hold negated values and passes
+// its decisions as masks: CS bit 4 p + o set means output o of pair p
+// (o: 0 R[j0], 1 I[j0], 2 R[j1], 3 I[j1]; pairs in register order) takes
+// the coefficient's negation, FM bit 4 p + o set means that output is
+// stored flipped; slot masks have bit j for slot j. The arithmetic of an
+// output is fma2(+-coef, A, B) with A and B fixed per kind.
+#define DGQS_PAIRS(K, CR, ...)                                                  \
+    _Pragma("unroll") for (int p_ = 0; p_ < kRegs / 2; p_++) {                  \
+        const int j0 = ((p_ >> (K)) << ((K) + 1)) | (p_ & ((1 << (K)) - 1));    \
+        const int j1 = j0 | (1 << (K));                                         \
+        if ((j0 & (CR)) != (CR)) continue;                                      \
+        const float2 rx = R[j0], ix = I[j0], ry = R[j1], iy = I[j1];            \
+        __VA_ARGS__                                                             \
+    }
+#define DGQS_C(o) ((CS >> (4 * p_ + (o))) & 1u ? n_ : c_)
+#define DGQS_F(o, v) ((FM >> (4 * p_ + (o))) & 1u ? flip2(v) : (v))
+template <int K, uint32_t CS>
+__device__ __forceinline__ void pRY1s(PRegs &R, PRegs &I, const double *c) {
+    const float2 c_ = b2((float) c[0]), n_ = b2(-(float) c[0]);
+    DGQS_PAIRS(K, 0, R[j0] = fma2(DGQS_C(0), ry, rx); I[j0] = fma2(DGQS_C(1), iy, ix);
+               R[j1] = fma2(DGQS_C(2), rx, ry); I[j1] = fma2(DGQS_C(3), ix, iy);)
+}
+template <int K, uint32_t CS>
+__device__ __forceinline__ void pRY2s(PRegs &R, PRegs &I, const double *c) {
+    const float2 c_ = b2((float) c[0]), n_ = b2(-(float) c[0]);
+    DGQS_PAIRS(K, 0, R[j0] = fma2(DGQS_C(0), rx, ry); I[j0] = fma2(DGQS_C(1), ix, iy);
+               R[j1] = fma2(DGQS_C(2), ry, rx); I[j1] = fma2(DGQS_C(3), iy, ix);)
+}
+template <int K, uint32_t CS>
+__device__ __forceinline__ void pRX1s(PRegs &R, PRegs &I, const double *c) {
+    const float2 c_ = b2((float) c[0]), n_ = b2(-(float) c[0]);
+    DGQS_PAIRS(K, 0, R[j0] = fma2(DGQS_C(0), iy, rx); I[j0] = fma2(DGQS_C(1), ry, ix);
+               R[j1] = fma2(DGQS_C(2), ix, ry); I[j1] = fma2(DGQS_C(3), rx, iy);)
+}
+template <int K, uint32_t CS>
+__device__ __forceinline__ void pRX2s(PRegs &R, PRegs &I, const double *c) {
+    const float2 c_ = b2((float) c[0]), n_ = b2(-(float) c[0]);
+    DGQS_PAIRS(K, 0, R[j0] = fma2(DGQS_C(0), rx, iy); I[j0] = fma2(DGQS_C(1), ix, ry);
+               R[j1] = fma2(DGQS_C(2), ry, ix); I[j1] = fma2(DGQS_C(3), iy, rx);)
+}
+// H without its 1/sqrt 2: a set CS bit subtracts A instead of adding it
+template <int K, uint32_t CS>
+__device__ __forceinline__ void pH1s(PRegs &R, PRegs &I) {
+    const float2 m1 = b2(-1.0f);
+#define DGQS_H(o, a, b) ((CS >> (4 * p_ + (o))) & 1u ? fma2(m1, (a), (b)) : add2((b), (a)))
+    DGQS_PAIRS(K, 0, R[j0] = DGQS_H(0, ry, rx); I[j0] = DGQS_H(1, iy, ix);
+               R[j1] = DGQS_H(2, ry, rx); I[j1] = DGQS_H(3, iy, ix);)
+#undef DGQS_H
+}
+// pair permutations: X swaps the slots; Y and Y* also swap the components
+template <int K, uint32_t CR, uint32_t FM>
+__device__ __forceinline__ void pXs(PRegs &R, PRegs &I) {
+    DGQS_PAIRS(K, CR, R[j0] = DGQS_F(0, ry); I[j0] = DGQS_F(1, iy); R[j1] = DGQS_F(2, rx); I[j1] = DGQS_F(3, ix);)
+}
+template <int K, uint32_t CR, uint32_t FM>
+__device__ __forceinline__ void pYs(PRegs &R, PRegs &I) {
+    DGQS_PAIRS(K, CR, R[j0] = DGQS_F(0, iy); I[j0] = DGQS_F(1, ry); R[j1] = DGQS_F(2, ix); I[j1] = DGQS_F(3, rx);)
+}
+// times +-i: the components swap (slot masks; FM bit 2 j + o, o: 0 R, 1 I)
+template <uint32_t NEED, uint32_t FM>
+__device__ __forceinline__ void pSwapRIs(PRegs &R, PRegs &I) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        if ((j & NEED) != NEED) continue;
+        const float2 r = R[j], i = I[j];
+        R[j] = (FM >> (2 * j)) & 1u ? flip2(i) : i;
+        I[j] = (FM >> (2 * j + 1)) & 1u ? flip2(r) : r;
+    }
+}
+// (c + i s) on the slots in SLOTS; DIFF: slots whose two pairs carry
+// different signs (the cross terms take the other sign); SW: slots that
+// take (c - i s) instead
+template <uint32_t SLOTS, uint32_t DIFF, uint32_t SW>
+__device__ __forceinline__ void pPhaseS(PRegs &R, PRegs &I, float2 c, float2 s, float2 ns) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        if (!((SLOTS >> j) & 1u)) continue;
+        const bool d = (((DIFF ^ SW) >> j) & 1u) != 0;
+        const float2 r = R[j];
+        R[j] = fma2(c, r, mul2(d ? s : ns, I[j]));
+        I[j] = fma2(c, I[j], mul2(d ? ns : s, r));
+    }
+}
+// every slot times (gr + i gi), leaving the values with their true signs
+template <uint32_t NR, uint32_t NI>
+__device__ __forceinline__ void pGlobalS(PRegs &R, PRegs &I, double grd, double gid) {
+    const float2 c = b2((float) grd), nc = b2(-(float) grd), s = b2((float) gid), ns = b2(-(float) gid);
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        const bool nr = (NR >> j) & 1u, ni = (NI >> j) & 1u;
+        const float2 r = R[j];
+        R[j] = fma2(nr ? nc : c, r, mul2(ni ? s : ns, I[j]));
+        I[j] = fma2(ni ? nc : c, I[j], mul2(nr ? ns : s, r));
+    }
+}
+// restores the true signs (integer-pipe flips)
+template <uint32_t NR, uint32_t NI>
+__device__ __forceinline__ void pFlushS(PRegs &R, PRegs &I) {
+#pragma unroll
+    for (int j = 0; j < kRegs; j++) {
+        if ((NR >> j) & 1u) R[j] = flip2(R[j]);
+        if ((NI >> j) & 1u) I[j] = flip2(I[j]);
+    }
+}
+#undef DGQS_F
+#undef DGQS_C
+#undef DGQS_PAIRS
 // Adds the CTA's sum of |a|^2 to *out (FP32 per thread, FP64 across threads).
 __device__ __forceinline__ void pNormAccumulate(const PRegs &R, const PRegs &I, double *out) {
     __shared__ double red[32];
