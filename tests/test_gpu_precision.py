@@ -102,6 +102,25 @@ def test_f32_paired_form(quest, env, specialise_all, n, tile_bits):
     assert np.abs(p0 - ref_p0).max() <= 1e-5
 
 
+@pytest.mark.parametrize("n,tile_bits", [(15, 13), (14, 11)])
+def test_f32_paired_sign_heavy(quest, env, specialise_all, n, tile_bits):
+    """Gates whose negations the paired generator carries as compile-time
+    signs (CZ, Y, S, controlled Y, X on a control, H and Rx / Ry at angles
+    of every quadrant), on every qubit including address bit 0, so signs
+    pass through rotations, swaps, phases, controls known only at run time
+    and the phase-end restore."""
+    Q = quest
+    kinds = [C.CZ, C.Y, C.S, C.CY, C.CNOT, C.H, C.RX, C.RY, C.RZ, C.Z, C.SWAP]
+    ops = np.concatenate([C.mixed_ops(n, 400, 700 + n, kinds=kinds), C.random_layers(n, 3, 11 + n)])
+    amps, p0, norm, _ = run_f32(Q, env, n, ops, tile_bits)
+    ref, ref_p0, _ = oracle.run(n, ops)
+    assert fidelity(ref, amps) >= 1 - 1e-6
+    assert np.abs(amps - ref).max() <= 2e-6
+    assert abs(norm - 1) <= 1e-5
+    assert np.abs(p0 - ref_p0).max() <= 1e-5
+
+
+
 def test_f32_paired_is_selected(quest, env, specialise_all):
     Q = quest
     n = 16
