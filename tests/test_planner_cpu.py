@@ -65,6 +65,24 @@ def test_generated_sweeps_compile(w, precision):
     assert all((b"float4 sm[]" in s) == (precision == 1) for s in srcs)
 
 
+def test_paired_sources_carry_signs_at_compile_time():
+    """The paired complex64 generator writes no negation into a kernel: CZ,
+    Y, S and the -1 entries of the factored rotations become compile-time
+    signs (template masks) that a phase's closing factor or a flip restores;
+    the kernels still compile."""
+    n = 14
+    kinds = [C.CZ, C.Y, C.S, C.CY, C.CNOT, C.H, C.RX, C.RY, C.RZ]
+    ops = np.concatenate([C.mixed_ops(n, 200, 21, kinds=kinds), C.random_layers(n, 2, 9)])
+    srcs = _sources(ops, n, 13, 1)
+    assert srcs and all(b"float4 sm[]" in s for s in srcs)
+    joined = b"".join(srcs)
+    assert b"neg2(" not in joined
+    assert b"dgq::pRY2s<" in joined or b"dgq::pRX2s<" in joined
+    assert b"dgq::pFlushS<" in joined or b"dgq::pGlobalS<" in joined
+    log = ctypes.create_string_buffer(1 << 16)
+    assert Q.dgq_compileSweepSource(srcs[0], log, len(log)) > 0, log.value.decode()
+
+
 @pytest.mark.parametrize("bad", ["multi_unitary_type", "type_out_of_range", "mask_beyond_register",
                                  "empty_target", "target_is_control"])
 def test_plan_gates_rejects_invalid_gates(bad):
